@@ -1,0 +1,192 @@
+// brig_common.cuh - types and integer mixing shared by the host planner and the sm_100a kernels.
+//
+// Tuples are (uint32 key, uint32 value). Inputs arrive as separate key and value arrays (the
+// reference's int* tableA / tableA_val, src/hash_kernel.cu:302-307). Every partitioned buffer the
+// engine writes stores a tuple as one 8-byte uint2 {key, value}, so a tuple moves with one
+// coalesced 8-byte access (the reference's int2 KV layout, src/kernel_functions.cu:251-281).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#if defined(__CUDACC__)
+#define BRIG_HD __host__ __device__ __forceinline__
+#else
+#define BRIG_HD inline
+#endif
+
+namespace brig {
+
+// ---- limits -------------------------------------------------------------------------------------
+constexpr int kMaxP1 = 4096;          // first-level fan-out (the reference caps at PARTITION_MAX=2048,
+                                      // src/kernel_functions.h:15)
+constexpr int kMaxP2 = 1024;          // second-level fan-out (SECOND_PASS_MAX=4096, :14)
+constexpr int kMaxTable = 8192;       // R tuples per shared-memory table
+constexpr int kMinTable = 256;
+constexpr int kMaxBloomK = 16;
+constexpr int kThreads = 512;         // threads per CTA of every partition and probe kernel
+constexpr int kTile = 4096;           // tuples per scatter tile staged in shared memory
+constexpr int kWarpBuf = 128;         // output pairs staged per warp before a global flush
+
+// Per-join device counters (int64 each).
+enum Counter : int {
+    kCntMatches = 0,      // exact number of matches
+    kCntSurvivors = 1,    // S tuples that passed the Bloom filter
+    kCntTasks = 2,        // probe tasks generated
+    kCntSplitTasks = 3,   // tasks whose R chunk is a piece of an oversized partition
+    kCntErrors = 4,       // device-side consistency failures (must stay 0)
+    kCntWords = 8
+};
+
+// ---- integer mixing -----------------------------------------------------------------------------
+// MurmurHash3 32-bit finaliser (Austin Appleby, public domain). A bijection on uint32: the radix
+// partition ids are its top bits, the shared-memory bucket its low bits. The reference's Bloom hash
+// is a variant of the same finaliser (src/bloom.cu:24-31).
+BRIG_HD uint32_t mix32(uint32_t x) {
+    x ^= x >> 16; x *= 0x85ebca6bu;
+    x ^= x >> 13; x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x;
+}
+
+// SplitMix64 finaliser (Steele, Lea, Flood, "Fast splittable pseudorandom number generators",
+// OOPSLA 2014). Used for the Bloom filter's block and bit positions and by the input generator.
+BRIG_HD uint64_t mix64(uint64_t x) {
+    x ^= x >> 30; x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27; x *= 0x94d049bb133111ebull;
+    x ^= x >> 31;
+    return x;
+}
+
+// Maps a uniform 32-bit value onto [0, n) with one multiply (Lemire, "Fast random integer
+// generation in an interval", 2019).
+BRIG_HD uint32_t fastrange32(uint32_t x, uint32_t n) {
+    return (uint32_t)(((uint64_t)x * (uint64_t)n) >> 32);
+}
+
+// a % d for a runtime divisor d >= 1 via a precomputed 64-bit magic M = floor((2^64-1)/d) + 1
+// (Lemire, Kaser, Kurz, "Faster remainder by direct computation", 2019).
+BRIG_HD uint64_t fastmod_magic(uint32_t d) { return ~0ull / d + 1; }
+BRIG_HD uint32_t fastmod(uint32_t a, uint64_t M, uint32_t d) {
+    uint64_t lowbits = M * a;
+#if defined(__CUDA_ARCH__)
+    return (uint32_t)__umul64hi(lowbits, (uint64_t)d);
+#else
+    return (uint32_t)(((unsigned __int128)lowbits * d) >> 64);
+#endif
+}
+
+// ---- partition functions ------------------------------------------------------------------------
+// Level-1 id p in [0, P1), level-2 id q in [0, P2). Hash mode: P1 = 2^b1, P2 = 2^b2 and the ids are
+// the top b1 bits and the next b2 bits of mix32(key). Modulo mode: p = key % P1, q = key % P2, the
+// reference's two modulo levels (src/kernel_functions.cu:66,187).
+struct PartFn {
+    int32_t mode;       // 0 hash, 1 modulo
+    int32_t b1, b2;     // radix bits (hash mode)
+    uint32_t P1, P2;    // fan-outs
+    uint64_t M1, M2;    // fastmod magics (modulo mode)
+};
+
+BRIG_HD uint32_t part1(const PartFn& f, uint32_t key) {
+    if (f.mode == 0) return f.b1 == 0 ? 0u : (mix32(key) >> (32 - f.b1));
+    return fastmod(key, f.M1, f.P1);
+}
+BRIG_HD uint32_t part2(const PartFn& f, uint32_t key) {
+    if (f.mode == 0) return f.b2 == 0 ? 0u : ((mix32(key) << f.b1) >> (32 - f.b2));
+    return fastmod(key, f.M2, f.P2);
+}
+// Finest partition id p * P2 + q: the probe-task unit and the Bloom segment index.
+BRIG_HD uint32_t part_fine(const PartFn& f, uint32_t key) {
+    return part1(f, key) * f.P2 + part2(f, key);
+}
+// Shared-memory bucket of a key in a table of nb (power of two) buckets: the low bits of the mix.
+BRIG_HD uint32_t bucket_of(uint32_t key, uint32_t nb_mask) { return mix32(key) & nb_mask; }
+
+// ---- Bloom filter -------------------------------------------------------------------------------
+// Cache-line blocked: the filter is one segment per finest partition, a segment is seg_blocks
+// blocks of 256 bits (one 32-byte DRAM sector), and a key sets k bits inside one block. Bit i of a
+// key is (a + i*b) mod 256 with b odd, so the k bits are distinct (double hashing, Kirsch &
+// Mitzenmacher, "Less hashing, same performance", 2006). The reference uses 256-bit blocks and one
+// segment per first-level partition (src/bloom.cu:698-722, src/hash_kernel.cu:555-582).
+struct BloomKey {
+    uint32_t block;     // block index inside the segment
+    uint32_t mask[8];   // bits to set/test in the block's 8 words
+};
+
+BRIG_HD uint64_t bloom_hash(uint32_t key) { return mix64((uint64_t)key ^ 0x6a09e667f3bcc909ull); }
+
+BRIG_HD void bloom_key(uint32_t key, uint32_t seg_blocks, int k, BloomKey& bk) {
+    uint64_t g = bloom_hash(key);
+    bk.block = fastrange32((uint32_t)(g >> 32), seg_blocks);
+    uint32_t a = (uint32_t)g & 255u;
+    uint32_t b = ((uint32_t)(g >> 8) & 255u) | 1u;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) bk.mask[w] = 0;
+    // Unrolled with compare-and-select so the mask stays in registers (no dynamic indexing).
+#pragma unroll
+    for (int i = 0; i < kMaxBloomK; ++i) {
+        if (i < k) {
+            const uint32_t pos = (a + (uint32_t)i * b) & 255u;
+            const uint32_t w = pos >> 5, bit = 1u << (pos & 31u);
+#pragma unroll
+            for (int ww = 0; ww < 8; ++ww) bk.mask[ww] |= (w == (uint32_t)ww) ? bit : 0u;
+        }
+    }
+}
+
+// ---- per-join descriptor (device resident) ------------------------------------------------------
+struct RelPlan {
+    const uint32_t* key;   // input keys
+    const uint32_t* val;   // input values
+    int64_t n;             // input tuples
+    uint2* l1;             // level-1 partitioned tuples [n]
+    uint2* l2;             // level-2 partitioned tuples [n] (nullptr when P2 == 1)
+    uint2* cmp;            // Bloom survivors staged per slice [n] (S with Bloom only)
+    int64_t slice_len;     // tuples per level-1 slice
+    int32_t nslices;       // level-1 slices
+    int32_t pad;
+    int64_t hist_base;     // offset of this relation's [P1][nslices]+1 histogram in the global array
+    int64_t* b1;           // [P1 + 1] start of each level-1 partition in l1
+    int64_t* bounds;       // [P1*P2 + 1] start of each finest partition in the final buffer
+                           // (equal to b1 when P2 == 1)
+    uint32_t* slice_cnt;   // [nslices] survivors per slice (S with Bloom only)
+};
+
+struct JoinDesc {
+    RelPlan rel[2];        // 0 = R (build side), 1 = S (probe side)
+    PartFn pf;
+    uint32_t* out_r;       // pair outputs
+    uint32_t* out_s;
+    uint32_t* out_k;       // may be nullptr
+    int64_t cap;           // output capacity (pairs)
+    int64_t* counters;     // [kCntWords]
+    int64_t* user_count;   // optional user int64 receiving the match count
+    uint32_t* bloom;       // filter words (nullptr when off)
+    uint32_t seg_blocks;   // blocks per Bloom segment
+    int32_t bloom_k;
+    int64_t fine_base;     // offset of this join's P1*P2 entries in the global task-count array
+    int32_t table_cap;     // max R tuples per probe task
+    int32_t s_chunk;       // max S tuples per probe task
+};
+
+// One probe task: build a table from R[r_begin, r_begin + r_len) and probe it with
+// S[s_begin, s_begin + s_len), both in the join's final partitioned buffers.
+struct Task {
+    int32_t join;
+    uint32_t r_len;
+    int64_t r_begin;
+    uint32_t s_len;
+    uint32_t split;        // 1 if the R chunk is a piece of an oversized partition
+    int64_t s_begin;
+};
+static_assert(sizeof(Task) == 32, "task layout");
+
+// Global queue/state words of one pipeline run (int64 each).
+enum GlobalWord : int {
+    kGQueue = 0,           // next task index to hand out
+    kGTasks = 1,           // total tasks (written by the task builder)
+    kGErrors = 2,          // device-side consistency failures
+    kGWords = 4
+};
+
+}  // namespace brig

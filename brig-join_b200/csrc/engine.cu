@@ -1,0 +1,526 @@
+// engine.cu - planner, workspace layout and pipeline orchestration (host C++).
+//
+// Replaces gpu_main's one-PE slice (src/hash_kernel.cu:103-1131): sizing (:173-284), allocation
+// (:370-480), the use_bf==10 partitioned filter (:555-582, :670-705), the S chunk prefilter
+// (:935-954) and the partition/probe sequence (:1073-1130). The reference synchronises the host
+// after nearly every stage (src/vlsplit_hash_kernel.cu:36-107, src/join_executor.cu:49); here the
+// whole pipeline is enqueued on one stream with every size it needs computed on the device, so a
+// run is a single stream-ordered unit that can be captured in a CUDA graph.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include "engine.h"
+
+namespace brig {
+
+[[noreturn]] void fail(int status, const std::string& msg) { throw Error{status, msg}; }
+
+void cuda_check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    const int st = (e == cudaErrorMemoryAllocation) ? BRIG_E_NOMEM : BRIG_E_CUDA;
+    fail(st, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+static int ceil_log2(int64_t x) {
+    int b = 0;
+    while (((int64_t)1 << b) < x) ++b;
+    return b;
+}
+static bool is_pow2(int64_t x) { return x > 0 && (x & (x - 1)) == 0; }
+
+JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
+    JoinPlan p;
+    p.nr = nr;
+    p.ns = ns;
+    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kMaxTable;
+    const int64_t target = std::max<int64_t>(1, (int64_t)T * 3 / 4);  // R tuples per finest partition
+    PartFn& f = p.pf;
+    f.mode = cfg.partition_mode;
+    if (f.mode == BRIG_PART_HASH) {
+        const int bits = ceil_log2(std::max<int64_t>(1, (nr + target - 1) / target));
+        int b1, b2;
+        if (cfg.partition_size > 0) {
+            if (!is_pow2(cfg.partition_size) || cfg.partition_size > kMaxP1)
+                fail(BRIG_E_INVALID, "hash partitioning needs a power-of-two partition_size <= 4096 "
+                                     "(use BRIG_PART_MODULO for other fan-outs)");
+            b1 = ceil_log2(cfg.partition_size);
+        } else {
+            b1 = bits <= 12 ? bits : 11;
+        }
+        if (cfg.second_partition_size > 0) {
+            if (!is_pow2(cfg.second_partition_size) || cfg.second_partition_size > kMaxP2)
+                fail(BRIG_E_INVALID, "hash partitioning needs a power-of-two second_partition_size <= 1024");
+            b2 = ceil_log2(cfg.second_partition_size);
+        } else {
+            b2 = std::max(0, bits - b1);
+            if (b2 > 10) fail(BRIG_E_UNSUPPORTED, "relation too large for two partition levels");
+        }
+        if (b1 + b2 > 24) fail(BRIG_E_UNSUPPORTED, "more than 2^24 finest partitions");
+        f.b1 = b1;
+        f.b2 = b2;
+        f.P1 = 1u << b1;
+        f.P2 = 1u << b2;
+    } else if (f.mode == BRIG_PART_MODULO) {
+        const int64_t P1 = cfg.partition_size > 0 ? cfg.partition_size : 512;
+        if (P1 > kMaxP1) fail(BRIG_E_INVALID, "partition_size > 4096");
+        int64_t P2 = cfg.second_partition_size;
+        if (P2 <= 0) {
+            // The reference starts at 67 and grows to the next odd value when the average
+            // sub-bucket exceeds the table target (src/hash_kernel.cu:240-284).
+            P2 = 67;
+            const int64_t sub = (nr + P1 * P2 - 1) / (P1 * P2);
+            if (sub > target) {
+                P2 = (nr + P1 * target - 1) / (P1 * target);
+                if (P2 % 2 == 0) ++P2;
+            }
+        }
+        if (P2 > kMaxP2) fail(BRIG_E_UNSUPPORTED, "second_partition_size > 1024 (raise partition_size)");
+        f.P1 = (uint32_t)P1;
+        f.P2 = (uint32_t)P2;
+        f.M1 = fastmod_magic(f.P1);
+        f.M2 = fastmod_magic(f.P2);
+    } else {
+        fail(BRIG_E_INVALID, "unknown partition_mode");
+    }
+    p.nfine = (int64_t)f.P1 * f.P2;
+    if (cfg.use_bloom) {
+        const double bpk = cfg.bloom_bits_per_key > 0 ? cfg.bloom_bits_per_key : 10.0;
+        int64_t bits = cfg.bloom_num_bits > 0 ? cfg.bloom_num_bits : (int64_t)std::llround(bpk * (double)nr);
+        bits = std::max<int64_t>(bits, 256);
+        int k = cfg.bloom_num_hashes > 0 ? cfg.bloom_num_hashes : (int)std::lround(bpk * std::log(2.0));
+        k = std::min(std::max(k, 1), kMaxBloomK);
+        const int64_t blocks = (bits + 255) / 256;
+        p.seg_blocks = (uint32_t)std::max<int64_t>(1, (blocks + p.nfine - 1) / p.nfine);
+        p.bloom = true;
+        p.k = k;
+        p.bloom_bits = p.nfine * (int64_t)p.seg_blocks * 256;
+    }
+    return p;
+}
+
+// ---- workspace layout ---------------------------------------------------------------------------
+namespace {
+
+struct Layout {
+    size_t off = 0;
+    size_t take(size_t bytes) {
+        off = (off + 255) & ~(size_t)255;
+        const size_t o = off;
+        off += bytes;
+        return o;
+    }
+};
+
+struct RelOffs {
+    size_t l1 = 0, l2 = 0, cmp = 0, b1 = 0, bounds = 0, slice_cnt = 0;
+    int64_t slice_len = 0;
+    int32_t nslices = 0;
+    int64_t hist_base = 0;
+};
+struct JoinOffs {
+    RelOffs rel[2];
+    size_t bloom = 0;
+};
+
+struct Shape {
+    std::vector<JoinOffs> jo;
+    int64_t slice_len = 0;
+    int64_t hist_len[2] = {0, 0};
+    int64_t total_slices[2] = {0, 0};
+    int64_t total_segs = 0, total_fine = 0, total_bloom_fine = 0;
+    int64_t task_cap = 0;
+    size_t hist = 0, hist_scan = 0, tcount = 0, toff = 0, tasks = 0, scan_tmp = 0, gwords = 0,
+           counters = 0, meta = 0;
+    int64_t scan_tmp_len = 0;
+    size_t meta_bytes = 0;
+    size_t total = 0;
+    int max_p1 = 1, max_p2 = 1, max_seg_words = 0;
+    bool any_bloom = false;
+};
+
+Shape layout_for(const brig_join_config& cfg, const std::vector<JoinPlan>& plans, int num_sms) {
+    Shape sh;
+    const int nj = (int)plans.size();
+    sh.jo.resize(nj);
+    int64_t total_tuples = 0;
+    for (const auto& p : plans) total_tuples += p.nr + p.ns;
+    // Slices of about total/(8 * SMs) tuples, a multiple of the scatter tile, at least 4 tiles.
+    const int64_t target = (int64_t)num_sms * 8;
+    int64_t sl = (total_tuples + target - 1) / std::max<int64_t>(target, 1);
+    sl = ((sl + kTile - 1) / kTile) * kTile;
+    sl = std::max<int64_t>(sl, 4 * kTile);
+    sh.slice_len = sl;
+    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kMaxTable;
+    const int C = cfg.s_chunk > 0 ? cfg.s_chunk : 16384;
+    Layout L;
+    for (int j = 0; j < nj; ++j) {
+        const JoinPlan& p = plans[j];
+        JoinOffs& o = sh.jo[j];
+        const int64_t n[2] = {p.nr, p.ns};
+        const bool two = p.pf.P2 > 1;
+        sh.max_p1 = std::max<int>(sh.max_p1, (int)p.pf.P1);
+        sh.max_p2 = std::max<int>(sh.max_p2, (int)p.pf.P2);
+        for (int r = 0; r < 2; ++r) {
+            RelOffs& ro = o.rel[r];
+            ro.slice_len = sl;
+            ro.nslices = (int32_t)std::max<int64_t>(1, (n[r] + sl - 1) / sl);
+            ro.l1 = L.take((size_t)std::max<int64_t>(n[r], 1) * 8);
+            if (two) ro.l2 = L.take((size_t)std::max<int64_t>(n[r], 1) * 8);
+            ro.b1 = L.take(((size_t)p.pf.P1 + 1) * 8);
+            if (two) ro.bounds = L.take(((size_t)p.nfine + 1) * 8);
+            if (r == 1 && p.bloom) {
+                ro.cmp = L.take((size_t)std::max<int64_t>(n[r], 1) * 8);
+                ro.slice_cnt = L.take((size_t)ro.nslices * 4);
+            }
+            ro.hist_base = sh.hist_len[0] + sh.hist_len[1];  // provisional, fixed below
+            sh.total_slices[r] += ro.nslices;
+        }
+        if (p.bloom) {
+            o.bloom = L.take((size_t)p.nfine * p.seg_blocks * 32);
+            sh.any_bloom = true;
+            sh.total_bloom_fine += p.nfine;
+            sh.max_seg_words = std::max<int>(sh.max_seg_words, (int)(p.seg_blocks * 8));
+        }
+        if (two) sh.total_segs += p.pf.P1;
+        sh.total_fine += p.nfine;
+        sh.task_cap += p.nfine + p.nr / T + p.ns / C + 2;
+    }
+    // Histograms: all R regions, then all S regions (each scanned as one sequence).
+    for (int r = 0; r < 2; ++r) {
+        int64_t base = (r == 0) ? 0 : sh.hist_len[0];
+        for (int j = 0; j < nj; ++j) {
+            RelOffs& ro = sh.jo[j].rel[r];
+            ro.hist_base = base;
+            base += (int64_t)plans[j].pf.P1 * ro.nslices + 1;
+        }
+        sh.hist_len[r] = base - ((r == 0) ? 0 : sh.hist_len[0]);
+    }
+    const int64_t hist_total = sh.hist_len[0] + sh.hist_len[1];
+    sh.hist = L.take((size_t)hist_total * 4);
+    sh.hist_scan = L.take((size_t)hist_total * 8);
+    sh.tcount = L.take(((size_t)sh.total_fine + 1) * 4);
+    sh.toff = L.take(((size_t)sh.total_fine + 1) * 8);
+    sh.tasks = L.take((size_t)sh.task_cap * sizeof(Task));
+    sh.scan_tmp_len = std::max(scan_tmp_words(std::max(sh.hist_len[0], sh.hist_len[1])),
+                               scan_tmp_words(sh.total_fine + 1));
+    sh.scan_tmp = L.take((size_t)sh.scan_tmp_len * 8);
+    sh.gwords = L.take(kGWords * 8);
+    sh.counters = L.take((size_t)nj * kCntWords * 8);
+    sh.meta_bytes = (size_t)nj * sizeof(JoinDesc) + 5 * ((size_t)nj + 1) * 8;
+    sh.meta = L.take(sh.meta_bytes);
+    sh.total = L.off + 256;
+    return sh;
+}
+
+}  // namespace
+
+int64_t Engine::workspace_needed(const brig_join_config& cfg, const std::vector<JoinPlan>& plans,
+                                 int num_sms) {
+    return (int64_t)layout_for(cfg, plans, num_sms).total;
+}
+
+Engine::Engine(const brig_join_config& cfg) : cfg_(cfg) {
+    if (cfg.device >= 0) cuda_check(cudaSetDevice(cfg.device), "cudaSetDevice");
+    cuda_check(cudaGetDevice(&device_), "cudaGetDevice");
+    cuda_check(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, device_),
+               "cudaDeviceGetAttribute");
+    int major = 0;
+    cuda_check(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device_),
+               "cudaDeviceGetAttribute");
+    if (major != 10) fail(BRIG_E_UNSUPPORTED, "this build targets sm_100a (B200)");
+    cuda_check(cudaEventCreateWithFlags(&stage_free_, cudaEventDisableTiming), "cudaEventCreate");
+    cuda_check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "cudaEventCreate");
+    if (cfg.profile_stages) {
+        for (auto& e : stage_ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        profiling_ = true;
+    }
+}
+
+void Engine::stage_times(double* ms, int n) {
+    if (!profiling_) fail(BRIG_E_INVALID, "handle created without profile_stages");
+    if (!have_run_) fail(BRIG_E_INVALID, "no run on this handle");
+    cuda_check(cudaEventSynchronize(done_), "cudaEventSynchronize");
+    for (int i = 0; i < n && i < kNumStages; ++i) {
+        float t = 0.f;
+        cuda_check(cudaEventElapsedTime(&t, stage_ev_[i], stage_ev_[i + 1]), "cudaEventElapsedTime");
+        ms[i] = t;
+    }
+}
+
+Engine::~Engine() {
+    if (have_run_) cudaEventSynchronize(done_);
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (ws_) cudaFree(ws_);
+    if (stage_) cudaFreeHost(stage_);
+    if (hio.rk) cudaFree(hio.rk);
+    if (hio.rv) cudaFree(hio.rv);
+    if (hio.sk) cudaFree(hio.sk);
+    if (hio.sv) cudaFree(hio.sv);
+    if (hio.outr) cudaFree(hio.outr);
+    if (hio.outs) cudaFree(hio.outs);
+    if (hio.outk) cudaFree(hio.outk);
+    for (auto& e : stage_ev_)
+        if (e) cudaEventDestroy(e);
+    if (stage_free_) cudaEventDestroy(stage_free_);
+    if (done_) cudaEventDestroy(done_);
+}
+
+void Engine::ensure_workspace(size_t bytes) {
+    if (bytes <= ws_bytes_) return;
+    if (have_run_) cuda_check(cudaEventSynchronize(done_), "cudaEventSynchronize");
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+        graph_key_.clear();
+    }
+    if (ws_) cudaFree(ws_);
+    ws_ = nullptr;
+    ws_bytes_ = 0;
+    cuda_check(cudaMalloc(&ws_, bytes), "workspace cudaMalloc");
+    ws_bytes_ = bytes;
+}
+
+void Engine::ensure_staging(size_t bytes) {
+    if (bytes <= stage_bytes_) return;
+    if (have_run_) cuda_check(cudaEventSynchronize(done_), "cudaEventSynchronize");
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+        graph_key_.clear();
+    }
+    if (stage_) cudaFreeHost(stage_);
+    stage_ = nullptr;
+    stage_bytes_ = 0;
+    const size_t b = std::max<size_t>(bytes, 64 * 1024);
+    cuda_check(cudaMallocHost(&stage_, b), "pinned staging cudaMallocHost");
+    stage_bytes_ = b;
+}
+
+static void grow(uint32_t*& p, int64_t& cap, int64_t need) {
+    if (need <= cap && p) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    cuda_check(cudaMalloc(&p, (size_t)std::max<int64_t>(need, 1) * 4), "io cudaMalloc");
+    cap = need;
+}
+
+void Engine::ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key) {
+    if (have_run_) cuda_check(cudaEventSynchronize(done_), "cudaEventSynchronize");
+    int64_t c = hio.cap_in_r;
+    grow(hio.rk, c, nr);
+    c = hio.cap_in_r;
+    grow(hio.rv, c, nr);
+    hio.cap_in_r = std::max(hio.cap_in_r, nr);
+    c = hio.cap_in_s;
+    grow(hio.sk, c, ns);
+    c = hio.cap_in_s;
+    grow(hio.sv, c, ns);
+    hio.cap_in_s = std::max(hio.cap_in_s, ns);
+    c = hio.cap_out;
+    grow(hio.outr, c, cap);
+    c = hio.cap_out;
+    grow(hio.outs, c, cap);
+    if (key) {
+        c = hio.outk_alloc ? hio.cap_out : 0;
+        grow(hio.outk, c, cap);
+        hio.outk_alloc = true;
+    }
+    hio.cap_out = std::max(hio.cap_out, cap);
+}
+
+void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph) {
+    const int nj = (int)joins.size();
+    if (nj <= 0) fail(BRIG_E_INVALID, "no joins");
+    std::vector<JoinPlan> plans(nj);
+    for (int j = 0; j < nj; ++j) plans[j] = plan_join(cfg_, joins[j].nr, joins[j].ns);
+    const Shape sh = layout_for(cfg_, plans, num_sms_);
+    const int T = cfg_.table_capacity > 0 ? cfg_.table_capacity : kMaxTable;
+    const int C = cfg_.s_chunk > 0 ? cfg_.s_chunk : 16384;
+    if (T < kMinTable || T > kMaxTable || !is_pow2(T))
+        fail(BRIG_E_INVALID, "table_capacity must be a power of two in [256, 8192]");
+    if (C < 1) fail(BRIG_E_INVALID, "s_chunk must be >= 1");
+
+    ensure_workspace(sh.total);
+    ensure_staging(sh.meta_bytes);
+    // The staging buffer may still be read by the previous run's copy.
+    if (have_run_) cuda_check(cudaEventSynchronize(stage_free_), "cudaEventSynchronize");
+
+    char* ws = ws_;
+    JoinDesc* hJ = reinterpret_cast<JoinDesc*>(stage_);
+    int64_t* hpre = reinterpret_cast<int64_t*>(stage_ + (size_t)nj * sizeof(JoinDesc));
+    int64_t* sp0 = hpre;
+    int64_t* sp1 = hpre + (nj + 1);
+    int64_t* segp = hpre + 2 * (nj + 1);
+    int64_t* finep = hpre + 3 * (nj + 1);
+    int64_t* bloomp = hpre + 4 * (nj + 1);
+    sp0[0] = sp1[0] = segp[0] = finep[0] = bloomp[0] = 0;
+    int64_t* counters = reinterpret_cast<int64_t*>(ws + sh.counters);
+    for (int j = 0; j < nj; ++j) {
+        const JoinPlan& p = plans[j];
+        const JoinOffs& o = sh.jo[j];
+        const JoinIO& io = joins[j];
+        JoinDesc d;
+        std::memset(&d, 0, sizeof(d));
+        const uint32_t* keys[2] = {io.rk, io.sk};
+        const uint32_t* vals[2] = {io.rv, io.sv};
+        const int64_t n[2] = {io.nr, io.ns};
+        for (int r = 0; r < 2; ++r) {
+            RelPlan& R = d.rel[r];
+            const RelOffs& ro = o.rel[r];
+            R.key = keys[r];
+            R.val = vals[r];
+            R.n = n[r];
+            R.l1 = reinterpret_cast<uint2*>(ws + ro.l1);
+            R.l2 = p.pf.P2 > 1 ? reinterpret_cast<uint2*>(ws + ro.l2) : nullptr;
+            R.cmp = ro.cmp ? reinterpret_cast<uint2*>(ws + ro.cmp) : nullptr;
+            R.slice_len = ro.slice_len;
+            R.nslices = ro.nslices;
+            R.hist_base = ro.hist_base;
+            R.b1 = reinterpret_cast<int64_t*>(ws + ro.b1);
+            R.bounds = p.pf.P2 > 1 ? reinterpret_cast<int64_t*>(ws + ro.bounds) : R.b1;
+            R.slice_cnt = ro.slice_cnt ? reinterpret_cast<uint32_t*>(ws + ro.slice_cnt) : nullptr;
+        }
+        d.pf = p.pf;
+        d.out_r = io.out.r_val;
+        d.out_s = io.out.s_val;
+        d.out_k = io.out.key;
+        d.cap = io.out.capacity;
+        d.counters = counters + (size_t)j * kCntWords;
+        d.user_count = io.out.d_count;
+        d.bloom = p.bloom ? reinterpret_cast<uint32_t*>(ws + o.bloom) : nullptr;
+        d.seg_blocks = p.seg_blocks;
+        d.bloom_k = p.k;
+        d.fine_base = finep[j];
+        d.table_cap = T;
+        d.s_chunk = C;
+        hJ[j] = d;
+        sp0[j + 1] = sp0[j] + o.rel[0].nslices;
+        sp1[j + 1] = sp1[j] + o.rel[1].nslices;
+        segp[j + 1] = segp[j] + (p.pf.P2 > 1 ? p.pf.P1 : 0);
+        finep[j + 1] = finep[j] + p.nfine;
+        bloomp[j + 1] = bloomp[j] + (p.bloom ? p.nfine : 0);
+    }
+    char* meta = ws + sh.meta;
+    const int64_t* dpre = reinterpret_cast<const int64_t*>(meta + (size_t)nj * sizeof(JoinDesc));
+
+    PipelineArgs a{};
+    a.J = reinterpret_cast<const JoinDesc*>(meta);
+    a.nj = nj;
+    a.slice_prefix[0] = dpre;
+    a.slice_prefix[1] = dpre + (nj + 1);
+    a.seg_prefix = dpre + 2 * (nj + 1);
+    a.fine_prefix = dpre + 3 * (nj + 1);
+    a.bloom_prefix = dpre + 4 * (nj + 1);
+    a.total_slices[0] = sh.total_slices[0];
+    a.total_slices[1] = sh.total_slices[1];
+    a.total_segs = sh.total_segs;
+    a.total_fine = sh.total_fine;
+    a.total_bloom_fine = sh.total_bloom_fine;
+    a.hist_begin[0] = 0;
+    a.hist_len[0] = sh.hist_len[0];
+    a.hist_begin[1] = sh.hist_len[0];
+    a.hist_len[1] = sh.hist_len[1];
+    a.hist = reinterpret_cast<uint32_t*>(ws + sh.hist);
+    a.hist_scan = reinterpret_cast<int64_t*>(ws + sh.hist_scan);
+    a.tcount = reinterpret_cast<uint32_t*>(ws + sh.tcount);
+    a.toff = reinterpret_cast<int64_t*>(ws + sh.toff);
+    a.tasks = reinterpret_cast<Task*>(ws + sh.tasks);
+    a.task_cap = sh.task_cap;
+    a.scan_tmp = reinterpret_cast<int64_t*>(ws + sh.scan_tmp);
+    a.scan_tmp_len = sh.scan_tmp_len;
+    a.gwords = reinterpret_cast<unsigned long long*>(ws + sh.gwords);
+    a.max_p1 = sh.max_p1;
+    a.max_p2 = sh.max_p2;
+    a.max_seg_words = sh.max_seg_words;
+    a.table_cap = T;
+    a.emit_key = 0;
+    for (const auto& io : joins)
+        if (io.out.key) a.emit_key = 1;
+    a.any_bloom = sh.any_bloom ? 1 : 0;
+    a.num_sms = num_sms_;
+    a.stage_events = profiling_ ? stage_ev_ : nullptr;
+
+    auto enqueue_all = [&](cudaStream_t st) {
+        cuda_check(cudaMemcpyAsync(meta, stage_, sh.meta_bytes, cudaMemcpyHostToDevice, st),
+                   "descriptor upload");
+        cuda_check(cudaMemsetAsync(counters, 0, (size_t)nj * kCntWords * 8, st), "counter reset");
+        cuda_check(enqueue_pipeline(a, st), "pipeline launch");
+    };
+
+    // Graph key: everything that shapes the launch sequence (sizes, plans, workspace address).
+    std::vector<int64_t> key;
+    if (use_graph) {
+        key.reserve(8 + (size_t)nj * 8);
+        key.push_back((int64_t)(uintptr_t)ws_);
+        key.push_back(nj);
+        key.push_back(a.emit_key);
+        for (int j = 0; j < nj; ++j) {
+            key.push_back(plans[j].nr);
+            key.push_back(plans[j].ns);
+            key.push_back(plans[j].pf.P1);
+            key.push_back(plans[j].pf.P2);
+            key.push_back(plans[j].bloom ? (int64_t)plans[j].seg_blocks : (int64_t)-1);
+        }
+    }
+    if (use_graph) {
+        if (!(graph_exec_ && key == graph_key_)) {
+            if (graph_exec_) {
+                cudaGraphExecDestroy(graph_exec_);
+                graph_exec_ = nullptr;
+            }
+            // Kernel attributes are set on the first direct launch, outside capture.
+            if (!have_run_) {
+                enqueue_all(stream);
+                cuda_check(cudaStreamSynchronize(stream), "warm-up run");
+            }
+            cudaStream_t cs;
+            cuda_check(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate");
+            cudaGraph_t g;
+            cuda_check(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+            set_capturing(true);
+            try {
+                enqueue_all(cs);
+            } catch (...) {
+                set_capturing(false);
+                cudaStreamEndCapture(cs, &g);
+                cudaStreamDestroy(cs);
+                throw;
+            }
+            set_capturing(false);
+            graph_kernels_ = take_capture_tally();
+            cuda_check(cudaStreamEndCapture(cs, &g), "end capture");
+            cudaStreamDestroy(cs);
+            cudaError_t e = cudaGraphInstantiate(&graph_exec_, g, 0);
+            cudaGraphDestroy(g);
+            cuda_check(e, "cudaGraphInstantiate");
+            graph_key_ = key;
+        }
+        cuda_check(cudaGraphLaunch(graph_exec_, stream), "cudaGraphLaunch");
+        note_launches((int)graph_kernels_);
+    } else {
+        enqueue_all(stream);
+    }
+    cuda_check(cudaEventRecord(stage_free_, stream), "cudaEventRecord");
+    cuda_check(cudaEventRecord(done_, stream), "cudaEventRecord");
+    have_run_ = true;
+    plans_ = plans;
+    caps_.resize(nj);
+    for (int j = 0; j < nj; ++j) caps_[j] = joins[j].out.capacity;
+    d_counters_ = counters;
+    d_gwords_ = a.gwords;
+    nj_ = nj;
+}
+
+void Engine::sync_counters(std::vector<int64_t>& counters, int64_t& errors) {
+    if (!have_run_) fail(BRIG_E_INVALID, "no run on this handle");
+    cuda_check(cudaEventSynchronize(done_), "cudaEventSynchronize");
+    counters.assign((size_t)nj_ * kCntWords, 0);
+    cuda_check(cudaMemcpy(counters.data(), d_counters_, counters.size() * 8, cudaMemcpyDeviceToHost),
+               "counter readback");
+    unsigned long long g[kGWords];
+    cuda_check(cudaMemcpy(g, d_gwords_, sizeof(g), cudaMemcpyDeviceToHost), "state readback");
+    errors = (int64_t)g[kGErrors];
+}
+
+}  // namespace brig

@@ -1,0 +1,103 @@
+// engine.h - host-side join engine: planner, workspace, pipeline enqueue, CUDA-graph cache.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "../../include/brig_join.h"
+#include "brig_common.cuh"
+#include "launch.h"
+
+namespace brig {
+
+// Thrown inside the engine; the C ABI turns it into a status code and a message.
+struct Error {
+    int status;
+    std::string msg;
+};
+[[noreturn]] void fail(int status, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what);
+
+// Fan-outs and Bloom sizing of one join (the reference's sizing heuristics,
+// src/hash_kernel.cu:188-284).
+struct JoinPlan {
+    int64_t nr = 0, ns = 0;
+    PartFn pf{};
+    int64_t nfine = 1;
+    bool bloom = false;
+    int k = 0;
+    uint32_t seg_blocks = 0;
+    int64_t bloom_bits = 0;     // allocated bits
+};
+JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns);
+
+// One join of a pipeline run, as given by the caller.
+struct JoinIO {
+    const uint32_t *rk, *rv, *sk, *sv;
+    int64_t nr, ns;
+    brig_join_output out;
+};
+
+class Engine {
+public:
+    explicit Engine(const brig_join_config& cfg);
+    ~Engine();
+
+    // Enqueues all joins on `stream` (asynchronous).
+    void run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph);
+    // Waits for the last run; copies per-join counters.
+    void sync_counters(std::vector<int64_t>& counters, int64_t& errors);
+    const std::vector<JoinPlan>& last_plans() const { return plans_; }
+    int64_t workspace_bytes() const { return (int64_t)ws_bytes_; }
+    const brig_join_config& config() const { return cfg_; }
+    int device() const { return device_; }
+    const std::vector<int64_t>& last_caps() const { return caps_; }
+    // Milliseconds of each pipeline stage in the last run (profile_stages only).
+    void stage_times(double* ms, int n);
+
+    // Device workspace needed for these joins (bytes).
+    static int64_t workspace_needed(const brig_join_config& cfg, const std::vector<JoinPlan>& plans,
+                                    int num_sms);
+
+    // Buffers owned by the engine for the host-array entry point.
+    struct HostIOBufs {
+        uint32_t *rk = nullptr, *rv = nullptr, *sk = nullptr, *sv = nullptr;
+        uint32_t *outr = nullptr, *outs = nullptr, *outk = nullptr;
+        int64_t cap_in_r = 0, cap_in_s = 0, cap_out = 0;
+        bool outk_alloc = false;
+    } hio;
+    void ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key);
+
+private:
+    void ensure_workspace(size_t bytes);
+    void ensure_staging(size_t bytes);
+
+    brig_join_config cfg_;
+    int device_ = 0;
+    int num_sms_ = 148;
+    char* ws_ = nullptr;
+    size_t ws_bytes_ = 0;
+    char* stage_ = nullptr;          // pinned staging for descriptors
+    size_t stage_bytes_ = 0;
+    cudaEvent_t stage_free_ = nullptr;  // recorded after the staging copy
+    cudaEvent_t done_ = nullptr;        // recorded after the last run
+    bool have_run_ = false;
+    std::vector<JoinPlan> plans_;
+    std::vector<int64_t> caps_;
+    int64_t* d_counters_ = nullptr;  // [nj * kCntWords] of the last run
+    unsigned long long* d_gwords_ = nullptr;
+    int nj_ = 0;
+
+    cudaEvent_t stage_ev_[kNumStages + 1] = {};
+    bool profiling_ = false;
+
+    // CUDA graph of the last pipeline shape.
+    int64_t graph_kernels_ = 0;      // kernel launches one replay performs
+    cudaGraphExec_t graph_exec_ = nullptr;
+    std::vector<int64_t> graph_key_;
+    cudaStream_t graph_stream_ = nullptr;
+};
+
+}  // namespace brig

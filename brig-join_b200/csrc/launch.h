@@ -1,0 +1,69 @@
+// launch.h - host-side launch wrappers for the sm_100a kernels (defined in kernels.cu, gen.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "brig_common.cuh"
+
+namespace brig {
+
+// Launch-time description of one pipeline run over `nj` joins. Every pointer is a device address.
+struct PipelineArgs {
+    const JoinDesc* J;            // [nj]
+    int nj;
+    const int64_t* slice_prefix[2];   // [nj+1] per relation: level-1 slices of joins before j
+    const int64_t* seg_prefix;        // [nj+1] level-1 partitions of joins with P2 > 1 (per relation
+                                      // the same count)
+    const int64_t* fine_prefix;       // [nj+1] finest partitions of joins before j
+    const int64_t* bloom_prefix;      // [nj+1] finest partitions of Bloom-enabled joins before j
+    int64_t total_slices[2];
+    int64_t total_segs;               // sum of P1 over joins with P2 > 1
+    int64_t total_fine;               // sum of P1*P2
+    int64_t total_bloom_fine;         // sum of P1*P2 over Bloom joins
+    int64_t hist_begin[2], hist_len[2];  // range of each relation in the global histogram array
+    uint32_t* hist;                   // global level-1 histogram array (both relations)
+    int64_t* hist_scan;               // exclusive scan of hist (same indexing)
+    uint32_t* tcount;                 // [total_fine + 1] tasks per finest partition
+    int64_t* toff;                    // exclusive scan of tcount
+    Task* tasks;                      // task list
+    int64_t task_cap;
+    int64_t* scan_tmp;                // block sums for the device-wide scan
+    int64_t scan_tmp_len;
+    unsigned long long* gwords;       // [kGWords]
+    int max_p1, max_p2;               // over the batch (shared-memory sizing)
+    int max_seg_words;                // largest Bloom segment (words)
+    int table_cap;                    // probe table capacity (tuples)
+    int emit_key;
+    int any_bloom;
+    int num_sms;
+    cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
+};
+
+constexpr int kNumStages = 11;
+const char* stage_name(int i);
+
+// Enqueues the full join pipeline (partition, Bloom, tasks, probe) for all joins on `stream`.
+cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t stream);
+
+// Shared memory the probe kernel needs for a table of `table_cap` tuples.
+size_t probe_smem_bytes(int table_cap, int emit_key);
+
+// Device-wide exclusive scan of n uint32 counts into int64 offsets; writes the sum to *total
+// (device pointer, may be null). tmp must hold scan_tmp_words(n) int64.
+int64_t scan_tmp_words(int64_t n);
+cudaError_t enqueue_scan(const uint32_t* in, int64_t* out, int64_t n, int64_t* tmp,
+                         int64_t* total, cudaStream_t stream);
+
+// Input generator (gen.cu).
+cudaError_t enqueue_gen(uint64_t seed, int64_t n_r, int64_t n_s, double match_frac, double zipf_s,
+                        uint32_t* r_key, uint32_t* r_val, uint32_t* s_key, uint32_t* s_val,
+                        cudaStream_t stream);
+
+// Count of kernel launches issued by this library on the calling thread. Launches enqueued while a
+// stream is being captured are not counted; each replay of a graph adds the kernels it holds.
+void note_launches(int n);
+int64_t launches_so_far();
+void set_capturing(bool on);   // while on, note_launches adds to the capture tally instead
+int64_t take_capture_tally();  // kernels noted since set_capturing(true)
+
+}  // namespace brig

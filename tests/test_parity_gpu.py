@@ -1,0 +1,142 @@
+"""Parity of the CUDA join path with the CPU oracle: exact match count and identical sorted
+multiset of (r_val, s_val) pairs, on seeded inputs, through the C ABI."""
+import numpy as np
+import pytest
+
+from gpu_helpers import assert_same_pairs, run_device
+
+pytestmark = pytest.mark.gpu
+
+
+def _parity(bj, oracle, torch, rk, rv, sk, sv, cap=None, **cfg):
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    st, r, s, _ = run_device(bj, torch, rk, rv, sk, sv, cap=cap if cap is not None else max(len(exp_r), 1), **cfg)
+    assert st.count == len(exp_r)
+    assert_same_pairs(oracle, r, s, exp_r, exp_s)
+    return st
+
+
+@pytest.mark.parametrize("bloom", [0, 1])
+@pytest.mark.parametrize("n", [1000, 100_000, 1 << 20])
+def test_uniform_hash(bj, oracle, torch_cuda, n, bloom):
+    rk, rv, sk, sv = bj.gen_host(7 + n, n, n, 0.1)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=bloom)
+    assert st.count == n // 10
+    if bloom:
+        assert st.count <= st.s_survivors < n
+
+
+@pytest.mark.parametrize("p1,p2", [(16, 16), (64, 8), (1, 1), (4096, 1), (2, 1024)])
+def test_two_level_hash_fanouts(bj, oracle, torch_cuda, p1, p2):
+    rk, rv, sk, sv = bj.gen_host(11, 300_000, 200_000, 0.3)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, partition_size=p1, second_partition_size=p2)
+    assert (st.partition_size, st.second_partition_size) == (p1, p2)
+
+
+@pytest.mark.parametrize("p1,p2", [(512, 0), (512, 67), (100, 3), (7, 1)])
+@pytest.mark.parametrize("bloom", [0, 1])
+def test_modulo_mode(bj, oracle, torch_cuda, p1, p2, bloom):
+    rk, rv, sk, sv = bj.gen_host(13, 200_000, 250_000, 0.1)
+    _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, partition_mode=bj.PART_MODULO, partition_size=p1,
+            second_partition_size=p2, use_bloom=bloom)
+
+
+@pytest.mark.parametrize("table", [256, 1024, 8192])
+def test_duplicates_and_split_path(bj, oracle, torch_cuda, table):
+    rng = np.random.default_rng(table)
+    rk = rng.integers(0, 300, 20_000, dtype=np.uint32)     # heavy duplicates in R
+    sk = rng.integers(0, 600, 5_000, dtype=np.uint32)
+    rv = np.arange(len(rk), dtype=np.uint32)
+    sv = np.arange(len(sk), dtype=np.uint32) + 7
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, table_capacity=table, partition_size=2,
+                 second_partition_size=1)
+    if table == 256:
+        assert st.split_tasks > 0
+
+
+def test_single_hot_key(bj, oracle, torch_cuda):
+    rk = np.full(3000, 0xDEADBEEF, np.uint32)
+    sk = np.concatenate([np.full(700, 0xDEADBEEF, np.uint32), np.arange(100, dtype=np.uint32)])
+    rv = np.arange(len(rk), dtype=np.uint32)
+    sv = np.arange(len(sk), dtype=np.uint32)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, table_capacity=1024)
+    assert st.count == 3000 * 700 and st.split_tasks > 0
+
+
+@pytest.mark.parametrize("bloom", [0, 1])
+def test_edge_keys_full_domain(bj, oracle, torch_cuda, bloom):
+    edge = np.array([0, 1, 0x7FFFFFFF, 0x80000000, 0x80000001, 0xFFFFFFFE, 0xFFFFFFFF], np.uint32)
+    rng = np.random.default_rng(5)
+    rk = np.concatenate([edge, edge, rng.integers(0, 2**32, 5000, dtype=np.uint64).astype(np.uint32)])
+    sk = np.concatenate([edge, rng.permutation(rk)[:3000], rng.integers(0, 2**32, 3000, dtype=np.uint64).astype(np.uint32)])
+    rv = rng.integers(0, 2**32, len(rk), dtype=np.uint64).astype(np.uint32)
+    sv = rng.integers(0, 2**32, len(sk), dtype=np.uint64).astype(np.uint32)
+    _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=bloom)
+
+
+@pytest.mark.parametrize("nr,ns", [(0, 100), (100, 0), (0, 0), (1, 1)])
+def test_empty_and_tiny(bj, oracle, torch_cuda, nr, ns):
+    rk = np.arange(nr, dtype=np.uint32)
+    sk = np.arange(ns, dtype=np.uint32)
+    st = _parity(bj, oracle, torch_cuda, rk, rk.copy(), sk, sk.copy(), use_bloom=1)
+    assert st.count == min(nr, ns)
+
+
+def test_ragged_unaligned_inputs(bj, oracle, torch_cuda):
+    rk, rv, sk, sv = bj.gen_host(21, 99_999, 77_777, 0.5)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    st, r, s, _ = run_device(bj, torch_cuda, rk, rv, sk, sv, cap=len(exp_r), offset=1, use_bloom=1)
+    assert st.count == len(exp_r)
+    assert_same_pairs(oracle, r, s, exp_r, exp_s)
+
+
+def test_capacity_overflow_counts_exactly(bj, oracle, torch_cuda):
+    rk, rv, sk, sv = bj.gen_host(3, 50_000, 50_000, 0.4)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    cap = len(exp_r) // 3
+    st, r, s, _ = run_device(bj, torch_cuda, rk, rv, sk, sv, cap=cap)
+    assert st.count == len(exp_r) and st.overflow == 1 and st.written == cap and len(r) == cap
+    exp = set(zip(exp_r.tolist(), exp_s.tolist()))
+    got = list(zip(r.tolist(), s.tolist()))
+    assert len(set(got)) == cap and all(p in exp for p in got)
+
+
+def test_emit_key(bj, oracle, torch_cuda):
+    rk, rv, sk, sv = bj.gen_host(4, 30_000, 40_000, 0.2)
+    st, r, s, k = run_device(bj, torch_cuda, rk, rv, sk, sv, emit_key=True)
+    assert np.array_equal(k, rk[r]) and np.array_equal(k, sk[s])
+
+
+def test_zipf_skewed_probe_side(bj, oracle, torch_cuda):
+    rk, rv, sk, sv = bj.gen_host(99, 200_000, 800_000, 0.1, zipf_s=1.0)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=1, s_chunk=4096)
+    assert st.count == 80_000
+
+
+def test_handle_reuse_and_graph_replay(bj, oracle, torch_cuda):
+    with bj.Join(use_bloom=1, use_cuda_graph=1) as j:
+        for seed in (1, 2, 3):
+            rk, rv, sk, sv = bj.gen_host(seed, 120_000, 90_000, 0.25)
+            exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+            st, r, s, _ = run_device(bj, torch_cuda, rk, rv, sk, sv, cap=len(exp_r) + 10, handle=j)
+            assert st.count == len(exp_r)
+            assert_same_pairs(oracle, r, s, exp_r, exp_s)
+
+
+def test_run_host_entry_point(bj, oracle):
+    rk, rv, sk, sv = bj.gen_host(8, 70_000, 60_000, 0.3)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    with bj.Join(use_bloom=1) as j:
+        cnt, r, s = j.run_host(rk, rv, sk, sv, capacity=len(exp_r))
+    assert cnt == len(exp_r)
+    assert_same_pairs(oracle, r, s, exp_r, exp_s)
+
+
+def test_device_generator_matches_host(bj, torch_cuda):
+    n_r, n_s = 300_001, 500_003
+    h = bj.gen_host(1234, n_r, n_s, 0.37)
+    d = [torch_cuda.empty(n, dtype=torch_cuda.int32, device="cuda") for n in (n_r, n_r, n_s, n_s)]
+    bj.gen_device(1234, n_r, n_s, 0.37, 0.0, *d)
+    torch_cuda.cuda.synchronize()
+    for a, b in zip(h, d):
+        assert np.array_equal(a, b.cpu().numpy().view(np.uint32))
