@@ -317,6 +317,52 @@ class Join:
         return c
 
 
+class Server:
+    """Served joins (brig_serve_*): submit host-array requests, poll tickets."""
+
+    def __init__(self, hbm_budget_bytes=0, max_wave=0, streams=0, max_queue=0, **join_cfg):
+        self.cfg = make_config(**join_cfg)
+        self.scfg = ServeConfig(hbm_budget_bytes, max_wave, streams, max_queue)
+        h = C.c_void_p()
+        check(lib().brig_serve_create(C.byref(self.cfg), C.byref(self.scfg), C.byref(h)), "brig_serve_create")
+        self.h = h
+        self._keep = {}
+
+    def submit(self, r_key, r_val, s_key, s_val, capacity=0, out=None, on_device=False) -> int:
+        """Queues a join; host arrays (numpy) unless on_device. Returns the ticket."""
+        if out is None and not on_device:
+            cap = capacity if capacity > 0 else max(len(s_key), 1)
+            out = (np.empty(cap, np.uint32), np.empty(cap, np.uint32))
+        n_r = r_key.numel() if hasattr(r_key, "numel") else len(r_key)
+        n_s = s_key.numel() if hasattr(s_key, "numel") else len(s_key)
+        req = ServeRequest(_ptr(r_key), _ptr(r_val), n_r, _ptr(s_key), _ptr(s_val), n_s, 1 if on_device else 0, 0,
+                           _ptr(out[0]) if out else None, _ptr(out[1]) if out else None, capacity)
+        t = C.c_int64()
+        check(lib().brig_serve_submit(self.h, C.byref(req), C.byref(t)), "brig_serve_submit")
+        self._keep[t.value] = (r_key, r_val, s_key, s_val, out)
+        return t.value
+
+    def poll(self, ticket: int, timeout_ms: int = -1):
+        """(result, r_vals, s_vals) once the ticket is done; raises BrigError(BRIG_E_NOT_READY) on timeout."""
+        res = ServeResult()
+        check(lib().brig_serve_poll(self.h, ticket, timeout_ms, C.byref(res)), "brig_serve_poll")
+        keep = self._keep.pop(ticket)
+        out = keep[4]
+        n = min(res.count, len(out[0])) if out else 0
+        return res, (out[0][:n] if out else None), (out[1][:n] if out else None)
+
+    def close(self):
+        if self.h:
+            lib().brig_serve_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 def gen_host(seed: int, n_r: int, n_s: int, match_frac: float = 0.1, zipf_s: float = 0.0):
     """Synthetic inputs on the host: (r_key, r_val, s_key, s_val) uint32 arrays."""
     rk = np.empty(n_r, np.uint32)

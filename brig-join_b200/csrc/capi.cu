@@ -298,7 +298,7 @@ const char* brig_join_stage_name(int32_t i) { return brig::stage_name(i); }
 int brig_join_stage_times(brig_join_t* h, double* ms, int32_t n) {
     return guarded([&] {
         if (!h || !ms || n < 0) fail(BRIG_E_INVALID, "bad arguments");
-        h->eng->stage_times(ms, n);
+        if (h->eng->stage_times(ms, n) == 0) fail(BRIG_E_INVALID, "no profiled run since the last call");
         return (int)BRIG_OK;
     });
 }

@@ -231,20 +231,31 @@ Engine::Engine(const brig_join_config& cfg) : cfg_(cfg) {
     cuda_check(cudaEventCreateWithFlags(&stage_free_, cudaEventDisableTiming), "cudaEventCreate");
     cuda_check(cudaEventCreateWithFlags(&done_, cudaEventDisableTiming), "cudaEventCreate");
     if (cfg.profile_stages) {
-        for (auto& e : stage_ev_) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
+        for (auto& set : stage_ev_)
+            for (auto& e : set) cuda_check(cudaEventCreate(&e), "cudaEventCreate");
         profiling_ = true;
     }
 }
 
-void Engine::stage_times(double* ms, int n) {
+int Engine::stage_times(double* ms, int n) {
     if (!profiling_) fail(BRIG_E_INVALID, "handle created without profile_stages");
     if (!have_run_) fail(BRIG_E_INVALID, "no run on this handle");
     cuda_check(cudaEventSynchronize(done_), "cudaEventSynchronize");
-    for (int i = 0; i < n && i < kNumStages; ++i) {
-        float t = 0.f;
-        cuda_check(cudaEventElapsedTime(&t, stage_ev_[i], stage_ev_[i + 1]), "cudaEventElapsedTime");
-        ms[i] = t;
+    const int64_t first = std::max(runs_read_, runs_recorded_ - kStageRing);
+    const int runs = (int)(runs_recorded_ - first);
+    for (int i = 0; i < n && i < kNumStages; ++i) ms[i] = 0.0;
+    for (int64_t r = first; r < runs_recorded_; ++r) {
+        cudaEvent_t* ev = stage_ev_[r % kStageRing];
+        for (int i = 0; i < n && i < kNumStages; ++i) {
+            float t = 0.f;
+            cuda_check(cudaEventElapsedTime(&t, ev[i], ev[i + 1]), "cudaEventElapsedTime");
+            ms[i] += t;
+        }
     }
+    if (runs > 0)
+        for (int i = 0; i < n && i < kNumStages; ++i) ms[i] /= runs;
+    runs_read_ = runs_recorded_;
+    return runs;
 }
 
 Engine::~Engine() {
@@ -259,8 +270,9 @@ Engine::~Engine() {
     if (hio.outr) cudaFree(hio.outr);
     if (hio.outs) cudaFree(hio.outs);
     if (hio.outk) cudaFree(hio.outk);
-    for (auto& e : stage_ev_)
-        if (e) cudaEventDestroy(e);
+    for (auto& set : stage_ev_)
+        for (auto& e : set)
+            if (e) cudaEventDestroy(e);
     if (stage_free_) cudaEventDestroy(stage_free_);
     if (done_) cudaEventDestroy(done_);
 }
@@ -439,11 +451,17 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
         if (io.out.key) a.emit_key = 1;
     a.any_bloom = sh.any_bloom ? 1 : 0;
     a.num_sms = num_sms_;
-    a.stage_events = profiling_ ? stage_ev_ : nullptr;
+    // Stage events are plain stream records, so a profiled handle launches directly (a record
+    // captured into a graph is only a dependency edge, not a timestamp).
+    if (profiling_) use_graph = false;
+    a.stage_events = profiling_ ? stage_ev_[runs_recorded_ % kStageRing] : nullptr;
 
     auto enqueue_all = [&](cudaStream_t st) {
         cuda_check(cudaMemcpyAsync(meta, stage_, sh.meta_bytes, cudaMemcpyHostToDevice, st),
                    "descriptor upload");
+        // Outside capture the staging buffer is free once this copy has run, so the next run's
+        // host work overlaps this run's kernels.
+        if (!use_graph) cuda_check(cudaEventRecord(stage_free_, st), "cudaEventRecord");
         cuda_check(cudaMemsetAsync(counters, 0, (size_t)nj * kCntWords * 8, st), "counter reset");
         cuda_check(enqueue_pipeline(a, st), "pipeline launch");
     };
@@ -501,9 +519,10 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
     } else {
         enqueue_all(stream);
     }
-    cuda_check(cudaEventRecord(stage_free_, stream), "cudaEventRecord");
+    if (use_graph) cuda_check(cudaEventRecord(stage_free_, stream), "cudaEventRecord");
     cuda_check(cudaEventRecord(done_, stream), "cudaEventRecord");
     have_run_ = true;
+    if (profiling_) ++runs_recorded_;
     plans_ = plans;
     caps_.resize(nj);
     for (int j = 0; j < nj; ++j) caps_[j] = joins[j].out.capacity;

@@ -54,8 +54,9 @@ public:
     const brig_join_config& config() const { return cfg_; }
     int device() const { return device_; }
     const std::vector<int64_t>& last_caps() const { return caps_; }
-    // Milliseconds of each pipeline stage in the last run (profile_stages only).
-    void stage_times(double* ms, int n);
+    // Mean milliseconds of each pipeline stage over the runs since the previous call (at most the
+    // last kStageRing); returns the number of runs averaged (profile_stages only).
+    int stage_times(double* ms, int n);
 
     // Device workspace needed for these joins (bytes).
     static int64_t workspace_needed(const brig_join_config& cfg, const std::vector<JoinPlan>& plans,
@@ -90,7 +91,10 @@ private:
     unsigned long long* d_gwords_ = nullptr;
     int nj_ = 0;
 
-    cudaEvent_t stage_ev_[kNumStages + 1] = {};
+    // Stage events of the last kStageRing runs (profile_stages): run i records into set i % ring.
+    static constexpr int kStageRing = 64;
+    cudaEvent_t stage_ev_[kStageRing][kNumStages + 1] = {};
+    int64_t runs_recorded_ = 0, runs_read_ = 0;
     bool profiling_ = false;
 
     // CUDA graph of the last pipeline shape.

@@ -152,9 +152,12 @@ int brig_join_get_stats(brig_join_t* h, brig_join_stats* st);
 /* Name of stage i ("r_hist", "r_scan", "r_scatter", "r_level2", "bloom_build", "s_hist_probe",
  * "s_scan", "s_scatter", "s_level2", "tasks", "probe"), or NULL. */
 const char* brig_join_stage_name(int32_t i);
-/* Waits for the last run and writes the device time of each stage in milliseconds into
- * ms[BRIG_NUM_STAGES] (the reference's per-stage timing table, src/hash_kernel.cu:1182-1358).
- * BRIG_E_INVALID if the handle was created without profile_stages. */
+/* Waits for the last run and writes the mean device time of each stage in milliseconds, over
+ * the runs since the previous call (at most the last 64), into ms[BRIG_NUM_STAGES] (the
+ * reference's per-stage timing table, src/hash_kernel.cu:1182-1358). Reading needs no
+ * synchronisation between runs. A profiled handle launches its kernels directly instead of
+ * replaying a CUDA graph. BRIG_E_INVALID if the handle was created without profile_stages or
+ * no run happened since the previous call. */
 int brig_join_stage_times(brig_join_t* h, double* ms, int32_t n);
 
 /* Device workspace the engine needs for one join of this shape (the reference's allocation plan,

@@ -1,0 +1,115 @@
+"""C-ABI checks that need no GPU: the library loads and exports every declared function, the
+planner's fan-outs, argument validation, error reporting without a device, and the host generator."""
+import ctypes as C
+import subprocess
+
+import numpy as np
+import pytest
+
+
+def test_exports_every_declared_symbol(bj):
+    names = bj.header_functions()
+    assert len(names) >= 15
+    lib = bj.lib()
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", bj.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    assert set(names) <= exported
+
+
+def test_config_defaults(bj):
+    cfg = bj.make_config()
+    assert cfg.abi_version == bj.ABI_VERSION
+    assert cfg.partition_mode == bj.PART_HASH
+    assert cfg.bloom_bits_per_key == 10.0 and cfg.use_bloom == 0 and cfg.device == -1
+    assert C.sizeof(bj.Config) == 88
+
+
+@pytest.mark.parametrize("n_r,n_s,kw,expect", [
+    (1 << 24, 1 << 24, {}, (4096, 1)),
+    (640_000_000, 640_000_000, {"use_bloom": 1}, (2048, 64)),
+    (1 << 26, 1 << 30, {"use_bloom": 1}, (2048, 8)),
+    (1 << 24, 1 << 24, {"partition_mode": 1, "partition_size": 512}, (512, 67)),
+    (640_000_000, 640_000_000, {"partition_mode": 1, "partition_size": 512}, (512, 205)),
+    (4096, 16384, {}, (1, 1)),
+    (0, 0, {}, (1, 1)),
+])
+def test_planner_fanouts(bj, n_r, n_s, kw, expect):
+    p1, p2, ws = bj.plan(n_r, n_s, **kw)
+    assert (p1, p2) == expect
+    assert ws >= 8 * (n_r + n_s)
+
+
+def test_planner_rejects_bad_configs(bj):
+    with pytest.raises(bj.BrigError) as e:
+        bj.plan(1000, 1000, partition_size=3)
+    assert e.value.status == bj.BRIG_E_INVALID
+    with pytest.raises(bj.BrigError) as e:
+        bj.plan(1000, 1000, partition_mode=1, partition_size=5000)
+    assert e.value.status == bj.BRIG_E_INVALID
+    with pytest.raises(bj.BrigError) as e:
+        bj.plan(1 << 33, 1000, partition_mode=1, partition_size=2)
+    assert e.value.status == bj.BRIG_E_UNSUPPORTED
+    with pytest.raises(bj.BrigError) as e:
+        bj.plan(-1, 10)
+    assert e.value.status == bj.BRIG_E_INVALID
+    cfg = bj.make_config()
+    cfg.abi_version = 99
+    assert bj.lib().brig_join_plan(C.byref(cfg), 10, 10, None, None, None) == bj.BRIG_E_INVALID
+    assert "ABI" in bj.last_error()
+
+
+def test_create_reports_missing_device(bj):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    cfg = bj.make_config()
+    st = bj.lib().brig_join_create(C.byref(cfg), C.byref(h))
+    assert st == bj.BRIG_E_CUDA and not h.value
+    assert bj.last_error()
+
+
+def test_null_arguments_rejected(bj):
+    assert bj.lib().brig_join_run(None, None, None, 0, None, None, 0, None, None) == bj.BRIG_E_INVALID
+    assert bj.lib().brig_join_get_stats(None, None) == bj.BRIG_E_INVALID
+    assert bj.lib().brig_join_destroy(None) == bj.BRIG_OK
+    assert bj.lib().brig_join_stage_name(0) == b"r_hist"
+    assert bj.lib().brig_join_stage_name(10) == b"probe"
+    assert bj.lib().brig_join_stage_name(11) is None
+
+
+def test_generator_properties(bj):
+    nr, ns, frac = 200_000, 300_000, 0.1
+    rk, rv, sk, sv = bj.gen_host(5, nr, ns, frac)
+    assert np.array_equal(rv, np.arange(nr)) and np.array_equal(sv, np.arange(ns))
+    assert len(np.unique(rk)) == nr and rk.min() >= 1 and rk.max() < 2**31
+    match = sk < 2**31
+    assert match.sum() == int(frac * ns)
+    assert np.isin(sk[match], rk).all()
+    nm = sk[~match]
+    assert nm.min() >= 2**31 and nm.max() < 2**32 - 1 and len(np.unique(nm)) == len(nm)
+    again = bj.gen_host(5, nr, ns, frac)
+    assert all(np.array_equal(a, b) for a, b in zip((rk, rv, sk, sv), again))
+    other = bj.gen_host(6, nr, ns, frac)
+    assert not np.array_equal(rk, other[0])
+
+
+def test_generator_zipf_skew(bj):
+    nr, ns = 100_000, 400_000
+    rk, _, sk, _ = bj.gen_host(9, nr, ns, 0.1, zipf_s=1.0)
+    m = sk[sk < 2**31]
+    assert len(m) == 40_000
+    pos = {k: i for i, k in enumerate(rk.tolist())}
+    ranks = np.array([pos[k] for k in m.tolist()])
+    # Zipf(1) over 100k ranks: rank 1 has probability 1/H(n) ~ 8%, the top 10 ranks ~ 24%
+    assert 0.06 < (ranks == 0).mean() < 0.11
+    assert 0.18 < (ranks < 10).mean() < 0.30
+
+
+def test_generator_rejects_bad_arguments(bj):
+    L = bj.lib()
+    assert L.brig_gen_host(1, -5, 10, 0.1, 0.0, None, None, None, None) == bj.BRIG_E_INVALID
+    assert L.brig_gen_host(1, 10, 10, 1.5, 0.0, None, None, None, None) == bj.BRIG_E_INVALID
+    assert L.brig_gen_host(1, 1 << 31, 10, 0.1, 0.0, None, None, None, None) == bj.BRIG_E_UNSUPPORTED

@@ -1,0 +1,86 @@
+"""Served joins: continuous batching under an HBM budget returns exactly the oracle result for every
+request, and a request's result is the same alone and in a mix of concurrent requests."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from gpu_helpers import assert_same_pairs
+
+pytestmark = pytest.mark.gpu
+
+
+def _req(bj, seed, nr, ratio, frac):
+    return bj.gen_host(seed, nr, nr * ratio, frac)
+
+
+def test_every_request_matches_oracle(bj, oracle, torch_cuda):
+    rng = np.random.default_rng(1)
+    reqs = [_req(bj, 1000 + i, int(rng.integers(1, 200_000)), int(rng.choice([1, 4, 16])),
+                 float(rng.choice([0.01, 0.1, 0.5]))) for i in range(40)]
+    with bj.Server(hbm_budget_bytes=2 << 30, max_wave=8, streams=2, use_bloom=1) as srv:
+        tickets = [srv.submit(*r) for r in reqs]
+        waves = set()
+        for t, r in zip(tickets, reqs):
+            res, a, b = srv.poll(t)
+            assert res.status == bj.BRIG_OK
+            er, es = oracle.pairs(*r)
+            assert res.count == len(er)
+            assert_same_pairs(oracle, a, b, er, es)
+            waves.add(res.wave)
+    assert len(waves) > 1
+
+
+def test_same_result_alone_and_in_mix(bj, oracle, torch_cuda):
+    x = _req(bj, 77, 150_000, 4, 0.5)
+    er, es = oracle.pairs(*x)
+    with bj.Server(hbm_budget_bytes=4 << 30, max_wave=16, streams=3, use_bloom=1) as srv:
+        res, a, b = srv.poll(srv.submit(*x))
+        assert res.count == len(er)
+        assert_same_pairs(oracle, a, b, er, es)
+        # the same request again, arriving while a stream of other requests is being served
+        others = [_req(bj, 200 + i, 50_000 + 7000 * i, 4, 0.1) for i in range(24)]
+        stop = threading.Event()
+        tix = []
+
+        def feeder():
+            for r in others:
+                tix.append((srv.submit(*r), r))
+                time.sleep(0.002)
+        th = threading.Thread(target=feeder)
+        th.start()
+        time.sleep(0.01)
+        t = srv.submit(*x)
+        th.join()
+        res2, a2, b2 = srv.poll(t)
+        assert res2.count == len(er)
+        assert_same_pairs(oracle, a2, b2, er, es)
+        for tk, r in tix:
+            resk, ak, bk = srv.poll(tk)
+            ork, osk = oracle.pairs(*r)
+            assert resk.count == len(ork)
+            assert_same_pairs(oracle, ak, bk, ork, osk)
+
+
+def test_admission_rejects_oversized_and_drains_under_tight_budget(bj, oracle, torch_cuda):
+    big = _req(bj, 5, 2_000_000, 1, 0.1)
+    small = [_req(bj, 50 + i, 100_000, 4, 0.1) for i in range(6)]
+    with bj.Server(hbm_budget_bytes=64 << 20, max_wave=4, streams=2) as srv:
+        with pytest.raises(bj.BrigError) as e:
+            srv.submit(*big)
+        assert e.value.status == bj.BRIG_E_REJECTED
+        tix = [srv.submit(*r) for r in small]
+        for t, r in zip(tix, small):
+            res, a, b = srv.poll(t)
+            assert res.status == bj.BRIG_OK and res.count == 40_000
+
+
+def test_poll_timeout_and_unknown_ticket(bj, torch_cuda):
+    with bj.Server(hbm_budget_bytes=1 << 30) as srv:
+        with pytest.raises(bj.BrigError) as e:
+            srv.poll(12345, 0)
+        assert e.value.status == bj.BRIG_E_INVALID
+        t = srv.submit(*_req(bj, 3, 10_000, 1, 0.1))
+        res, _, _ = srv.poll(t, 10_000)
+        assert res.status == bj.BRIG_OK
