@@ -43,6 +43,7 @@ PART_HASH = 0
 PART_MODULO = 1
 ABI_VERSION = 1
 NUM_STAGES = 11
+NOALLOC_MAX_TUPLES = 262144
 
 _u32p = C.POINTER(C.c_uint32)
 _i64p = C.POINTER(C.c_int64)
@@ -172,6 +173,8 @@ def lib() -> C.CDLL:
     L.brig_join_stage_name.argtypes = [C.c_int32]
     L.brig_join_stage_name.restype = C.c_char_p
     L.brig_join_stage_times.argtypes = [vp, C.POINTER(C.c_double), C.c_int32]
+    L.brig_join_run_noalloc.argtypes = [C.POINTER(Config), vp, vp, C.c_int64, vp, vp, C.c_int64,
+                                        C.POINTER(Output), vp]
     L.brig_join_last_error.argtypes = []
     L.brig_join_last_error.restype = C.c_char_p
     L.brig_join_kernel_launches.argtypes = []

@@ -68,6 +68,10 @@ void check_out(const brig_join_output* out) {
 
 }  // namespace
 
+namespace brig {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace brig
+
 extern "C" {
 
 void brig_join_config_init(brig_join_config* cfg) {

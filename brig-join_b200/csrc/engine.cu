@@ -111,39 +111,15 @@ struct Layout {
     }
 };
 
-struct RelOffs {
-    size_t l1 = 0, l2 = 0, cmp = 0, b1 = 0, bounds = 0, slice_cnt = 0;
-    int64_t slice_len = 0;
-    int32_t nslices = 0;
-    int64_t hist_base = 0;
-};
-struct JoinOffs {
-    RelOffs rel[2];
-    size_t bloom = 0;
-};
+}  // namespace
 
-struct Shape {
-    std::vector<JoinOffs> jo;
-    int64_t slice_len = 0;
-    int64_t hist_len[2] = {0, 0};
-    int64_t total_slices[2] = {0, 0};
-    int64_t total_segs = 0, total_fine = 0, total_bloom_fine = 0;
-    int64_t task_cap = 0;
-    size_t hist = 0, hist_scan = 0, tcount = 0, toff = 0, tasks = 0, scan_tmp = 0, gwords = 0,
-           counters = 0, meta = 0;
-    int64_t scan_tmp_len = 0;
-    size_t meta_bytes = 0;
-    size_t total = 0;
-    int max_p1 = 1, max_p2 = 1, max_seg_words = 0;
-    bool any_bloom = false;
-};
-
-Shape layout_for(const brig_join_config& cfg, const std::vector<JoinPlan>& plans, int num_sms) {
-    Shape sh;
-    const int nj = (int)plans.size();
-    sh.jo.resize(nj);
+void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int num_sms, JoinOffs* jo,
+                Shape& sh) {
+    sh = Shape{};
+    sh.jo = jo;
+    for (int j = 0; j < nj; ++j) jo[j] = JoinOffs{};
     int64_t total_tuples = 0;
-    for (const auto& p : plans) total_tuples += p.nr + p.ns;
+    for (int j = 0; j < nj; ++j) total_tuples += plans[j].nr + plans[j].ns;
     // Slices of about total/(8 * SMs) tuples, a multiple of the scatter tile, at least 4 tiles.
     const int64_t target = (int64_t)num_sms * 8;
     int64_t sl = (total_tuples + target - 1) / std::max<int64_t>(target, 1);
@@ -209,14 +185,14 @@ Shape layout_for(const brig_join_config& cfg, const std::vector<JoinPlan>& plans
     sh.meta_bytes = (size_t)nj * sizeof(JoinDesc) + 5 * ((size_t)nj + 1) * 8;
     sh.meta = L.take(sh.meta_bytes);
     sh.total = L.off + 256;
-    return sh;
 }
-
-}  // namespace
 
 int64_t Engine::workspace_needed(const brig_join_config& cfg, const std::vector<JoinPlan>& plans,
                                  int num_sms) {
-    return (int64_t)layout_for(cfg, plans, num_sms).total;
+    std::vector<JoinOffs> jo(plans.size());
+    Shape sh;
+    layout_for(cfg, plans.data(), (int)plans.size(), num_sms, jo.data(), sh);
+    return (int64_t)sh.total;
 }
 
 Engine::Engine(const brig_join_config& cfg) : cfg_(cfg) {
@@ -341,26 +317,15 @@ void Engine::ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key) {
     hio.cap_out = std::max(hio.cap_out, cap);
 }
 
-void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph) {
-    const int nj = (int)joins.size();
-    if (nj <= 0) fail(BRIG_E_INVALID, "no joins");
-    std::vector<JoinPlan> plans(nj);
-    for (int j = 0; j < nj; ++j) plans[j] = plan_join(cfg_, joins[j].nr, joins[j].ns);
-    const Shape sh = layout_for(cfg_, plans, num_sms_);
-    const int T = cfg_.table_capacity > 0 ? cfg_.table_capacity : kMaxTable;
-    const int C = cfg_.s_chunk > 0 ? cfg_.s_chunk : 16384;
+void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const JoinIO* joins, int nj,
+                   const Shape& sh, char* ws, char* meta_host, int num_sms, PipelineArgs& a) {
+    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kMaxTable;
+    const int C = cfg.s_chunk > 0 ? cfg.s_chunk : 16384;
     if (T < kMinTable || T > kMaxTable || !is_pow2(T))
         fail(BRIG_E_INVALID, "table_capacity must be a power of two in [256, 8192]");
     if (C < 1) fail(BRIG_E_INVALID, "s_chunk must be >= 1");
-
-    ensure_workspace(sh.total);
-    ensure_staging(sh.meta_bytes);
-    // The staging buffer may still be read by the previous run's copy.
-    if (have_run_) cuda_check(cudaEventSynchronize(stage_free_), "cudaEventSynchronize");
-
-    char* ws = ws_;
-    JoinDesc* hJ = reinterpret_cast<JoinDesc*>(stage_);
-    int64_t* hpre = reinterpret_cast<int64_t*>(stage_ + (size_t)nj * sizeof(JoinDesc));
+    JoinDesc* hJ = reinterpret_cast<JoinDesc*>(meta_host);
+    int64_t* hpre = reinterpret_cast<int64_t*>(meta_host + (size_t)nj * sizeof(JoinDesc));
     int64_t* sp0 = hpre;
     int64_t* sp1 = hpre + (nj + 1);
     int64_t* segp = hpre + 2 * (nj + 1);
@@ -415,8 +380,7 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
     }
     char* meta = ws + sh.meta;
     const int64_t* dpre = reinterpret_cast<const int64_t*>(meta + (size_t)nj * sizeof(JoinDesc));
-
-    PipelineArgs a{};
+    a = PipelineArgs{};
     a.J = reinterpret_cast<const JoinDesc*>(meta);
     a.nj = nj;
     a.slice_prefix[0] = dpre;
@@ -447,10 +411,31 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
     a.max_seg_words = sh.max_seg_words;
     a.table_cap = T;
     a.emit_key = 0;
-    for (const auto& io : joins)
-        if (io.out.key) a.emit_key = 1;
+    for (int j = 0; j < nj; ++j)
+        if (joins[j].out.key) a.emit_key = 1;
     a.any_bloom = sh.any_bloom ? 1 : 0;
-    a.num_sms = num_sms_;
+    a.num_sms = num_sms;
+    a.stage_events = nullptr;
+}
+
+void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph) {
+    const int nj = (int)joins.size();
+    if (nj <= 0) fail(BRIG_E_INVALID, "no joins");
+    std::vector<JoinPlan> plans(nj);
+    for (int j = 0; j < nj; ++j) plans[j] = plan_join(cfg_, joins[j].nr, joins[j].ns);
+    std::vector<JoinOffs> jo(nj);
+    Shape sh;
+    layout_for(cfg_, plans.data(), nj, num_sms_, jo.data(), sh);
+    ensure_workspace(sh.total);
+    ensure_staging(sh.meta_bytes);
+    // The staging buffer may still be read by the previous run's copy.
+    if (have_run_) cuda_check(cudaEventSynchronize(stage_free_), "cudaEventSynchronize");
+
+    char* ws = ws_;
+    PipelineArgs a{};
+    fill_pipeline(cfg_, plans.data(), joins.data(), nj, sh, ws, stage_, num_sms_, a);
+    char* meta = ws + sh.meta;
+    int64_t* counters = reinterpret_cast<int64_t*>(ws + sh.counters);
     // Stage events are plain stream records, so a profiled handle launches directly (a record
     // captured into a graph is only a dependency edge, not a timestamp).
     if (profiling_) use_graph = false;

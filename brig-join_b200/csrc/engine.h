@@ -18,6 +18,8 @@ struct Error {
     std::string msg;
 };
 [[noreturn]] void fail(int status, const std::string& msg);
+// Message returned by brig_join_last_error() on the calling thread.
+void set_last_error(const std::string& msg);
 void cuda_check(cudaError_t e, const char* what);
 
 // Fan-outs and Bloom sizing of one join (the reference's sizing heuristics,
@@ -39,6 +41,44 @@ struct JoinIO {
     int64_t nr, ns;
     brig_join_output out;
 };
+
+// Byte offsets of one relation's buffers inside a pipeline workspace.
+struct RelOffs {
+    size_t l1 = 0, l2 = 0, cmp = 0, b1 = 0, bounds = 0, slice_cnt = 0;
+    int64_t slice_len = 0;
+    int32_t nslices = 0;
+    int64_t hist_base = 0;
+};
+struct JoinOffs {
+    RelOffs rel[2];
+    size_t bloom = 0;
+};
+
+// Workspace layout of one pipeline run (all offsets relative to the workspace base).
+struct Shape {
+    JoinOffs* jo = nullptr;      // [nj], caller-owned
+    int64_t slice_len = 0;
+    int64_t hist_len[2] = {0, 0};
+    int64_t total_slices[2] = {0, 0};
+    int64_t total_segs = 0, total_fine = 0, total_bloom_fine = 0;
+    int64_t task_cap = 0;
+    size_t hist = 0, hist_scan = 0, tcount = 0, toff = 0, tasks = 0, scan_tmp = 0, gwords = 0,
+           counters = 0, meta = 0;
+    int64_t scan_tmp_len = 0;
+    size_t meta_bytes = 0;      // descriptor image: nj JoinDesc + 5 prefix arrays of nj+1 int64
+    size_t total = 0;           // workspace bytes
+    int max_p1 = 1, max_p2 = 1, max_seg_words = 0;
+    bool any_bloom = false;
+};
+
+// Lays out `nj` joins in one workspace; fills jo[0..nj) and sh. Allocates nothing.
+void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int num_sms, JoinOffs* jo,
+                Shape& sh);
+
+// Writes the descriptor image for the joins into meta_host (sh.meta_bytes bytes of host memory,
+// to be copied to ws + sh.meta) and the launch arguments into `a`. Allocates nothing.
+void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const JoinIO* joins, int nj,
+                   const Shape& sh, char* ws, char* meta_host, int num_sms, PipelineArgs& a);
 
 class Engine {
 public:

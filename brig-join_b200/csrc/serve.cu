@@ -254,17 +254,16 @@ struct brig_serve_t {
 };
 
 namespace {
-thread_local std::string g_serve_error;
-
 template <class F>
 int serve_guard(F&& f) {
     try {
+        brig::set_last_error("");
         return f();
     } catch (const brig::Error& e) {
-        g_serve_error = e.msg;
+        brig::set_last_error(e.msg);
         return e.status;
     } catch (...) {
-        g_serve_error = "unknown failure";
+        brig::set_last_error("unknown failure");
         return (int)BRIG_E_INTERNAL;
     }
 }

@@ -242,6 +242,27 @@ int brig_gen_device(uint64_t seed, int64_t n_r, int64_t n_s, double match_frac, 
 int brig_gen_host(uint64_t seed, int64_t n_r, int64_t n_s, double match_frac, double zipf_s,
                   uint32_t* r_key, uint32_t* r_val, uint32_t* s_key, uint32_t* s_val);
 
+/* ---- Allocation-free join ----------------------------------------------------------------------
+ * No counterpart in the reference. For callers that cannot allocate device memory when they join:
+ * host frameworks that own all device memory through their own pool and forbid their operators to
+ * allocate outside it, and latency-critical callers that cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree. Same kernels and result as brig_join_run, but every
+ * intermediate buffer lives in one static device array of BRIG_NOALLOC_SCRATCH_BYTES that each GPU
+ * loading the library holds until the process exits; no handle, no cudaMalloc/cudaFree/
+ * cudaMallocHost. Limit: at most BRIG_NOALLOC_MAX_TUPLES tuples per relation, and the join's layout
+ * must fit the array (the default planner and the modulo preset with partition_size 512 do);
+ * larger requests return BRIG_E_UNSUPPORTED. The count is written to out->d_count (required).
+ * The first call on a device looks up the array's address and the first call on a host thread sets
+ * kernel attributes: make it before any stream capture. All calls on a device share the array and
+ * it keeps the last call's contents (the pipeline clears what must start at zero); calls whose work
+ * overlaps on the GPU race on it, so order them on one stream or with events. */
+#define BRIG_NOALLOC_MAX_TUPLES 262144
+#define BRIG_NOALLOC_SCRATCH_BYTES (16u << 20)
+int brig_join_run_noalloc(const brig_join_config* cfg,
+                          const uint32_t* r_key, const uint32_t* r_val, int64_t n_r,
+                          const uint32_t* s_key, const uint32_t* s_val, int64_t n_s,
+                          const brig_join_output* out, void* stream);
+
 /* Message for the last failed call on this thread (empty string if none). */
 const char* brig_join_last_error(void);
 
