@@ -65,7 +65,8 @@ class Config(C.Structure):
         ("device", C.c_int32),
         ("use_cuda_graph", C.c_int32),
         ("profile_stages", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("bloom_probe_level", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

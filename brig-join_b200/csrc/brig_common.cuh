@@ -21,7 +21,8 @@ namespace brig {
 constexpr int kMaxP1 = 4096;          // first-level fan-out (the reference caps at PARTITION_MAX=2048,
                                       // src/kernel_functions.h:15)
 constexpr int kMaxP2 = 1024;          // second-level fan-out (SECOND_PASS_MAX=4096, :14)
-constexpr int kMaxTable = 8192;       // R tuples per shared-memory table
+constexpr int kMaxTable = 8192;       // build-side tuples per shared-memory table (largest allowed)
+constexpr int kDefaultTable = 4096;   // default table capacity
 constexpr int kMinTable = 256;
 constexpr int kMaxBloomK = 16;
 constexpr int kThreads = 512;         // threads per CTA of every partition and probe kernel
@@ -33,7 +34,7 @@ enum Counter : int {
     kCntMatches = 0,      // exact number of matches
     kCntSurvivors = 1,    // S tuples that passed the Bloom filter
     kCntTasks = 2,        // probe tasks generated
-    kCntSplitTasks = 3,   // tasks whose R chunk is a piece of an oversized partition
+    kCntSplitTasks = 3,   // tasks whose build chunk is a piece of an oversized partition
     kCntErrors = 4,       // device-side consistency failures (must stay 0)
     kCntWords = 8
 };
@@ -103,11 +104,14 @@ BRIG_HD uint32_t part_fine(const PartFn& f, uint32_t key) {
 BRIG_HD uint32_t bucket_of(uint32_t key, uint32_t nb_mask) { return mix32(key) & nb_mask; }
 
 // ---- Bloom filter -------------------------------------------------------------------------------
-// Cache-line blocked: the filter is one segment per finest partition, a segment is seg_blocks
-// blocks of 256 bits (one 32-byte DRAM sector), and a key sets k bits inside one block. Bit i of a
-// key is (a + i*b) mod 256 with b odd, so the k bits are distinct (double hashing, Kirsch &
-// Mitzenmacher, "Less hashing, same performance", 2006). The reference uses 256-bit blocks and one
-// segment per first-level partition (src/bloom.cu:698-722, src/hash_kernel.cu:555-582).
+// Cache-line blocked and sectorised: the filter is one segment per finest partition, a segment is
+// seg_blocks blocks of 256 bits (one 32-byte DRAM sector, eight 32-bit words), and a key sets one
+// bit in each of its first k words (words 0..7, then again from word 0 for k > 8). So a probe is one
+// sector load and the masks are shifts, with no search or dynamic indexing ("sectorized" blocked
+// filters, Lang et al., "Performance-Optimal Filtering: Bloom overtakes Cuckoo at High
+// Throughput", VLDB 2019). The reference uses 256-bit blocks with k bit positions anywhere in the
+// block and one segment per first-level partition (src/bloom.cu:698-722,
+// src/hash_kernel.cu:555-582).
 struct BloomKey {
     uint32_t block;     // block index inside the segment
     uint32_t mask[8];   // bits to set/test in the block's 8 words
@@ -116,21 +120,15 @@ struct BloomKey {
 BRIG_HD uint64_t bloom_hash(uint32_t key) { return mix64((uint64_t)key ^ 0x6a09e667f3bcc909ull); }
 
 BRIG_HD void bloom_key(uint32_t key, uint32_t seg_blocks, int k, BloomKey& bk) {
-    uint64_t g = bloom_hash(key);
-    bk.block = fastrange32((uint32_t)(g >> 32), seg_blocks);
-    uint32_t a = (uint32_t)g & 255u;
-    uint32_t b = ((uint32_t)(g >> 8) & 255u) | 1u;
+    const uint64_t g = bloom_hash(key);
+    // bits 40..63 pick the block (24-bit multiply-shift range reduction), bits 0..39 the word bits
+    bk.block = (uint32_t)(((g >> 40) * (uint64_t)seg_blocks) >> 24);
+    const uint64_t g2 = k > 8 ? mix64(g) : 0ull;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) bk.mask[w] = 0;
-    // Unrolled with compare-and-select so the mask stays in registers (no dynamic indexing).
-#pragma unroll
-    for (int i = 0; i < kMaxBloomK; ++i) {
-        if (i < k) {
-            const uint32_t pos = (a + (uint32_t)i * b) & 255u;
-            const uint32_t w = pos >> 5, bit = 1u << (pos & 31u);
-#pragma unroll
-            for (int ww = 0; ww < 8; ++ww) bk.mask[ww] |= (w == (uint32_t)ww) ? bit : 0u;
-        }
+    for (int w = 0; w < 8; ++w) {
+        uint32_t m = (w < k) ? (1u << ((uint32_t)(g >> (5 * w)) & 31u)) : 0u;
+        if (w + 8 < k) m |= 1u << ((uint32_t)(g2 >> (5 * w)) & 31u);
+        bk.mask[w] = m;
     }
 }
 
@@ -149,7 +147,9 @@ struct RelPlan {
     int64_t* b1;           // [P1 + 1] start of each level-1 partition in l1
     int64_t* bounds;       // [P1*P2 + 1] start of each finest partition in the final buffer
                            // (equal to b1 when P2 == 1)
-    uint32_t* slice_cnt;   // [nslices] survivors per slice (S with Bloom only)
+    uint32_t* slice_cnt;   // [nslices] survivors per slice (S with a level-1 Bloom probe)
+    uint32_t* fine_cnt;    // [P1*P2] tuples per finest partition when the final buffer has gaps
+                           // (S with a level-2 Bloom probe), else nullptr: size = bounds[f+1]-bounds[f]
 };
 
 struct JoinDesc {
@@ -164,20 +164,28 @@ struct JoinDesc {
     uint32_t* bloom;       // filter words (nullptr when off)
     uint32_t seg_blocks;   // blocks per Bloom segment
     int32_t bloom_k;
+    int32_t bloom_level;   // S pass that probes the filter: 1 first (fused with the histogram of
+                           // S's level-1 pass), 2 second (fused with S's level-2 pass)
     int64_t fine_base;     // offset of this join's P1*P2 entries in the global task-count array
-    int32_t table_cap;     // max R tuples per probe task
-    int32_t s_chunk;       // max S tuples per probe task
+    int32_t table_cap;     // max build-side tuples per probe task
+    int32_t s_chunk;       // max streamed tuples per probe task
 };
 
-// One probe task: build a table from R[r_begin, r_begin + r_len) and probe it with
-// S[s_begin, s_begin + s_len), both in the join's final partitioned buffers.
+// One probe task of one finest partition: build a shared-memory table from a chunk of the build
+// side, then stream a chunk of the other side through it. The build side is the smaller of the
+// two partitions (with the Bloom filter on, usually S's survivors), so the larger side is read
+// once, as a coalesced stream. Both ranges index the join's final partitioned buffers.
+enum TaskFlag : uint32_t {
+    kTaskSplit = 1u,       // the build chunk is a piece of a build side larger than one table
+    kTaskBuildS = 2u,      // build from S and stream R (otherwise build from R and stream S)
+};
 struct Task {
     int32_t join;
-    uint32_t r_len;
-    int64_t r_begin;
-    uint32_t s_len;
-    uint32_t split;        // 1 if the R chunk is a piece of an oversized partition
-    int64_t s_begin;
+    uint32_t flags;
+    int64_t b_begin;       // build-side chunk
+    int64_t p_begin;       // streamed chunk
+    uint32_t b_len;
+    uint32_t p_len;
 };
 static_assert(sizeof(Task) == 32, "task layout");
 

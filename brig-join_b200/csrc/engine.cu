@@ -32,7 +32,7 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
     JoinPlan p;
     p.nr = nr;
     p.ns = ns;
-    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kMaxTable;
+    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
     const int64_t target = std::max<int64_t>(1, (int64_t)T * 3 / 4);  // R tuples per finest partition
     PartFn& f = p.pf;
     f.mode = cfg.partition_mode;
@@ -45,7 +45,10 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
                                      "(use BRIG_PART_MODULO for other fan-outs)");
             b1 = ceil_log2(cfg.partition_size);
         } else {
-            b1 = bits <= 12 ? bits : 11;
+            // At most 512 level-1 partitions: every CTA keeps one open output run per partition,
+            // and at 512 the runs of all CTAs (148 x 512 lines) stay resident in L2 until they are
+            // completed, so DRAM sees whole lines. Anything finer goes to level 2.
+            b1 = bits <= 9 ? bits : 9;
         }
         if (cfg.second_partition_size > 0) {
             if (!is_pow2(cfg.second_partition_size) || cfg.second_partition_size > kMaxP2)
@@ -94,6 +97,15 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
         p.bloom = true;
         p.k = k;
         p.bloom_bits = p.nfine * (int64_t)p.seg_blocks * 256;
+        // Probing in S's first pass reads one random 32-byte block per S tuple; that is cheap only
+        // while the filter stays in the 126 MB L2. A larger filter is probed in S's second pass,
+        // one level-1 partition (a contiguous run of segments) at a time.
+        const int64_t kL2FilterBytes = 64ll << 20;
+        int lvl = cfg.bloom_probe_level;
+        if (lvl == 0) lvl = (p.bloom_bits / 8 <= kL2FilterBytes) ? 1 : 2;
+        if (lvl != 1 && lvl != 2) fail(BRIG_E_INVALID, "bloom_probe_level must be 0, 1 or 2");
+        if (f.P2 == 1) lvl = 1;
+        p.bloom_level = lvl;
     }
     return p;
 }
@@ -126,7 +138,7 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
     sl = ((sl + kTile - 1) / kTile) * kTile;
     sl = std::max<int64_t>(sl, 4 * kTile);
     sh.slice_len = sl;
-    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kMaxTable;
+    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
     const int C = cfg.s_chunk > 0 ? cfg.s_chunk : 16384;
     Layout L;
     for (int j = 0; j < nj; ++j) {
@@ -146,7 +158,8 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
             if (two) ro.bounds = L.take(((size_t)p.nfine + 1) * 8);
             if (r == 1 && p.bloom) {
                 ro.cmp = L.take((size_t)std::max<int64_t>(n[r], 1) * 8);
-                ro.slice_cnt = L.take((size_t)ro.nslices * 4);
+                if (p.bloom_level == 1) ro.slice_cnt = L.take((size_t)ro.nslices * 4);
+                else ro.fine_cnt = L.take((size_t)p.nfine * 4);
             }
             ro.hist_base = sh.hist_len[0] + sh.hist_len[1];  // provisional, fixed below
             sh.total_slices[r] += ro.nslices;
@@ -319,7 +332,7 @@ void Engine::ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key) {
 
 void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const JoinIO* joins, int nj,
                    const Shape& sh, char* ws, char* meta_host, int num_sms, PipelineArgs& a) {
-    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kMaxTable;
+    const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
     const int C = cfg.s_chunk > 0 ? cfg.s_chunk : 16384;
     if (T < kMinTable || T > kMaxTable || !is_pow2(T))
         fail(BRIG_E_INVALID, "table_capacity must be a power of two in [256, 8192]");
@@ -357,6 +370,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
             R.b1 = reinterpret_cast<int64_t*>(ws + ro.b1);
             R.bounds = p.pf.P2 > 1 ? reinterpret_cast<int64_t*>(ws + ro.bounds) : R.b1;
             R.slice_cnt = ro.slice_cnt ? reinterpret_cast<uint32_t*>(ws + ro.slice_cnt) : nullptr;
+            R.fine_cnt = ro.fine_cnt ? reinterpret_cast<uint32_t*>(ws + ro.fine_cnt) : nullptr;
         }
         d.pf = p.pf;
         d.out_r = io.out.r_val;
@@ -368,6 +382,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
         d.bloom = p.bloom ? reinterpret_cast<uint32_t*>(ws + o.bloom) : nullptr;
         d.seg_blocks = p.seg_blocks;
         d.bloom_k = p.k;
+        d.bloom_level = p.bloom_level;
         d.fine_base = finep[j];
         d.table_cap = T;
         d.s_chunk = C;
@@ -464,6 +479,7 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
             key.push_back(plans[j].pf.P1);
             key.push_back(plans[j].pf.P2);
             key.push_back(plans[j].bloom ? (int64_t)plans[j].seg_blocks : (int64_t)-1);
+            key.push_back(plans[j].bloom_level);
         }
     }
     if (use_graph) {

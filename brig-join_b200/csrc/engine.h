@@ -29,6 +29,7 @@ struct JoinPlan {
     PartFn pf{};
     int64_t nfine = 1;
     bool bloom = false;
+    int bloom_level = 0;        // S pass that probes the filter (1 or 2)
     int k = 0;
     uint32_t seg_blocks = 0;
     int64_t bloom_bits = 0;     // allocated bits
@@ -44,7 +45,7 @@ struct JoinIO {
 
 // Byte offsets of one relation's buffers inside a pipeline workspace.
 struct RelOffs {
-    size_t l1 = 0, l2 = 0, cmp = 0, b1 = 0, bounds = 0, slice_cnt = 0;
+    size_t l1 = 0, l2 = 0, cmp = 0, b1 = 0, bounds = 0, slice_cnt = 0, fine_cnt = 0;
     int64_t slice_len = 0;
     int32_t nslices = 0;
     int64_t hist_base = 0;

@@ -127,19 +127,100 @@ __device__ __forceinline__ const uint2* final_buf(const JoinDesc& d, int rel) {
     return d.pf.P2 > 1 ? d.rel[rel].l2 : d.rel[rel].l1;
 }
 
-// Loads one tuple from separate key/value arrays.
-struct SoASrc {
-    const uint32_t* __restrict__ k;
-    const uint32_t* __restrict__ v;
-    __device__ __forceinline__ uint2 operator()(int64_t i) const {
-        return make_uint2(__ldg(k + i), __ldg(v + i));
+// ---- TMA bulk copies (cp.async.bulk, no multicast) into shared memory ---------------------------
+// A CTA double-buffers its input: while it processes tile t out of one buffer, the bulk-copy engine
+// fills the other with tile t+1, so the load latency overlaps the shared-memory phases of the
+// previous tile. Completion is tracked with one mbarrier per buffer (arrival count 1: the issuing
+// thread's expect_tx). Every wait is bounded; a wait that runs out counts an error, waits once
+// more (also bounded) and lets the kernel continue, so the host reports BRIG_E_INTERNAL instead of
+// the GPU hanging.
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// Global -> shared bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// Orders this thread's earlier shared-memory accesses before later async-proxy (bulk copy) writes.
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+constexpr uint32_t kMaxPolls = 1u << 22;  // each poll may suspend for a bounded hardware interval
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long* err) {
+    for (uint32_t it = 0; it < kMaxPolls; ++it)
+        if (mbar_try_wait(bar, parity)) return;
+    if (threadIdx.x == 0) atomicAdd(err, 1ull);
+    for (uint32_t it = 0; it < kMaxPolls; ++it)
+        if (mbar_try_wait(bar, parity)) return;
+}
+
+// Where the tuples of a tile come from: packed tuples in an engine buffer (p), or the caller's
+// separate key/value arrays (k, v). Packed tiles are copied from the 16-byte boundary at or below
+// their first tuple (engine buffers are padded, so reading up to 8 bytes past either end stays
+// inside the workspace). Key/value tiles are bulk-copied when both arrays are 16-byte aligned at
+// tile starts; the last (tn mod 4) tuples of a tile, or every tuple of unaligned arrays, are
+// read with ordinary loads, so nothing outside the caller's arrays is read.
+struct TileIn {
+    const uint2* p;
+    const uint32_t* k;
+    const uint32_t* v;
+    bool bulk_kv;
+};
+constexpr size_t kTileBuf = (size_t)(kTile + 2) * 8;  // one input buffer
+
+__device__ __forceinline__ uint32_t tile_mis(const TileIn& in, int64_t t0) {
+    return in.p ? (uint32_t)((((uintptr_t)(in.p + t0)) & 15) ? 1 : 0) : 0u;
+}
+// Thread 0: starts the copy of tuples [t0, t0 + tn) into buf and arms bar.
+__device__ __forceinline__ void tile_issue(const TileIn& in, int64_t t0, int tn, unsigned char* buf, uint64_t* bar) {
+    fence_proxy_async();
+    if (in.p) {
+        const uint32_t mis = tile_mis(in, t0);
+        const uint32_t bytes = (((uint32_t)tn + mis) * 8u + 15u) & ~15u;
+        mbar_arrive_tx(bar, bytes);
+        bulk_g2s(buf, in.p + t0 - mis, bytes, bar);
+    } else if (in.bulk_kv && (tn & ~3) > 0) {
+        const uint32_t bytes = (uint32_t)(tn & ~3) * 4u;
+        mbar_arrive_tx(bar, 2 * bytes);
+        bulk_g2s(buf, in.k + t0, bytes, bar);
+        bulk_g2s(buf + (size_t)kTile * 4, in.v + t0, bytes, bar);
+    } else {
+        mbar_arrive(bar);
     }
-};
-// Loads one packed tuple.
-struct AoSSrc {
-    const uint2* __restrict__ p;
-    __device__ __forceinline__ uint2 operator()(int64_t i) const { return __ldg(p + i); }
-};
+}
+__device__ __forceinline__ uint2 tile_item(const TileIn& in, const unsigned char* buf, int64_t t0, int i, int tn,
+                                           uint32_t mis) {
+    if (in.p) return reinterpret_cast<const uint2*>(buf)[i + mis];
+    if (in.bulk_kv && i < (tn & ~3))
+        return make_uint2(reinterpret_cast<const uint32_t*>(buf)[i],
+                          reinterpret_cast<const uint32_t*>(buf + (size_t)kTile * 4)[i]);
+    return make_uint2(__ldcs(in.k + t0 + i), __ldcs(in.v + t0 + i));
+}
+
 struct Bin1 {
     PartFn f;
     __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return part1(f, key); }
@@ -149,29 +230,40 @@ struct Bin2 {
     __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return part2(f, key); }
 };
 
-// Scatters tuples [begin, end) of `src` into `out`. cursor[b] is the next output position of bin
-// b; it advances as tiles are written. Each tile of kTile tuples is counted, reordered by bin in
-// shared memory (stage), and written so that consecutive threads store consecutive positions of
-// one bin's run.
-template <class Src, class Bin>
-__device__ void scatter_tiles(const Src& src, int64_t begin, int64_t end, const Bin& bin, int nbins,
-                              uint2* __restrict__ out, int64_t out_limit, int64_t* cursor,
-                              uint32_t* cnt, uint32_t* tmp, uint2* stage,
+// Scatters tuples [begin, end) of `in` into `out`. cursor[b] is the next output position of bin
+// b; it advances as tiles are written. Each tile of kTile tuples arrives by bulk copy (the next
+// one is in flight meanwhile), is counted by bin, reordered by bin in shared memory (stage) and
+// written so that consecutive threads store consecutive positions of one bin's run.
+// `inbuf` holds two tile buffers, `bars` their mbarriers, `ph` the parity of each barrier.
+template <class Bin>
+__device__ void scatter_tiles(const TileIn& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
+                              uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, uint32_t* cnt,
+                              uint32_t* tmp, uint2* stage, unsigned char* inbuf, uint64_t* bars, uint32_t& ph,
                               unsigned long long* errors) {
     constexpr int kItems = kTile / kThreads;
-    for (int64_t t0 = begin; t0 < end; t0 += kTile) {
+    const int64_t ntiles = (end - begin + kTile - 1) / kTile;
+    if (ntiles <= 0) return;
+    if (threadIdx.x == 0) tile_issue(in, begin, (int)min_i64(kTile, end - begin), inbuf, &bars[0]);
+    for (int64_t t = 0; t < ntiles; ++t) {
+        const int64_t t0 = begin + t * kTile;
         const int tn = (int)min_i64(kTile, end - t0);
-        for (int b = threadIdx.x; b < nbins; b += kThreads) cnt[b] = 0;
+        const int b = (int)(t & 1);
+        if (threadIdx.x == 0 && t + 1 < ntiles)
+            tile_issue(in, t0 + kTile, (int)min_i64(kTile, end - t0 - kTile), inbuf + (b ^ 1) * kTileBuf,
+                       &bars[b ^ 1]);
+        for (int x = threadIdx.x; x < nbins; x += kThreads) cnt[x] = 0;
+        mbar_wait(&bars[b], (ph >> b) & 1u, errors);
+        ph ^= 1u << b;
         __syncthreads();
-        uint2 v[kItems];
-        uint32_t bb[kItems], rk[kItems];
+        const unsigned char* buf = inbuf + b * kTileBuf;
+        const uint32_t mis = tile_mis(in, t0);
+        uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const int i = k * kThreads + threadIdx.x;
             if (i < tn) {
-                v[k] = src(t0 + i);
-                bb[k] = bin(v[k].x);
-                rk[k] = atomicAdd(&cnt[bb[k]], 1u);
+                const uint32_t bb = bin(tile_item(in, buf, t0, i, tn, mis).x);
+                br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
             }
         }
         __syncthreads();
@@ -179,23 +271,44 @@ __device__ void scatter_tiles(const Src& src, int64_t begin, int64_t end, const 
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const int i = k * kThreads + threadIdx.x;
-            if (i < tn) stage[cnt[bb[k]] + rk[k]] = v[k];
+            if (i < tn) stage[cnt[br[k] >> 16] + (br[k] & 0xffffu)] = tile_item(in, buf, t0, i, tn, mis);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < tn; i += kThreads) {
             const uint2 e = stage[i];
-            const uint32_t b = bin(e.x);
-            const int64_t dst = cursor[b] + (int64_t)(i - (int)cnt[b]);
+            const uint32_t bb = bin(e.x);
+            const int64_t dst = cursor[bb] + (int64_t)(i - (int)cnt[bb]);
             if (dst >= 0 && dst < out_limit) out[dst] = e;
             else atomicAdd(errors, 1ull);
         }
         __syncthreads();
-        for (int b = threadIdx.x; b < nbins; b += kThreads) {
-            const uint32_t nxt = (b + 1 < nbins) ? cnt[b + 1] : (uint32_t)tn;
-            cursor[b] += (int64_t)(nxt - cnt[b]);
+        for (int x = threadIdx.x; x < nbins; x += kThreads) {
+            const uint32_t nxt = (x + 1 < nbins) ? cnt[x + 1] : (uint32_t)tn;
+            cursor[x] += (int64_t)(nxt - cnt[x]);
         }
         __syncthreads();
     }
+}
+
+__device__ __forceinline__ void init_bars(uint64_t* bars) {
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+}
+
+// Bloom test of one key against the segment of its finest partition f.
+__device__ __forceinline__ bool bloom_test(const JoinDesc& d, uint32_t f, uint32_t key) {
+    BloomKey bk;
+    bloom_key(key, d.seg_blocks, d.bloom_k, bk);
+    const uint4* blk = reinterpret_cast<const uint4*>(d.bloom + ((int64_t)f * d.seg_blocks + bk.block) * 8);
+    const uint4 w0 = __ldg(blk), w1 = __ldg(blk + 1);
+    return ((w0.x & bk.mask[0]) == bk.mask[0]) && ((w0.y & bk.mask[1]) == bk.mask[1]) &&
+           ((w0.z & bk.mask[2]) == bk.mask[2]) && ((w0.w & bk.mask[3]) == bk.mask[3]) &&
+           ((w1.x & bk.mask[4]) == bk.mask[4]) && ((w1.y & bk.mask[5]) == bk.mask[5]) &&
+           ((w1.z & bk.mask[6]) == bk.mask[6]) && ((w1.w & bk.mask[7]) == bk.mask[7]);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -222,13 +335,13 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         for (uint32_t i = threadIdx.x; i < P1; i += kThreads) sh_cnt[i] = 0;
         if (threadIdx.x == 0) s_cursor = 0;
         __syncthreads();
-        const bool bloom = (rel == 1) && d.bloom != nullptr;
+        const bool bloom = (rel == 1) && d.bloom != nullptr && d.bloom_level == 1;
         if (!bloom) {
             const uint32_t* __restrict__ key = R.key;
             if ((((uintptr_t)(key + b)) & 15) == 0) {
                 int64_t i = b + 4 * (int64_t)threadIdx.x;
                 for (; i + 3 < e; i += 4 * kThreads) {
-                    const uint4 k4 = __ldg(reinterpret_cast<const uint4*>(key + i));
+                    const uint4 k4 = __ldcs(reinterpret_cast<const uint4*>(key + i));
                     atomicAdd(&sh_cnt[part1(pf, k4.x)], 1u);
                     atomicAdd(&sh_cnt[part1(pf, k4.y)], 1u);
                     atomicAdd(&sh_cnt[part1(pf, k4.z)], 1u);
@@ -237,36 +350,24 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                 // tail: at most 3 tuples past the last full vector
                 const int64_t tail0 = b + ((e - b) & ~(int64_t)3);
                 for (int64_t t = tail0 + threadIdx.x; t < e; t += kThreads)
-                    atomicAdd(&sh_cnt[part1(pf, __ldg(key + t))], 1u);
+                    atomicAdd(&sh_cnt[part1(pf, __ldcs(key + t))], 1u);
             } else {
                 for (int64_t t = b + threadIdx.x; t < e; t += kThreads)
-                    atomicAdd(&sh_cnt[part1(pf, __ldg(key + t))], 1u);
+                    atomicAdd(&sh_cnt[part1(pf, __ldcs(key + t))], 1u);
             }
         } else {
             // Bloom probe of every S key against the segment of its finest partition; survivors are
             // compacted (key, value) into R.cmp[b, b + count) and counted per level-1 partition.
             const uint32_t* __restrict__ key = R.key;
             const uint32_t* __restrict__ val = R.val;
-            const uint32_t* __restrict__ filt = d.bloom;
-            const uint32_t seg_blocks = d.seg_blocks;
-            const int k = d.bloom_k;
             for (int64_t i0 = b; i0 < e; i0 += kThreads) {
                 const int64_t i = i0 + threadIdx.x;
                 bool pass = false;
                 uint32_t kk = 0, p = 0;
                 if (i < e) {
-                    kk = __ldg(key + i);
+                    kk = __ldcs(key + i);
                     p = part1(pf, kk);
-                    const uint32_t f = p * pf.P2 + part2(pf, kk);
-                    BloomKey bk;
-                    bloom_key(kk, seg_blocks, k, bk);
-                    const uint4* blk = reinterpret_cast<const uint4*>(
-                        filt + ((int64_t)f * seg_blocks + bk.block) * 8);
-                    const uint4 w0 = __ldg(blk), w1 = __ldg(blk + 1);
-                    pass = ((w0.x & bk.mask[0]) == bk.mask[0]) && ((w0.y & bk.mask[1]) == bk.mask[1]) &&
-                           ((w0.z & bk.mask[2]) == bk.mask[2]) && ((w0.w & bk.mask[3]) == bk.mask[3]) &&
-                           ((w1.x & bk.mask[4]) == bk.mask[4]) && ((w1.y & bk.mask[5]) == bk.mask[5]) &&
-                           ((w1.z & bk.mask[6]) == bk.mask[6]) && ((w1.w & bk.mask[7]) == bk.mask[7]);
+                    pass = bloom_test(d, p * pf.P2 + part2(pf, kk), kk);
                 }
                 const uint32_t m = __ballot_sync(0xffffffffu, pass);
                 if (m) {
@@ -291,7 +392,7 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                 R.slice_cnt[s] = s_cursor;
                 atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSurvivors]),
                           (unsigned long long)s_cursor);
-            } else if (rel == 1) {
+            } else if (rel == 1 && d.bloom == nullptr) {
                 atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSurvivors]),
                           (unsigned long long)(e - b));
             }
@@ -304,12 +405,16 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 // of this relation, i.e. the partition's start plus the counts of all earlier slices.
 __global__ void __launch_bounds__(kThreads)
 k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
-             const int64_t* __restrict__ scan, unsigned long long* gwords) {
+             const int64_t* __restrict__ scan, unsigned long long* gwords, int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint2* stage = reinterpret_cast<uint2*>(smem);                          // [kTile]
-    int64_t* cursor = reinterpret_cast<int64_t*>(stage + kTile);            // [max P1]
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(cursor + kMaxP1);           // [max P1]
+    unsigned char* inbuf = smem;                                                // 2 tile buffers
+    uint2* stage = reinterpret_cast<uint2*>(smem + 2 * kTileBuf);               // [kTile]
+    int64_t* cursor = reinterpret_cast<int64_t*>(stage + kTile);                // [max_bins]
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(cursor + max_bins);             // [max_bins]
     __shared__ uint32_t tmp[kThreads / 32];
+    __shared__ __align__(8) uint64_t bars[2];
+    init_bars(bars);
+    uint32_t ph = 0;
     const int64_t total = slice_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(slice_prefix, nj, g);
@@ -317,7 +422,7 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const RelPlan& R = d.rel[rel];
         const int s = (int)(g - slice_prefix[j]);
         const int64_t b = (int64_t)s * R.slice_len;
-        const bool bloom = (rel == 1) && d.bloom != nullptr;
+        const bool bloom = (rel == 1) && d.bloom != nullptr && d.bloom_level == 1;
         const int64_t e = bloom ? b + R.slice_cnt[s] : min(b + R.slice_len, R.n);
         const uint32_t P1 = d.pf.P1;
         const int64_t* S = scan + R.hist_base;
@@ -326,13 +431,15 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
             cursor[p] = S[(int64_t)p * R.nslices + s] - s0;
         __syncthreads();
         const Bin1 bin{d.pf};
+        TileIn in;
         if (bloom) {
-            scatter_tiles(AoSSrc{R.cmp}, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, tmp, stage,
-                          &gwords[kGErrors]);
+            in = TileIn{R.cmp, nullptr, nullptr, false};
         } else {
-            scatter_tiles(SoASrc{R.key, R.val}, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, tmp, stage,
-                          &gwords[kGErrors]);
+            const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 15) == 0;
+            in = TileIn{nullptr, R.key, R.val, al};
         }
+        scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, tmp, stage, inbuf, bars, ph,
+                      &gwords[kGErrors]);
     }
 }
 
@@ -355,12 +462,17 @@ __global__ void k_bounds_l1(const JoinDesc* __restrict__ J, int nj, int rel, con
 // the finest-partition bounds, then scatters the partition from l1 into l2 in the same range.
 __global__ void __launch_bounds__(kThreads)
 k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
-               unsigned long long* gwords) {
+               unsigned long long* gwords, int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint2* stage = reinterpret_cast<uint2*>(smem);                 // [kTile]
-    int64_t* cursor = reinterpret_cast<int64_t*>(stage + kTile);   // [max P2]
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(cursor + kMaxP2);  // [max P2]
+    unsigned char* inbuf = smem;                                                // 2 tile buffers
+    uint2* stage = reinterpret_cast<uint2*>(smem + 2 * kTileBuf);               // [kTile]
+    int64_t* cursor = reinterpret_cast<int64_t*>(stage + kTile);                // [max_bins]
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(cursor + max_bins);             // [max_bins]
     __shared__ uint32_t tmp[kThreads / 32];
+    __shared__ uint32_t s_surv;
+    __shared__ __align__(8) uint64_t bars[2];
+    init_bars(bars);
+    uint32_t ph = 0;
     const int64_t total = seg_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(seg_prefix, nj, g);
@@ -370,10 +482,68 @@ k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* _
         const uint32_t P2 = d.pf.P2, P1 = d.pf.P1;
         const int64_t begin = R.b1[p], end = R.b1[p + 1];
         const Bin2 bin{d.pf};
+        const bool bloom = rel == 1 && d.bloom != nullptr && d.bloom_level == 2;
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cnt[q] = 0;
+        if (threadIdx.x == 0) s_surv = 0;
         __syncthreads();
-        for (int64_t i = begin + threadIdx.x; i < end; i += kThreads)
-            atomicAdd(&cnt[bin(__ldg(&R.l1[i].x))], 1u);
+        int64_t src_end = end;
+        const uint2* src = R.l1;
+        if (!bloom) {
+            // eight independent loads in flight per thread
+            const uint2* __restrict__ l1 = R.l1;
+            for (int64_t i0 = begin + threadIdx.x; i0 < end; i0 += 8 * kThreads) {
+                uint32_t kk[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int64_t i = i0 + u * kThreads;
+                    kk[u] = i < end ? __ldcs(&l1[i].x) : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+                    if (i0 + u * kThreads < end) atomicAdd(&cnt[bin(kk[u])], 1u);
+            }
+        } else {
+            // Bloom probe fused into the level-2 pass: this level-1 partition's filter segments are
+            // contiguous and stay in L2 while the CTA works on it. Survivors are compacted into
+            // cmp[begin, begin + survivors) and counted by level-2 id.
+            const int lane = threadIdx.x & 31;
+            for (int64_t i0 = begin; i0 < end; i0 += kThreads) {
+                const int64_t i = i0 + threadIdx.x;
+                bool pass = false;
+                uint2 e = make_uint2(0u, 0u);
+                uint32_t q = 0;
+                if (i < end) {
+                    e = __ldcs(&R.l1[i]);
+                    q = bin(e.x);
+                    pass = bloom_test(d, p * P2 + q, e.x);
+                }
+                const uint32_t m = __ballot_sync(0xffffffffu, pass);
+                if (m) {
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(&s_surv, (uint32_t)__popc(m));
+                    base = __shfl_sync(0xffffffffu, base, 0);
+                    if (pass) {
+                        atomicAdd(&cnt[q], 1u);
+                        const int64_t dst = begin + base + __popc(m & lanemask_lt());
+                        if (dst < end) R.cmp[dst] = e;
+                        else atomicAdd(&gwords[kGErrors], 1ull);
+                    }
+                }
+            }
+            // the survivors are read back below by bulk copies (async proxy)
+            asm volatile("fence.proxy.async.global;" ::: "memory");
+            __syncthreads();
+            src_end = begin + s_surv;
+            src = R.cmp;
+            if (threadIdx.x == 0)
+                atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSurvivors]),
+                          (unsigned long long)s_surv);
+        }
+        __syncthreads();
+        for (uint32_t q = threadIdx.x; q < P2; q += kThreads) {
+            const uint32_t c = cnt[q];
+            if (R.fine_cnt) R.fine_cnt[(int64_t)p * P2 + q] = c;
+        }
         __syncthreads();
         block_scan_excl(cnt, (int)P2, tmp);
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) {
@@ -382,8 +552,8 @@ k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* _
         }
         if (threadIdx.x == 0 && p == P1 - 1) R.bounds[(int64_t)P1 * P2] = end;
         __syncthreads();
-        scatter_tiles(AoSSrc{R.l1}, begin, end, bin, (int)P2, R.l2, end, cursor, cnt, tmp, stage,
-                      &gwords[kGErrors]);
+        scatter_tiles(TileIn{src, nullptr, nullptr, false}, begin, src_end, bin, (int)P2, R.l2, src_end, cursor,
+                      cnt, tmp, stage, inbuf, bars, ph, &gwords[kGErrors]);
     }
 }
 
@@ -435,14 +605,21 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
     }
 }
 
-// Probe tasks per finest partition. An R partition of at most table_cap tuples is built once per
-// S chunk of s_chunk tuples; a larger one is cut into table_cap chunks, each probed by the whole S
-// partition (the exact form of the reference's split path).
-__device__ __forceinline__ void task_shape(int64_t nr, int64_t ns, int64_t T, int64_t C,
-                                           int64_t& nrc, int64_t& nsc) {
-    if (nr == 0 || ns == 0) { nrc = 0; nsc = 0; return; }
-    nrc = (nr + T - 1) / T;
-    nsc = nrc == 1 ? (ns + C - 1) / C : 1;
+// Probe tasks per finest partition. The smaller of the two partitions is the build side. A build
+// side of at most table_cap tuples is built once per streamed chunk of s_chunk tuples (so a hot
+// partition spreads over many CTAs); a larger one is cut into table_cap chunks, each streamed
+// against the whole other side (the exact form of the reference's split path, which stops at the
+// first match, src/kernel_functions.cu:356-395).
+__device__ __forceinline__ void fine_range(const RelPlan& R, int64_t f, int64_t& begin, int64_t& n) {
+    begin = R.bounds[f];
+    n = R.fine_cnt ? (int64_t)R.fine_cnt[f] : R.bounds[f + 1] - begin;
+}
+
+__device__ __forceinline__ void task_shape(int64_t nb, int64_t np, int64_t T, int64_t C, int64_t& nbc,
+                                           int64_t& npc) {
+    if (nb == 0 || np == 0) { nbc = 0; npc = 0; return; }
+    nbc = (nb + T - 1) / T;
+    npc = nbc == 1 ? (np + C - 1) / C : 1;
 }
 
 __global__ void k_tasks_count(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ fine_prefix,
@@ -454,11 +631,12 @@ __global__ void k_tasks_count(const JoinDesc* __restrict__ J, int nj, const int6
         const int j = find_owner(fine_prefix, nj, g);
         const JoinDesc& d = J[j];
         const int64_t f = g - fine_prefix[j];
-        const int64_t nr = d.rel[0].bounds[f + 1] - d.rel[0].bounds[f];
-        const int64_t ns = d.rel[1].bounds[f + 1] - d.rel[1].bounds[f];
-        int64_t nrc, nsc;
-        task_shape(nr, ns, d.table_cap, d.s_chunk, nrc, nsc);
-        tcount[g] = (uint32_t)(nrc * nsc);
+        int64_t r0, nr, s0, ns, nbc, npc;
+        fine_range(d.rel[0], f, r0, nr);
+        fine_range(d.rel[1], f, s0, ns);
+        const bool bs = ns < nr;
+        task_shape(bs ? ns : nr, bs ? nr : ns, d.table_cap, d.s_chunk, nbc, npc);
+        tcount[g] = (uint32_t)(nbc * npc);
     }
 }
 
@@ -471,31 +649,33 @@ __global__ void k_tasks_write(const JoinDesc* __restrict__ J, int nj, const int6
         const int j = find_owner(fine_prefix, nj, g);
         const JoinDesc& d = J[j];
         const int64_t f = g - fine_prefix[j];
-        const int64_t r0 = d.rel[0].bounds[f], nr = d.rel[0].bounds[f + 1] - r0;
-        const int64_t s0 = d.rel[1].bounds[f], ns = d.rel[1].bounds[f + 1] - s0;
-        int64_t nrc, nsc;
+        int64_t r0, nr, s0, ns, nbc, npc;
+        fine_range(d.rel[0], f, r0, nr);
+        fine_range(d.rel[1], f, s0, ns);
+        const bool bs = ns < nr;
+        const int64_t b0 = bs ? s0 : r0, nb = bs ? ns : nr;
+        const int64_t p0 = bs ? r0 : s0, np = bs ? nr : ns;
         const int64_t T = d.table_cap, C = d.s_chunk;
-        task_shape(nr, ns, T, C, nrc, nsc);
-        const int64_t n = nrc * nsc;
+        task_shape(nb, np, T, C, nbc, npc);
+        const int64_t n = nbc * npc;
         if (n == 0) continue;
         int64_t t = toff[g];
         if (t < 0 || t + n > task_cap) { atomicAdd(&gwords[kGErrors], 1ull); continue; }
         for (int64_t c = 0; c < n; ++c, ++t) {
             Task tk;
             tk.join = j;
-            if (nrc == 1) {
-                tk.r_begin = r0; tk.r_len = (uint32_t)nr;
-                tk.s_begin = s0 + c * C; tk.s_len = (uint32_t)min_i64(C, ns - c * C);
-                tk.split = 0;
+            tk.flags = (bs ? kTaskBuildS : 0u) | (nbc > 1 ? kTaskSplit : 0u);
+            if (nbc == 1) {
+                tk.b_begin = b0; tk.b_len = (uint32_t)nb;
+                tk.p_begin = p0 + c * C; tk.p_len = (uint32_t)min_i64(C, np - c * C);
             } else {
-                tk.r_begin = r0 + c * T; tk.r_len = (uint32_t)min_i64(T, nr - c * T);
-                tk.s_begin = s0; tk.s_len = (uint32_t)ns;
-                tk.split = 1;
+                tk.b_begin = b0 + c * T; tk.b_len = (uint32_t)min_i64(T, nb - c * T);
+                tk.p_begin = p0; tk.p_len = (uint32_t)np;
             }
             tasks[t] = tk;
         }
         atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntTasks]), (unsigned long long)n);
-        if (nrc > 1)
+        if (nbc > 1)
             atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSplitTasks]),
                       (unsigned long long)n);
     }
@@ -526,18 +706,28 @@ __device__ __forceinline__ void warp_flush(const JoinDesc& d, const uint32_t* wr
 }
 
 // Persistent probe kernel. Each CTA repeatedly takes the next task, builds a bucketised table of
-// the task's R chunk in shared memory (count per bucket, exclusive scan, place), then streams the
-// S chunk: every S tuple scans its bucket and every key-equal entry is a match. After placement
-// off[b] holds the end of bucket b, so bucket b spans [off[b-1], off[b]).
+// the task's build chunk in shared memory (count per bucket, exclusive scan, place), then streams
+// the other side through it: the streamed tuples arrive in chunks of kChunk by bulk copy (the next
+// chunk in flight while the current one is probed), every streamed tuple scans its bucket, and
+// every key-equal entry is a match. After placement off[b] holds the end of bucket b, so bucket b
+// spans [off[b-1], off[b]).
+constexpr int kChunk = 2048;                                // streamed tuples per bulk copy
+constexpr size_t kChunkBuf = (size_t)(kChunk + 2) * 8;      // one chunk buffer (alignment slack)
+
 __global__ void __launch_bounds__(kThreads, 2)
 k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned long long* gwords,
         int table_cap, int emit_key) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint2* table = reinterpret_cast<uint2*>(smem);                          // [table_cap]
-    uint32_t* off = reinterpret_cast<uint32_t*>(table + table_cap);         // [table_cap] (+pad)
+    unsigned char* sbuf = smem;                                                     // 2 chunk buffers
+    uint2* table = reinterpret_cast<uint2*>(smem + 2 * kChunkBuf);                  // [table_cap]
+    uint32_t* off = reinterpret_cast<uint32_t*>(table + table_cap);                 // [table_cap] (+pad)
     uint32_t* wbuf = off + table_cap + 4;
     __shared__ uint32_t tmp[kThreads / 32];
     __shared__ long long s_task;
+    __shared__ __align__(8) uint64_t bars[2];
+    init_bars(bars);
+    uint32_t ph = 0;
+    unsigned long long* errors = &gwords[kGErrors];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int words_per_warp = kWarpBuf * (emit_key ? 3 : 2);
     uint32_t* wr = wbuf + wid * words_per_warp;
@@ -558,65 +748,80 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
             cur = tk.join;
         }
         const JoinDesc& d = J[tk.join];
-        const uint2* __restrict__ Rb = final_buf(d, 0) + tk.r_begin;
-        const uint2* __restrict__ Sb = final_buf(d, 1) + tk.s_begin;
-        const uint32_t nr = min(tk.r_len, (uint32_t)table_cap);
-        if (tk.r_len > (uint32_t)table_cap && threadIdx.x == 0) atomicAdd(&gwords[kGErrors], 1ull);
+        const bool bs = (tk.flags & kTaskBuildS) != 0;
+        const uint2* __restrict__ Bb = final_buf(d, bs ? 1 : 0) + tk.b_begin;   // build side
+        const uint2* Pb = final_buf(d, bs ? 0 : 1) + tk.p_begin;                // streamed side
+        const uint32_t nr = min(tk.b_len, (uint32_t)table_cap);
+        if (tk.b_len > (uint32_t)table_cap && threadIdx.x == 0) atomicAdd(errors, 1ull);
+        const uint32_t np = tk.p_len;
+        const int nchunks = (int)((np + kChunk - 1) / kChunk);
+        // first streamed chunk flies while the table is built
+        const TileIn pin{Pb, nullptr, nullptr, false};
+        if (threadIdx.x == 0 && nchunks > 0) tile_issue(pin, 0, (int)min(np, (uint32_t)kChunk), sbuf, &bars[0]);
         uint32_t nb = 32;
         while (nb < nr) nb <<= 1;
         const uint32_t mask = nb - 1;
-        // build: count, scan, place
         for (uint32_t i = threadIdx.x; i < nb; i += kThreads) off[i] = 0;
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < nr; i += kThreads)
-            atomicAdd(&off[bucket_of(__ldg(&Rb[i].x), mask)], 1u);
+            atomicAdd(&off[bucket_of(__ldg(&Bb[i].x), mask)], 1u);
         __syncthreads();
         block_scan_excl(off, (int)nb, tmp);
         for (uint32_t i = threadIdx.x; i < nr; i += kThreads) {
-            const uint2 e = __ldg(&Rb[i]);
+            const uint2 e = __ldg(&Bb[i]);
             const uint32_t pos = atomicAdd(&off[bucket_of(e.x, mask)], 1u);
             table[pos] = e;
         }
         __syncthreads();
-        // probe
-        for (uint32_t base = 0; base < tk.s_len; base += kThreads) {
-            const uint32_t i = base + threadIdx.x;
-            uint2 e = make_uint2(0u, 0u);
-            uint32_t lo = 0, hi = 0;
-            if (i < tk.s_len) {
-                e = __ldg(&Sb[i]);
-                const uint32_t b = bucket_of(e.x, mask);
-                lo = b ? off[b - 1] : 0u;
-                hi = off[b];
-            }
-            while (__any_sync(0xffffffffu, lo < hi)) {
-                bool m = false;
-                uint32_t rv = 0;
-                if (lo < hi) {
-                    const uint2 c = table[lo];
-                    m = (c.x == e.x);
-                    rv = c.y;
-                    ++lo;
+        for (int c = 0; c < nchunks; ++c) {
+            const int b = c & 1;
+            const int64_t c0 = (int64_t)c * kChunk;
+            const int cn = (int)min((int64_t)kChunk, (int64_t)np - c0);
+            if (threadIdx.x == 0 && c + 1 < nchunks)
+                tile_issue(pin, c0 + kChunk, (int)min((int64_t)kChunk, (int64_t)np - c0 - kChunk),
+                           sbuf + (b ^ 1) * kChunkBuf, &bars[b ^ 1]);
+            mbar_wait(&bars[b], (ph >> b) & 1u, errors);
+            ph ^= 1u << b;
+            const uint2* chunk = reinterpret_cast<const uint2*>(sbuf + b * kChunkBuf) + tile_mis(pin, c0);
+            for (int base = 0; base < cn; base += kThreads) {
+                const int i = base + (int)threadIdx.x;
+                uint2 e = make_uint2(0u, 0u);
+                uint32_t lo = 0, hi = 0;
+                if (i < cn) {
+                    e = chunk[i];
+                    const uint32_t bk = bucket_of(e.x, mask);
+                    lo = bk ? off[bk - 1] : 0u;
+                    hi = off[bk];
                 }
-                const uint32_t mm = __ballot_sync(0xffffffffu, m);
-                if (mm) {
-                    const int n = __popc(mm);
-                    if (wcount + n > kWarpBuf) {
-                        warp_flush(d, wr, ws, wk, wcount, lane);
-                        wcount = 0;
+                while (__any_sync(0xffffffffu, lo < hi)) {
+                    bool m = false;
+                    uint32_t rv = 0;
+                    if (lo < hi) {
+                        const uint2 cc = table[lo];
+                        m = (cc.x == e.x);
+                        rv = cc.y;
+                        ++lo;
                     }
-                    if (m) {
-                        const int pos = wcount + __popc(mm & lanemask_lt());
-                        wr[pos] = rv;
-                        ws[pos] = e.y;
-                        if (emit_key) wk[pos] = e.x;
+                    const uint32_t mm = __ballot_sync(0xffffffffu, m);
+                    if (mm) {
+                        const int n = __popc(mm);
+                        if (wcount + n > kWarpBuf) {
+                            warp_flush(d, wr, ws, wk, wcount, lane);
+                            wcount = 0;
+                        }
+                        if (m) {
+                            const int pos = wcount + __popc(mm & lanemask_lt());
+                            wr[pos] = bs ? e.y : rv;
+                            ws[pos] = bs ? rv : e.y;
+                            if (emit_key) wk[pos] = e.x;
+                        }
+                        wcount += n;
+                        __syncwarp();
                     }
-                    wcount += n;
-                    __syncwarp();
                 }
             }
+            __syncthreads();  // chunk buffer b is free for the copy issued next iteration
         }
-        __syncthreads();
     }
     if (cur >= 0 && wcount > 0) warp_flush(J[cur], wr, ws, wk, wcount, lane);
 }
@@ -725,12 +930,15 @@ cudaError_t enqueue_scan(const uint32_t* in, int64_t* out, int64_t n, int64_t* t
 }
 
 size_t probe_smem_bytes(int table_cap, int emit_key) {
-    return (size_t)table_cap * 8 + ((size_t)table_cap + 4) * 4 +
+    return 2 * kChunkBuf + (size_t)table_cap * 8 + ((size_t)table_cap + 4) * 4 +
            (size_t)(kThreads / 32) * kWarpBuf * (emit_key ? 3 : 2) * 4;
 }
 
-static size_t l1_scatter_smem() { return (size_t)kTile * 8 + (size_t)kMaxP1 * 8 + (size_t)kMaxP1 * 4; }
-static size_t l2_smem() { return (size_t)kTile * 8 + (size_t)kMaxP2 * 8 + (size_t)kMaxP2 * 4; }
+// Shared memory of the scatter kernels: two bulk-copy tile buffers, the reordered tile, and a
+// cursor and a count per bin.
+static size_t scatter_smem(int max_bins) {
+    return 2 * kTileBuf + (size_t)kTile * 8 + (size_t)max_bins * 12;
+}
 
 static cudaError_t set_smem_attr(const void* fn, size_t bytes) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -745,8 +953,8 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     static thread_local bool attrs_done = false;
     cudaError_t err;
     if (!attrs_done) {
-        if ((err = set_smem_attr((const void*)k_l1_scatter, l1_scatter_smem())) != cudaSuccess) return err;
-        if ((err = set_smem_attr((const void*)k_l2_partition, l2_smem())) != cudaSuccess) return err;
+        if ((err = set_smem_attr((const void*)k_l1_scatter, scatter_smem(kMaxP1))) != cudaSuccess) return err;
+        if ((err = set_smem_attr((const void*)k_l2_partition, scatter_smem(kMaxP2))) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_bloom_build, 200 * 1024)) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_probe, probe_smem_bytes(kMaxTable, 1))) != cudaSuccess)
             return err;
@@ -784,8 +992,8 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             return err;
         mark(m0 + 1);
         if (a.total_slices[rel] > 0) {
-            k_l1_scatter<<<grid_for(a.total_slices[rel], sms, 2), kThreads, l1_scatter_smem(), st>>>(
-                a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords);
+            k_l1_scatter<<<grid_for(a.total_slices[rel], sms, 2), kThreads, scatter_smem(a.max_p1), st>>>(
+                a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
             ++launches;
         }
         mark(m0 + 2);
@@ -795,8 +1003,8 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             ++launches;
         }
         if (a.total_segs > 0) {
-            k_l2_partition<<<grid_for(a.total_segs, sms, 2), kThreads, l2_smem(), st>>>(
-                a.J, a.nj, rel, a.seg_prefix, a.gwords);
+            k_l2_partition<<<grid_for(a.total_segs, sms, 2), kThreads, scatter_smem(a.max_p2), st>>>(
+                a.J, a.nj, rel, a.seg_prefix, a.gwords, a.max_p2);
             ++launches;
         }
         mark(m0 + 3);

@@ -62,8 +62,8 @@ typedef struct brig_join_config {
     int32_t bloom_num_hashes;       /* k (--num_hashes); 0 = round(bits_per_key * ln 2), max 16 */
     double  bloom_bits_per_key;     /* filter size when bloom_num_bits == 0; default 10 */
     int64_t bloom_num_bits;         /* total filter bits (--num_bits); 0 = bits_per_key * |R| */
-    int32_t table_capacity;         /* max R tuples per shared-memory table, power of two in
-                                       [256, 8192]; 0 = 8192 (the reference's HT_SIZE is 10007,
+    int32_t table_capacity;         /* max build-side tuples per shared-memory table, power of two
+                                       in [256, 8192]; 0 = 4096 (the reference's HT_SIZE is 10007,
                                        src/common.h:15) */
     int32_t s_chunk;                /* max S tuples per probe task; 0 = 16384 */
     int32_t emit_key;               /* 1 = also write the key of each pair (GPU_answer array,
@@ -74,7 +74,13 @@ typedef struct brig_join_config {
     int32_t profile_stages;         /* 1 = record a CUDA event after every pipeline stage (read with
                                        brig_join_stage_times); replaces the reference's chrono timers
                                        with forced syncs (src/vlsplit_hash_kernel.cu:36-107) */
-    int32_t reserved[6];
+    int32_t bloom_probe_level;      /* S partition pass that probes the filter: 1 = the first pass
+                                       (the reference's prefilter before S's partitioning,
+                                       src/hash_kernel.cu:935-954), 2 = the second pass, where each
+                                       level-1 partition's filter segments stay in L2 (needs two
+                                       partition levels); 0 = auto: 1 while the whole filter fits
+                                       comfortably in L2, else 2 */
+    int32_t reserved[5];
 } brig_join_config;
 
 /* Output of one join. Pairs are written in an unspecified order; the multiset is exact. When the

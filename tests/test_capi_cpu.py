@@ -23,16 +23,17 @@ def test_config_defaults(bj):
     assert cfg.abi_version == bj.ABI_VERSION
     assert cfg.partition_mode == bj.PART_HASH
     assert cfg.bloom_bits_per_key == 10.0 and cfg.use_bloom == 0 and cfg.device == -1
-    assert C.sizeof(bj.Config) == 88
+    assert C.sizeof(bj.Config) == 88  # layout of brig_join_config
 
 
 @pytest.mark.parametrize("n_r,n_s,kw,expect", [
-    (1 << 24, 1 << 24, {}, (4096, 1)),
-    (640_000_000, 640_000_000, {"use_bloom": 1}, (2048, 64)),
-    (1 << 26, 1 << 30, {"use_bloom": 1}, (2048, 8)),
+    (1 << 24, 1 << 24, {}, (512, 16)),
+    (640_000_000, 640_000_000, {"use_bloom": 1}, (512, 512)),
+    (1 << 26, 1 << 30, {"use_bloom": 1}, (512, 64)),
     (1 << 24, 1 << 24, {"partition_mode": 1, "partition_size": 512}, (512, 67)),
-    (640_000_000, 640_000_000, {"partition_mode": 1, "partition_size": 512}, (512, 205)),
-    (4096, 16384, {}, (1, 1)),
+    (640_000_000, 640_000_000, {"partition_mode": 1, "partition_size": 512}, (512, 407)),
+    (4096, 16384, {}, (2, 1)),
+    (3000, 16384, {}, (1, 1)),
     (0, 0, {}, (1, 1)),
 ])
 def test_planner_fanouts(bj, n_r, n_s, kw, expect):

@@ -26,6 +26,16 @@ def test_uniform_hash(bj, oracle, torch_cuda, n, bloom):
         assert st.count <= st.s_survivors < n
 
 
+@pytest.mark.parametrize("level", [1, 2])
+@pytest.mark.parametrize("mode,p1,p2", [(0, 16, 16), (0, 64, 64), (1, 100, 7), (1, 512, 67)])
+def test_bloom_probe_levels(bj, oracle, torch_cuda, level, mode, p1, p2):
+    """The filter probed in S's first partition pass or fused into its second pass."""
+    rk, rv, sk, sv = bj.gen_host(31 + level, 400_000, 600_000, 0.05)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=1, bloom_probe_level=level,
+                 partition_mode=mode, partition_size=p1, second_partition_size=p2)
+    assert st.count == 30_000 and st.count <= st.s_survivors < 600_000 // 4
+
+
 @pytest.mark.parametrize("p1,p2", [(16, 16), (64, 8), (1, 1), (4096, 1), (2, 1024)])
 def test_two_level_hash_fanouts(bj, oracle, torch_cuda, p1, p2):
     rk, rv, sk, sv = bj.gen_host(11, 300_000, 200_000, 0.3)
