@@ -191,6 +191,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--bloom", type=int, default=None, help="override Bloom on/off")
+    ap.add_argument("--bloom-level", type=int, default=0,
+                    help="S pass that probes the filter (1 first, 2 second, 0 planner's choice)")
     args = ap.parse_args()
     if args.steps > 64:
         ap.error("--steps above 64: per-stage events keep the last 64 runs")
@@ -228,7 +230,7 @@ def main():
     out_r = torch.empty(cap, dtype=i32, device="cuda")
     out_s = torch.empty(cap, dtype=i32, device="cuda")
     j = bj.Join(use_bloom=wl["bloom"], bloom_bits_per_key=wl["bpk"], bloom_num_hashes=wl["k"],
-                use_cuda_graph=1, profile_stages=1)
+                bloom_probe_level=args.bloom_level, use_cuda_graph=1, profile_stages=1)
 
     def step():
         j.run(rk, rv, nr, sk, sv, ns, out_r, out_s, cap, stream=sp)
