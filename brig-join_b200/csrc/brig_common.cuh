@@ -23,6 +23,7 @@ constexpr int kMaxP1 = 4096;          // first-level fan-out (the reference caps
 constexpr int kMaxP2 = 1024;          // second-level fan-out (SECOND_PASS_MAX=4096, :14)
 constexpr int kMaxTable = 8192;       // build-side tuples per shared-memory table (largest allowed)
 constexpr int kDefaultTable = 4096;   // default table capacity
+constexpr int kDefaultChunk = 65536;  // default streamed tuples per probe task
 constexpr int kMinTable = 256;
 constexpr int kMaxBloomK = 16;
 constexpr int kThreads = 512;         // threads per CTA of every partition and probe kernel
@@ -166,7 +167,10 @@ struct JoinDesc {
     int32_t bloom_k;
     int32_t bloom_level;   // S pass that probes the filter: 1 first (fused with the histogram of
                            // S's level-1 pass), 2 second (fused with S's level-2 pass)
-    int64_t fine_base;     // offset of this join's P1*P2 entries in the global task-count array
+    int32_t bloom_group;   // consecutive finest partitions per Bloom build CTA
+    int32_t pad0;
+    int64_t dom_base;      // offset of this join's task domains in the global task-count array
+    int64_t fine_base;     // unused (kept zero)
     int32_t table_cap;     // max build-side tuples per probe task
     int32_t s_chunk;       // max streamed tuples per probe task
 };

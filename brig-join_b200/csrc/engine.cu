@@ -97,6 +97,8 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
         p.bloom = true;
         p.k = k;
         p.bloom_bits = p.nfine * (int64_t)p.seg_blocks * 256;
+        const int64_t nw = (int64_t)p.seg_blocks * 8;
+        p.bloom_group = nw <= kBloomSmemWords ? (int)std::min<int64_t>(kBloomSmemWords / nw, p.nfine) : 1;
         // Probing in S's first pass reads one random 32-byte block per S tuple; that is cheap only
         // while the filter stays in the 126 MB L2. A larger filter is probed in S's second pass,
         // one level-1 partition (a contiguous run of segments) at a time.
@@ -139,7 +141,7 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
     sl = std::max<int64_t>(sl, 4 * kTile);
     sh.slice_len = sl;
     const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
-    const int C = cfg.s_chunk > 0 ? cfg.s_chunk : 16384;
+    const int C = cfg.s_chunk > 0 ? cfg.s_chunk : kDefaultChunk;
     Layout L;
     for (int j = 0; j < nj; ++j) {
         const JoinPlan& p = plans[j];
@@ -167,12 +169,18 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
         if (p.bloom) {
             o.bloom = L.take((size_t)p.nfine * p.seg_blocks * 32);
             sh.any_bloom = true;
-            sh.total_bloom_fine += p.nfine;
-            sh.max_seg_words = std::max<int>(sh.max_seg_words, (int)(p.seg_blocks * 8));
+            sh.total_bloom_groups += (p.nfine + p.bloom_group - 1) / p.bloom_group;
+            const int64_t nw = (int64_t)p.seg_blocks * 8;
+            sh.max_seg_words = std::max<int>(sh.max_seg_words, (int)nw);
+            if (nw <= kBloomSmemWords)
+                sh.bloom_smem_words = std::max<int>(sh.bloom_smem_words, (int)(nw * p.bloom_group));
         }
         if (two) sh.total_segs += p.pf.P1;
         sh.total_fine += p.nfine;
-        sh.task_cap += p.nfine + p.nr / T + p.ns / C + 2;
+        sh.total_domains += two ? p.pf.P1 : 1;
+        // Grouped tasks per domain: at most one group per finest partition, plus one task per
+        // streamed chunk, plus the split chunks of oversized partitions.
+        sh.task_cap += 2 * p.nfine + (p.nr + p.ns) / C + (p.nr + p.ns) / T + 4;
     }
     // Histograms: all R regions, then all S regions (each scanned as one sequence).
     for (int r = 0; r < 2; ++r) {
@@ -187,11 +195,11 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
     const int64_t hist_total = sh.hist_len[0] + sh.hist_len[1];
     sh.hist = L.take((size_t)hist_total * 4);
     sh.hist_scan = L.take((size_t)hist_total * 8);
-    sh.tcount = L.take(((size_t)sh.total_fine + 1) * 4);
-    sh.toff = L.take(((size_t)sh.total_fine + 1) * 8);
+    sh.tcount = L.take(((size_t)sh.total_domains + 1) * 4);
+    sh.toff = L.take(((size_t)sh.total_domains + 1) * 8);
     sh.tasks = L.take((size_t)sh.task_cap * sizeof(Task));
     sh.scan_tmp_len = std::max(scan_tmp_words(std::max(sh.hist_len[0], sh.hist_len[1])),
-                               scan_tmp_words(sh.total_fine + 1));
+                               scan_tmp_words(sh.total_domains + 1));
     sh.scan_tmp = L.take((size_t)sh.scan_tmp_len * 8);
     sh.gwords = L.take(kGWords * 8);
     sh.counters = L.take((size_t)nj * kCntWords * 8);
@@ -333,7 +341,7 @@ void Engine::ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key) {
 void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const JoinIO* joins, int nj,
                    const Shape& sh, char* ws, char* meta_host, int num_sms, PipelineArgs& a) {
     const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
-    const int C = cfg.s_chunk > 0 ? cfg.s_chunk : 16384;
+    const int C = cfg.s_chunk > 0 ? cfg.s_chunk : kDefaultChunk;
     if (T < kMinTable || T > kMaxTable || !is_pow2(T))
         fail(BRIG_E_INVALID, "table_capacity must be a power of two in [256, 8192]");
     if (C < 1) fail(BRIG_E_INVALID, "s_chunk must be >= 1");
@@ -344,7 +352,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     int64_t* segp = hpre + 2 * (nj + 1);
     int64_t* finep = hpre + 3 * (nj + 1);
     int64_t* bloomp = hpre + 4 * (nj + 1);
-    sp0[0] = sp1[0] = segp[0] = finep[0] = bloomp[0] = 0;
+    sp0[0] = sp1[0] = segp[0] = finep[0] = bloomp[0] = 0;  // finep: task domains
     int64_t* counters = reinterpret_cast<int64_t*>(ws + sh.counters);
     for (int j = 0; j < nj; ++j) {
         const JoinPlan& p = plans[j];
@@ -383,15 +391,17 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
         d.seg_blocks = p.seg_blocks;
         d.bloom_k = p.k;
         d.bloom_level = p.bloom_level;
-        d.fine_base = finep[j];
+        d.fine_base = 0;
+        d.dom_base = finep[j];
+        d.bloom_group = p.bloom_group;
         d.table_cap = T;
         d.s_chunk = C;
         hJ[j] = d;
         sp0[j + 1] = sp0[j] + o.rel[0].nslices;
         sp1[j + 1] = sp1[j] + o.rel[1].nslices;
         segp[j + 1] = segp[j] + (p.pf.P2 > 1 ? p.pf.P1 : 0);
-        finep[j + 1] = finep[j] + p.nfine;
-        bloomp[j + 1] = bloomp[j] + (p.bloom ? p.nfine : 0);
+        finep[j + 1] = finep[j] + (p.pf.P2 > 1 ? p.pf.P1 : 1);
+        bloomp[j + 1] = bloomp[j] + (p.bloom ? (p.nfine + p.bloom_group - 1) / p.bloom_group : 0);
     }
     char* meta = ws + sh.meta;
     const int64_t* dpre = reinterpret_cast<const int64_t*>(meta + (size_t)nj * sizeof(JoinDesc));
@@ -401,13 +411,16 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     a.slice_prefix[0] = dpre;
     a.slice_prefix[1] = dpre + (nj + 1);
     a.seg_prefix = dpre + 2 * (nj + 1);
-    a.fine_prefix = dpre + 3 * (nj + 1);
+    a.fine_prefix = nullptr;
+    a.dom_prefix = dpre + 3 * (nj + 1);
     a.bloom_prefix = dpre + 4 * (nj + 1);
     a.total_slices[0] = sh.total_slices[0];
     a.total_slices[1] = sh.total_slices[1];
     a.total_segs = sh.total_segs;
     a.total_fine = sh.total_fine;
-    a.total_bloom_fine = sh.total_bloom_fine;
+    a.total_bloom_groups = sh.total_bloom_groups;
+    a.total_domains = sh.total_domains;
+    a.bloom_smem_words = sh.bloom_smem_words;
     a.hist_begin[0] = 0;
     a.hist_len[0] = sh.hist_len[0];
     a.hist_begin[1] = sh.hist_len[0];

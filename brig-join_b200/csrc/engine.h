@@ -30,6 +30,7 @@ struct JoinPlan {
     int64_t nfine = 1;
     bool bloom = false;
     int bloom_level = 0;        // S pass that probes the filter (1 or 2)
+    int bloom_group = 1;        // consecutive finest partitions per Bloom build CTA
     int k = 0;
     uint32_t seg_blocks = 0;
     int64_t bloom_bits = 0;     // allocated bits
@@ -61,14 +62,14 @@ struct Shape {
     int64_t slice_len = 0;
     int64_t hist_len[2] = {0, 0};
     int64_t total_slices[2] = {0, 0};
-    int64_t total_segs = 0, total_fine = 0, total_bloom_fine = 0;
+    int64_t total_segs = 0, total_fine = 0, total_bloom_groups = 0, total_domains = 0;
     int64_t task_cap = 0;
     size_t hist = 0, hist_scan = 0, tcount = 0, toff = 0, tasks = 0, scan_tmp = 0, gwords = 0,
            counters = 0, meta = 0;
     int64_t scan_tmp_len = 0;
     size_t meta_bytes = 0;      // descriptor image: nj JoinDesc + 5 prefix arrays of nj+1 int64
     size_t total = 0;           // workspace bytes
-    int max_p1 = 1, max_p2 = 1, max_seg_words = 0;
+    int max_p1 = 1, max_p2 = 1, max_seg_words = 0, bloom_smem_words = 0;
     bool any_bloom = false;
 };
 

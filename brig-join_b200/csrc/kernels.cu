@@ -299,17 +299,22 @@ __device__ __forceinline__ void init_bars(uint64_t* bars) {
     __syncthreads();
 }
 
-// Bloom test of one key against the segment of its finest partition f.
-__device__ __forceinline__ bool bloom_test(const JoinDesc& d, uint32_t f, uint32_t key) {
+// Bloom probe, split in two so a thread can have several block loads in flight: the address of a
+// key's 32-byte block in the segment of its finest partition f, then the test of the loaded words.
+__device__ __forceinline__ const uint4* bloom_block(const JoinDesc& d, uint32_t f, uint32_t key) {
     BloomKey bk;
     bloom_key(key, d.seg_blocks, d.bloom_k, bk);
-    const uint4* blk = reinterpret_cast<const uint4*>(d.bloom + ((int64_t)f * d.seg_blocks + bk.block) * 8);
-    const uint4 w0 = __ldg(blk), w1 = __ldg(blk + 1);
+    return reinterpret_cast<const uint4*>(d.bloom + ((int64_t)f * d.seg_blocks + bk.block) * 8);
+}
+__device__ __forceinline__ bool bloom_words_pass(uint32_t key, uint32_t seg_blocks, int k, uint4 w0, uint4 w1) {
+    BloomKey bk;
+    bloom_key(key, seg_blocks, k, bk);
     return ((w0.x & bk.mask[0]) == bk.mask[0]) && ((w0.y & bk.mask[1]) == bk.mask[1]) &&
            ((w0.z & bk.mask[2]) == bk.mask[2]) && ((w0.w & bk.mask[3]) == bk.mask[3]) &&
            ((w1.x & bk.mask[4]) == bk.mask[4]) && ((w1.y & bk.mask[5]) == bk.mask[5]) &&
            ((w1.z & bk.mask[6]) == bk.mask[6]) && ((w1.w & bk.mask[7]) == bk.mask[7]);
 }
+constexpr int kProbeILP = 4;  // keys per thread with their filter blocks in flight together
 
 // ---------------------------------------------------------------------------------------------
 // Level 1, pass 1: per-slice histogram over P1 partitions (R, or S without Bloom), or the fused
@@ -360,25 +365,38 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             // compacted (key, value) into R.cmp[b, b + count) and counted per level-1 partition.
             const uint32_t* __restrict__ key = R.key;
             const uint32_t* __restrict__ val = R.val;
-            for (int64_t i0 = b; i0 < e; i0 += kThreads) {
-                const int64_t i = i0 + threadIdx.x;
-                bool pass = false;
-                uint32_t kk = 0, p = 0;
-                if (i < e) {
-                    kk = __ldcs(key + i);
-                    p = part1(pf, kk);
-                    pass = bloom_test(d, p * pf.P2 + part2(pf, kk), kk);
+            for (int64_t i0 = b; i0 < e; i0 += kProbeILP * kThreads) {
+                uint32_t kk[kProbeILP];
+                uint4 w0[kProbeILP], w1[kProbeILP];
+#pragma unroll
+                for (int u = 0; u < kProbeILP; ++u) {
+                    const int64_t i = i0 + u * kThreads + threadIdx.x;
+                    kk[u] = i < e ? __ldcs(key + i) : 0u;
                 }
-                const uint32_t m = __ballot_sync(0xffffffffu, pass);
-                if (m) {
-                    uint32_t base = 0;
-                    if (lane == 0) base = atomicAdd(&s_cursor, (uint32_t)__popc(m));
-                    base = __shfl_sync(0xffffffffu, base, 0);
-                    if (pass) {
-                        atomicAdd(&sh_cnt[p], 1u);
-                        const int64_t dst = b + base + __popc(m & lanemask_lt());
-                        if (dst < e) R.cmp[dst] = make_uint2(kk, __ldg(val + i));
-                        else atomicAdd(&gwords[kGErrors], 1ull);
+#pragma unroll
+                for (int u = 0; u < kProbeILP; ++u) {
+                    const int64_t i = i0 + u * kThreads + threadIdx.x;
+                    if (i < e) {
+                        const uint4* blk = bloom_block(d, part1(pf, kk[u]) * pf.P2 + part2(pf, kk[u]), kk[u]);
+                        w0[u] = __ldg(blk);
+                        w1[u] = __ldg(blk + 1);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kProbeILP; ++u) {
+                    const int64_t i = i0 + u * kThreads + threadIdx.x;
+                    const bool pass = i < e && bloom_words_pass(kk[u], d.seg_blocks, d.bloom_k, w0[u], w1[u]);
+                    const uint32_t m = __ballot_sync(0xffffffffu, pass);
+                    if (m) {
+                        uint32_t base = 0;
+                        if (lane == 0) base = atomicAdd(&s_cursor, (uint32_t)__popc(m));
+                        base = __shfl_sync(0xffffffffu, base, 0);
+                        if (pass) {
+                            atomicAdd(&sh_cnt[part1(pf, kk[u])], 1u);
+                            const int64_t dst = b + base + __popc(m & lanemask_lt());
+                            if (dst < e) R.cmp[dst] = make_uint2(kk[u], __ldg(val + i));
+                            else atomicAdd(&gwords[kGErrors], 1ull);
+                        }
                     }
                 }
             }
@@ -507,26 +525,38 @@ k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* _
             // contiguous and stay in L2 while the CTA works on it. Survivors are compacted into
             // cmp[begin, begin + survivors) and counted by level-2 id.
             const int lane = threadIdx.x & 31;
-            for (int64_t i0 = begin; i0 < end; i0 += kThreads) {
-                const int64_t i = i0 + threadIdx.x;
-                bool pass = false;
-                uint2 e = make_uint2(0u, 0u);
-                uint32_t q = 0;
-                if (i < end) {
-                    e = __ldcs(&R.l1[i]);
-                    q = bin(e.x);
-                    pass = bloom_test(d, p * P2 + q, e.x);
+            for (int64_t i0 = begin; i0 < end; i0 += kProbeILP * kThreads) {
+                uint2 e[kProbeILP];
+                uint4 w0[kProbeILP], w1[kProbeILP];
+#pragma unroll
+                for (int u = 0; u < kProbeILP; ++u) {
+                    const int64_t i = i0 + u * kThreads + threadIdx.x;
+                    e[u] = i < end ? __ldcs(&R.l1[i]) : make_uint2(0u, 0u);
                 }
-                const uint32_t m = __ballot_sync(0xffffffffu, pass);
-                if (m) {
-                    uint32_t base = 0;
-                    if (lane == 0) base = atomicAdd(&s_surv, (uint32_t)__popc(m));
-                    base = __shfl_sync(0xffffffffu, base, 0);
-                    if (pass) {
-                        atomicAdd(&cnt[q], 1u);
-                        const int64_t dst = begin + base + __popc(m & lanemask_lt());
-                        if (dst < end) R.cmp[dst] = e;
-                        else atomicAdd(&gwords[kGErrors], 1ull);
+#pragma unroll
+                for (int u = 0; u < kProbeILP; ++u) {
+                    const int64_t i = i0 + u * kThreads + threadIdx.x;
+                    if (i < end) {
+                        const uint4* blk = bloom_block(d, p * P2 + bin(e[u].x), e[u].x);
+                        w0[u] = __ldg(blk);
+                        w1[u] = __ldg(blk + 1);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kProbeILP; ++u) {
+                    const int64_t i = i0 + u * kThreads + threadIdx.x;
+                    const bool pass = i < end && bloom_words_pass(e[u].x, d.seg_blocks, d.bloom_k, w0[u], w1[u]);
+                    const uint32_t m = __ballot_sync(0xffffffffu, pass);
+                    if (m) {
+                        uint32_t base = 0;
+                        if (lane == 0) base = atomicAdd(&s_surv, (uint32_t)__popc(m));
+                        base = __shfl_sync(0xffffffffu, base, 0);
+                        if (pass) {
+                            atomicAdd(&cnt[bin(e[u].x)], 1u);
+                            const int64_t dst = begin + base + __popc(m & lanemask_lt());
+                            if (dst < end) R.cmp[dst] = e[u];
+                            else atomicAdd(&gwords[kGErrors], 1ull);
+                        }
                     }
                 }
             }
@@ -557,127 +587,171 @@ k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* _
     }
 }
 
-// Bloom build: one CTA per finest partition of a Bloom-enabled join. The segment is built in shared
-// memory with 32-bit atomicOr and written out whole (so the filter needs no clearing); segments too
-// large for shared memory are built with global atomicOr.
+// Bloom build: one CTA per group of G consecutive finest partitions of a Bloom-enabled join
+// (G = JoinDesc::bloom_group, chosen so the group's segments fit in shared memory). The group's R
+// tuples are contiguous in the final R buffer; every key sets its bits with 32-bit atomicOr in the
+// shared-memory copy of its segment, and the segments are written out whole, so the filter needs
+// no clearing. A segment too large for shared memory (G = 1 then) is built with global atomicOr.
 __global__ void __launch_bounds__(kThreads)
 k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ bloom_prefix,
-              int smem_words) {
+              int smem_words, unsigned long long* gwords) {
     extern __shared__ uint32_t seg[];
     const int64_t total = bloom_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(bloom_prefix, nj, g);
         const JoinDesc& d = J[j];
-        const int64_t f = g - bloom_prefix[j];
         const RelPlan& R = d.rel[0];
+        const int64_t nfine = (int64_t)d.pf.P1 * d.pf.P2;
+        const int64_t f0 = (g - bloom_prefix[j]) * d.bloom_group;
+        const int64_t f1 = min_i64(f0 + d.bloom_group, nfine);
         const uint2* buf = final_buf(d, 0);
-        const int64_t begin = R.bounds[f], end = R.bounds[f + 1];
+        const int64_t begin = R.bounds[f0], end = R.bounds[f1];
         const uint32_t nw = d.seg_blocks * 8;
-        uint32_t* gseg = d.bloom + f * (int64_t)nw;
+        const int64_t words = (f1 - f0) * (int64_t)nw;
+        uint32_t* gseg = d.bloom + f0 * (int64_t)nw;
         const int k = d.bloom_k;
-        if ((int)nw <= smem_words) {
-            for (uint32_t w = threadIdx.x; w < nw; w += kThreads) seg[w] = 0;
-            __syncthreads();
-            for (int64_t i = begin + threadIdx.x; i < end; i += kThreads) {
+        const bool in_smem = words <= smem_words;
+        uint32_t* dst = in_smem ? seg : gseg;
+        for (int64_t w = threadIdx.x; w < words; w += kThreads) dst[w] = 0;
+        __syncthreads();
+        for (int64_t i0 = begin; i0 < end; i0 += kProbeILP * kThreads) {
+            uint32_t kk[kProbeILP];
+#pragma unroll
+            for (int u = 0; u < kProbeILP; ++u) {
+                const int64_t i = i0 + u * kThreads + threadIdx.x;
+                kk[u] = i < end ? __ldcs(&buf[i].x) : 0u;
+            }
+#pragma unroll
+            for (int u = 0; u < kProbeILP; ++u) {
+                const int64_t i = i0 + u * kThreads + threadIdx.x;
+                if (i >= end) continue;
+                const int64_t local = (int64_t)part_fine(d.pf, kk[u]) - f0;
+                if (local < 0 || local >= f1 - f0) {
+                    atomicAdd(&gwords[kGErrors], 1ull);
+                    continue;
+                }
                 BloomKey bk;
-                bloom_key(__ldg(&buf[i].x), d.seg_blocks, k, bk);
-                uint32_t* blk = seg + bk.block * 8;
+                bloom_key(kk[u], d.seg_blocks, k, bk);
+                uint32_t* blk = dst + local * nw + (int64_t)bk.block * 8;
 #pragma unroll
                 for (int w = 0; w < 8; ++w)
                     if (bk.mask[w]) atomicOr(blk + w, bk.mask[w]);
             }
-            __syncthreads();
-            for (uint32_t w = threadIdx.x; w < nw; w += kThreads) gseg[w] = seg[w];
-            __syncthreads();
-        } else {
-            for (uint32_t w = threadIdx.x; w < nw; w += kThreads) gseg[w] = 0;
-            __syncthreads();
-            for (int64_t i = begin + threadIdx.x; i < end; i += kThreads) {
-                BloomKey bk;
-                bloom_key(__ldg(&buf[i].x), d.seg_blocks, k, bk);
-                uint32_t* blk = gseg + (int64_t)bk.block * 8;
-#pragma unroll
-                for (int w = 0; w < 8; ++w)
-                    if (bk.mask[w]) atomicOr(blk + w, bk.mask[w]);
-            }
+        }
+        __syncthreads();
+        if (in_smem) {
+            for (int64_t w = threadIdx.x; w < words; w += kThreads) gseg[w] = seg[w];
             __syncthreads();
         }
     }
 }
 
-// Probe tasks per finest partition. The smaller of the two partitions is the build side. A build
-// side of at most table_cap tuples is built once per streamed chunk of s_chunk tuples (so a hot
-// partition spreads over many CTAs); a larger one is cut into table_cap chunks, each streamed
-// against the whole other side (the exact form of the reference's split path, which stops at the
-// first match, src/kernel_functions.cu:356-395).
+// Probe tasks. A task domain is one level-1 partition (two-level plans) or the whole join
+// (one-level plans); inside a domain the finest partitions of each side are adjacent in memory.
+// The smaller side of the domain is the build side. Consecutive finest partitions are grouped into
+// one task until their build sides would exceed table_cap tuples: keys of different partitions
+// never match, so one table over the group is exact, and fewer, larger tasks amortise the per-task
+// table set-up. A group's streamed side is cut into chunks of s_chunk tuples, each a task of its
+// own (a hot partition spreads over many CTAs). A single partition whose build side exceeds
+// table_cap is cut into table_cap chunks, each streamed against the partition's whole other side:
+// the exact form of the reference's split path, which stops at the first match
+// (src/kernel_functions.cu:356-395).
 __device__ __forceinline__ void fine_range(const RelPlan& R, int64_t f, int64_t& begin, int64_t& n) {
     begin = R.bounds[f];
     n = R.fine_cnt ? (int64_t)R.fine_cnt[f] : R.bounds[f + 1] - begin;
 }
 
-__device__ __forceinline__ void task_shape(int64_t nb, int64_t np, int64_t T, int64_t C, int64_t& nbc,
-                                           int64_t& npc) {
-    if (nb == 0 || np == 0) { nbc = 0; npc = 0; return; }
-    nbc = (nb + T - 1) / T;
-    npc = nbc == 1 ? (np + C - 1) / C : 1;
+// Walks domain `dom` of join d and calls emit(b_begin, b_len, p_begin, p_len, split, build_s)
+// for every task, in order.
+template <class Emit>
+__device__ void walk_domain(const JoinDesc& d, int64_t dom, Emit&& emit) {
+    const int64_t P2 = d.pf.P2;
+    const int64_t f_first = P2 > 1 ? dom * P2 : 0;
+    const int64_t f_last = P2 > 1 ? f_first + P2 : (int64_t)d.pf.P1;
+    int64_t tot_r = 0, tot_s = 0;
+    for (int64_t f = f_first; f < f_last; ++f) {
+        int64_t b, n;
+        fine_range(d.rel[0], f, b, n);
+        tot_r += n;
+        fine_range(d.rel[1], f, b, n);
+        tot_s += n;
+    }
+    if (tot_r == 0 || tot_s == 0) return;
+    const bool bs = tot_s < tot_r;
+    const RelPlan& B = d.rel[bs ? 1 : 0];
+    const RelPlan& P = d.rel[bs ? 0 : 1];
+    const int64_t T = d.table_cap, C = d.s_chunk;
+    int64_t gb0 = -1, gp0 = -1, nb = 0, np = 0;
+    auto close = [&]() {
+        if (nb > 0 && np > 0)
+            for (int64_t c = 0; c * C < np; ++c) emit(gb0, nb, gp0 + c * C, min_i64(C, np - c * C), false, bs);
+        gb0 = -1;
+        nb = 0;
+        np = 0;
+    };
+    for (int64_t f = f_first; f < f_last; ++f) {
+        int64_t bb, bn, pb, pn;
+        fine_range(B, f, bb, bn);
+        fine_range(P, f, pb, pn);
+        if (bn > T) {
+            close();
+            if (pn > 0)
+                for (int64_t c = 0; c * T < bn; ++c) emit(bb + c * T, min_i64(T, bn - c * T), pb, pn, true, bs);
+            continue;
+        }
+        if (nb + bn > T) close();
+        if (gb0 < 0) {
+            gb0 = bb;
+            gp0 = pb;
+        }
+        nb += bn;
+        np += pn;
+    }
+    close();
 }
 
-__global__ void k_tasks_count(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ fine_prefix,
+__global__ void k_tasks_count(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ dom_prefix,
                               uint32_t* __restrict__ tcount) {
-    const int64_t total = fine_prefix[nj];
+    const int64_t total = dom_prefix[nj];
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= total;
          g += (int64_t)gridDim.x * blockDim.x) {
         if (g == total) { tcount[g] = 0; continue; }
-        const int j = find_owner(fine_prefix, nj, g);
-        const JoinDesc& d = J[j];
-        const int64_t f = g - fine_prefix[j];
-        int64_t r0, nr, s0, ns, nbc, npc;
-        fine_range(d.rel[0], f, r0, nr);
-        fine_range(d.rel[1], f, s0, ns);
-        const bool bs = ns < nr;
-        task_shape(bs ? ns : nr, bs ? nr : ns, d.table_cap, d.s_chunk, nbc, npc);
-        tcount[g] = (uint32_t)(nbc * npc);
+        const int j = find_owner(dom_prefix, nj, g);
+        uint32_t n = 0;
+        walk_domain(J[j], g - dom_prefix[j], [&](int64_t, int64_t, int64_t, int64_t, bool, bool) { ++n; });
+        tcount[g] = n;
     }
 }
 
-__global__ void k_tasks_write(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ fine_prefix,
+__global__ void k_tasks_write(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ dom_prefix,
                               const int64_t* __restrict__ toff, Task* __restrict__ tasks, int64_t task_cap,
                               unsigned long long* gwords) {
-    const int64_t total = fine_prefix[nj];
+    const int64_t total = dom_prefix[nj];
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total;
          g += (int64_t)gridDim.x * blockDim.x) {
-        const int j = find_owner(fine_prefix, nj, g);
+        const int j = find_owner(dom_prefix, nj, g);
         const JoinDesc& d = J[j];
-        const int64_t f = g - fine_prefix[j];
-        int64_t r0, nr, s0, ns, nbc, npc;
-        fine_range(d.rel[0], f, r0, nr);
-        fine_range(d.rel[1], f, s0, ns);
-        const bool bs = ns < nr;
-        const int64_t b0 = bs ? s0 : r0, nb = bs ? ns : nr;
-        const int64_t p0 = bs ? r0 : s0, np = bs ? nr : ns;
-        const int64_t T = d.table_cap, C = d.s_chunk;
-        task_shape(nb, np, T, C, nbc, npc);
-        const int64_t n = nbc * npc;
-        if (n == 0) continue;
         int64_t t = toff[g];
-        if (t < 0 || t + n > task_cap) { atomicAdd(&gwords[kGErrors], 1ull); continue; }
-        for (int64_t c = 0; c < n; ++c, ++t) {
+        int64_t n = 0, nsplit = 0;
+        walk_domain(d, g - dom_prefix[j], [&](int64_t b0, int64_t bn, int64_t p0, int64_t pn, bool split, bool bs) {
+            if (t < 0 || t >= task_cap) {
+                atomicAdd(&gwords[kGErrors], 1ull);
+                return;
+            }
             Task tk;
             tk.join = j;
-            tk.flags = (bs ? kTaskBuildS : 0u) | (nbc > 1 ? kTaskSplit : 0u);
-            if (nbc == 1) {
-                tk.b_begin = b0; tk.b_len = (uint32_t)nb;
-                tk.p_begin = p0 + c * C; tk.p_len = (uint32_t)min_i64(C, np - c * C);
-            } else {
-                tk.b_begin = b0 + c * T; tk.b_len = (uint32_t)min_i64(T, nb - c * T);
-                tk.p_begin = p0; tk.p_len = (uint32_t)np;
-            }
-            tasks[t] = tk;
-        }
-        atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntTasks]), (unsigned long long)n);
-        if (nbc > 1)
-            atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSplitTasks]),
-                      (unsigned long long)n);
+            tk.flags = (bs ? kTaskBuildS : 0u) | (split ? kTaskSplit : 0u);
+            tk.b_begin = b0;
+            tk.b_len = (uint32_t)bn;
+            tk.p_begin = p0;
+            tk.p_len = (uint32_t)pn;
+            tasks[t++] = tk;
+            ++n;
+            nsplit += split ? 1 : 0;
+        });
+        if (n) atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntTasks]), (unsigned long long)n);
+        if (nsplit)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSplitTasks]), (unsigned long long)nsplit);
     }
 }
 
@@ -955,7 +1029,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     if (!attrs_done) {
         if ((err = set_smem_attr((const void*)k_l1_scatter, scatter_smem(kMaxP1))) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_l2_partition, scatter_smem(kMaxP2))) != cudaSuccess) return err;
-        if ((err = set_smem_attr((const void*)k_bloom_build, 200 * 1024)) != cudaSuccess) return err;
+        if ((err = set_smem_attr((const void*)k_bloom_build, kBloomSmemWords * 4)) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_probe, probe_smem_bytes(kMaxTable, 1))) != cudaSuccess)
             return err;
         attrs_done = true;
@@ -972,11 +1046,11 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
 
     // ---- R: level 1 -------------------------------------------------------------------------
     for (int rel = 0; rel < 2; ++rel) {
-        if (rel == 1 && a.any_bloom && a.total_bloom_fine > 0) {
+        if (rel == 1 && a.any_bloom && a.total_bloom_groups > 0) {
             // Bloom filter over the final R partitions, before S's first pass probes it.
-            const int smem_words = std::min(a.max_seg_words, 200 * 1024 / 4);
-            k_bloom_build<<<grid_for(a.total_bloom_fine, sms, 4), kThreads,
-                            (size_t)smem_words * 4, st>>>(a.J, a.nj, a.bloom_prefix, smem_words);
+            k_bloom_build<<<grid_for(a.total_bloom_groups, sms, 4), kThreads,
+                            (size_t)a.bloom_smem_words * 4, st>>>(a.J, a.nj, a.bloom_prefix,
+                                                                  a.bloom_smem_words, a.gwords);
             ++launches;
         }
         if (rel == 1) mark(5);
@@ -1011,14 +1085,14 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     }
     // ---- tasks --------------------------------------------------------------------------------
     {
-        const int64_t n = a.total_fine + 1;
-        const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8);
-        k_tasks_count<<<blocks, 256, 0, st>>>(a.J, a.nj, a.fine_prefix, a.tcount);
+        const int64_t n = a.total_domains + 1;
+        const int blocks = (int)std::min<int64_t>((n + 127) / 128, (int64_t)sms * 8);
+        k_tasks_count<<<blocks, 128, 0, st>>>(a.J, a.nj, a.dom_prefix, a.tcount);
         ++launches;
         if ((err = enqueue_scan(a.tcount, a.toff, n, a.scan_tmp,
                                 reinterpret_cast<int64_t*>(a.gwords + kGTasks), st)) != cudaSuccess)
             return err;
-        k_tasks_write<<<blocks, 256, 0, st>>>(a.J, a.nj, a.fine_prefix, a.toff, a.tasks, a.task_cap,
+        k_tasks_write<<<blocks, 128, 0, st>>>(a.J, a.nj, a.dom_prefix, a.toff, a.tasks, a.task_cap,
                                               a.gwords);
         ++launches;
     }

@@ -15,11 +15,14 @@ struct PipelineArgs {
     const int64_t* seg_prefix;        // [nj+1] level-1 partitions of joins with P2 > 1 (per relation
                                       // the same count)
     const int64_t* fine_prefix;       // [nj+1] finest partitions of joins before j
-    const int64_t* bloom_prefix;      // [nj+1] finest partitions of Bloom-enabled joins before j
+    const int64_t* bloom_prefix;      // [nj+1] Bloom build groups of joins before j
+    const int64_t* dom_prefix;        // [nj+1] task domains of joins before j
     int64_t total_slices[2];
     int64_t total_segs;               // sum of P1 over joins with P2 > 1
     int64_t total_fine;               // sum of P1*P2
-    int64_t total_bloom_fine;         // sum of P1*P2 over Bloom joins
+    int64_t total_bloom_groups;       // Bloom build groups over all joins
+    int64_t total_domains;            // task domains over all joins
+    int bloom_smem_words;             // shared-memory words of one Bloom build group
     int64_t hist_begin[2], hist_len[2];  // range of each relation in the global histogram array
     uint32_t* hist;                   // global level-1 histogram array (both relations)
     int64_t* hist_scan;               // exclusive scan of hist (same indexing)
@@ -40,6 +43,7 @@ struct PipelineArgs {
 };
 
 constexpr int kNumStages = 11;
+constexpr int kBloomSmemWords = 12288;  // 48 KB of Bloom segments per build CTA
 const char* stage_name(int i);
 
 // Enqueues the full join pipeline (partition, Bloom, tasks, probe) for all joins on `stream`.

@@ -65,7 +65,7 @@ typedef struct brig_join_config {
     int32_t table_capacity;         /* max build-side tuples per shared-memory table, power of two
                                        in [256, 8192]; 0 = 4096 (the reference's HT_SIZE is 10007,
                                        src/common.h:15) */
-    int32_t s_chunk;                /* max S tuples per probe task; 0 = 16384 */
+    int32_t s_chunk;                /* max streamed tuples per probe task; 0 = 65536 */
     int32_t emit_key;               /* 1 = also write the key of each pair (GPU_answer array,
                                        src/kernel_functions.cu:422) */
     int32_t device;                 /* CUDA device ordinal; -1 = current device */

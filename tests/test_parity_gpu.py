@@ -69,7 +69,7 @@ def test_single_hot_key(bj, oracle, torch_cuda):
     sk = np.concatenate([np.full(700, 0xDEADBEEF, np.uint32), np.arange(100, dtype=np.uint32)])
     rv = np.arange(len(rk), dtype=np.uint32)
     sv = np.arange(len(sk), dtype=np.uint32)
-    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, table_capacity=1024)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, table_capacity=256)
     assert st.count == 3000 * 700 and st.split_tasks > 0
 
 
