@@ -181,13 +181,176 @@ def stage_bytes(nr, ns, surv, matches, bloom_bits):
     }
 
 
+# ---- batched uneven joins -------------------------------------------------------------------------
+def batch_shapes(n_joins, seed, lo=4096, hi=1 << 24):
+    """|R_j| log-uniform in [lo, hi], |S_j| = 4 |R_j| (the 256-join uneven batch)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    nr = np.exp(rng.uniform(math.log(lo), math.log(hi), n_joins)).astype(np.int64)
+    return [(int(r), int(4 * r)) for r in nr]
+
+
+def run_batch_workload(args):
+    """256 independent joins, S = 10% Zipf(1.0) matches over R's row order: one batched pipeline
+    (autotuned, CUDA-graph replayed) against 256 sequential single-join calls."""
+    import torch
+    import brig_join as bj
+    torch.cuda.set_device(0)
+    shapes = batch_shapes(args.joins, 7)
+    tot_r = sum(r for r, _ in shapes)
+    tot_s = sum(s for _, s in shapes)
+    i32 = torch.int32
+    big = [torch.empty(n, dtype=i32, device="cuda") for n in (tot_r, tot_r, tot_s, tot_s)]
+    ms = [int(math.floor(0.1 * s)) for _, s in shapes]
+    caps = [m + 64 for m in ms]
+    out_r = torch.empty(sum(caps), dtype=i32, device="cuda")
+    out_s = torch.empty(sum(caps), dtype=i32, device="cuda")
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    items, ro, so, oo = [], 0, 0, 0
+    for j, (nr, ns) in enumerate(shapes):
+        v = [big[0][ro:ro + nr], big[1][ro:ro + nr], big[2][so:so + ns], big[3][so:so + ns]]
+        bj.gen_device(1000 + j, nr, ns, 0.1, 1.0, *v, stream=sp)
+        items.append(dict(r_key=v[0], r_val=v[1], n_r=nr, s_key=v[2], s_val=v[3], n_s=ns,
+                          out_r=out_r[oo:oo + caps[j]], out_s=out_s[oo:oo + caps[j]], capacity=caps[j]))
+        ro += nr; so += ns; oo += caps[j]
+    torch.cuda.synchronize()
+    tuples = tot_r + tot_s
+
+    def timed(fn, steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    # batched: autotune once (outside the timed region), then graph replays
+    jb = bj.Join(use_cuda_graph=1)
+    tuned = jb.autotune(items, stream=sp)
+    for _ in range(args.warmup):
+        jb.run_batch(items, stream=sp)
+    counts = jb.batch_counts(len(items))
+    assert list(counts) == ms, "batched counts differ from the constructed match counts"
+    launches0 = bj.kernel_launches()
+    with ClockSampler(0) as clk:
+        ms_batch = timed(lambda: jb.run_batch(items, stream=sp), args.steps)
+    launches = bj.kernel_launches() - launches0
+    jb.batch_counts(len(items))
+    # sequential: the same joins, one plain join call each
+    js = bj.Join()
+    def seq():
+        for it in items:
+            js.run(it["r_key"], it["r_val"], it["n_r"], it["s_key"], it["s_val"], it["n_s"], it["out_r"], it["out_s"],
+                   it["capacity"], stream=sp)
+    seq()
+    seq_counts = []
+    for it in items:
+        js.run(it["r_key"], it["r_val"], it["n_r"], it["s_key"], it["s_val"], it["n_s"], it["out_r"], it["out_s"],
+               it["capacity"], stream=sp)
+        seq_counts.append(js.stats().count)
+    assert seq_counts == ms, "sequential counts differ"
+    ms_seq = timed(seq, max(1, args.steps // 4))
+    line = {
+        "metric": "batched join tuples/s (sum |R|+|S| over 256 joins / t)", "value": tuples / (ms_batch / 1e3),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch,
+        "higher_is_better": True, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"{args.joins} joins, |R| log-uniform [4K, 16M], |S| = 4|R|, 10% Zipf(1.0) matches",
+                   "total_r": tot_r, "total_s": tot_s, "autotuned": tuned, "graph": True},
+        "sequential": {"ms_per_batch": ms_seq, "value": tuples / (ms_seq / 1e3)},
+        "speedup_vs_sequential": ms_seq / ms_batch, "gpu_launches": launches, "clocks": clk.summary(),
+        "identical_results": True,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---- served joins ---------------------------------------------------------------------------------
+def run_serve_workload(args):
+    """Poisson stream of join requests against a 120 GB budget: p50/p99 latency and aggregate
+    tuples/s per offered load, against one request at a time."""
+    import numpy as np
+    import threading
+    import torch
+    import brig_join as bj
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(11)
+    pool = []
+    for i in range(args.pool):
+        nr = int(math.exp(rng.uniform(math.log(1 << 16), math.log(1 << 26))))
+        ratio = int(rng.choice([1, 4, 16]))
+        frac = float(rng.choice([0.01, 0.1, 0.5]))
+        ns = nr * ratio
+        t = [torch.empty(n, dtype=torch.int32, device="cuda") for n in (nr, nr, ns, ns)]
+        bj.gen_device(5000 + i, nr, ns, frac, 0.0, *t)
+        pool.append((t, nr, ns, int(math.floor(frac * ns))))
+    torch.cuda.synchronize()
+    seq = [int(x) for x in rng.integers(0, len(pool), args.requests)]
+
+    def serve(rate, streams, max_wave):
+        lat, queue, results = [], [], []
+        outs = {i: (np.empty(pool[i][3] + 16, np.uint32), np.empty(pool[i][3] + 16, np.uint32)) for i in set(seq)}
+        gaps = np.random.default_rng(3).exponential(1.0 / rate, len(seq)) if rate > 0 else np.zeros(len(seq))
+        with bj.Server(hbm_budget_bytes=120 * 10**9, max_wave=max_wave, streams=streams) as srv:
+            tickets = []
+            t0 = time.perf_counter()
+            def submitter():
+                nxt = t0
+                for k, i in enumerate(seq):
+                    nxt += gaps[k]
+                    d = nxt - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                    t, nr, ns, m = pool[i]
+                    tickets.append((srv.submit(t[0], t[1], t[2], t[3], capacity=m + 16, out=outs[i],
+                                               on_device=True), i))
+            th = threading.Thread(target=submitter)
+            th.start()
+            done = 0
+            while done < len(seq):
+                while len(tickets) <= done:
+                    time.sleep(0.0005)
+                tk, i = tickets[done]
+                res, a, b = srv.poll(tk)
+                assert res.status == bj.BRIG_OK and res.count == pool[i][3]
+                lat.append(res.submit_to_done_ms)
+                queue.append(res.queue_ms)
+                done += 1
+            th.join()
+            wall = time.perf_counter() - t0
+        tuples = sum(pool[i][1] + pool[i][2] for i in seq)
+        return {"offered_req_per_s": rate, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "mean_queue_ms": float(np.mean(queue)), "tuples_per_s": tuples / wall, "wall_s": wall}
+
+    rates = [float(x) for x in args.rates.split(",")]
+    sweep = [serve(r, args.streams, 16) for r in rates]
+    base = [serve(r, 1, 1) for r in rates]
+    line = {
+        "metric": "served join tuples/s and p50/p99 latency", "value": max(x["tuples_per_s"] for x in sweep),
+        "unit": UNIT, "n_gpus": 1, "dtype": "u32", "data": "synthetic", "higher_is_better": True,
+        "config": {"workload": f"{args.requests} Poisson requests from a pool of {len(pool)}: |R| log-uniform "
+                               "[64K, 64M], |S|/|R| in {1,4,16}, match in {1%,10%,50%}, budget 120 GB",
+                   "streams": args.streams, "max_wave": 16},
+        "continuous_batching": sweep, "one_at_a_time": base,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["batch", "serve"])
+    ap.add_argument("--joins", type=int, default=256, help="batch workload: number of joins")
+    ap.add_argument("--pool", type=int, default=24, help="serve workload: distinct requests")
+    ap.add_argument("--requests", type=int, default=64, help="serve workload: requests per load point")
+    ap.add_argument("--rates", default="5,20,80", help="serve workload: offered loads (requests/s)")
+    ap.add_argument("--streams", type=int, default=3, help="serve workload: concurrent waves")
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--bloom", type=int, default=None, help="override Bloom on/off")
@@ -196,6 +359,10 @@ def main():
     args = ap.parse_args()
     if args.steps > 64:
         ap.error("--steps above 64: per-stage events keep the last 64 runs")
+    if args.workload == "batch":
+        return run_batch_workload(args)
+    if args.workload == "serve":
+        return run_serve_workload(args)
     wl = dict(WORKLOADS[args.workload])
     if args.bloom is not None:
         wl["bloom"] = args.bloom

@@ -66,7 +66,8 @@ class Config(C.Structure):
         ("use_cuda_graph", C.c_int32),
         ("profile_stages", C.c_int32),
         ("bloom_probe_level", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("max_level1_bits", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -167,6 +168,7 @@ def lib() -> C.CDLL:
                                  C.POINTER(C.c_int32), _i64p]
     L.brig_join_run_batch.argtypes = [vp, C.POINTER(BatchItem), C.c_int32, vp]
     L.brig_join_batch_counts.argtypes = [vp, _i64p, C.c_int32]
+    L.brig_join_autotune.argtypes = [vp, C.POINTER(BatchItem), C.c_int32, vp, C.POINTER(Config)]
     L.brig_gen_device.argtypes = [C.c_uint64, C.c_int64, C.c_int64, C.c_double, C.c_double,
                                   vp, vp, vp, vp, vp]
     L.brig_gen_host.argtypes = [C.c_uint64, C.c_int64, C.c_int64, C.c_double, C.c_double,
@@ -306,13 +308,25 @@ class Join:
         return res
 
     def run_batch(self, items: list[dict], stream=None):
+        check(lib().brig_join_run_batch(self.h, self._items(items), len(items), _ptr(stream)),
+              "brig_join_run_batch")
+
+    @staticmethod
+    def _items(items):
         arr = (BatchItem * len(items))()
         for i, it in enumerate(items):
             arr[i] = BatchItem(_ptr(it["r_key"]), _ptr(it["r_val"]), it["n_r"], _ptr(it["s_key"]),
                                _ptr(it["s_val"]), it["n_s"],
                                Output(_ptr(it["out_r"]), _ptr(it["out_s"]), _ptr(it.get("out_key")),
                                       it["capacity"], _ptr(it.get("d_count"))))
-        check(lib().brig_join_run_batch(self.h, arr, len(items), _ptr(stream)), "brig_join_run_batch")
+        return arr
+
+    def autotune(self, items: list[dict], stream=None) -> dict:
+        """Times candidate configurations on this batch; keeps and returns the fastest."""
+        chosen = Config()
+        check(lib().brig_join_autotune(self.h, self._items(items), len(items), _ptr(stream), C.byref(chosen)),
+              "brig_join_autotune")
+        return {"table_capacity": chosen.table_capacity, "max_level1_bits": chosen.max_level1_bits}
 
     def batch_counts(self, n: int, allow_overflow=False) -> np.ndarray:
         c = np.zeros(n, np.int64)

@@ -242,6 +242,26 @@ int brig_join_run_batch(brig_join_t* h, const brig_join_batch_item* items, int32
     });
 }
 
+int brig_join_autotune(brig_join_t* h, const brig_join_batch_item* items, int32_t n_items, void* stream,
+                       brig_join_config* chosen) {
+    return guarded([&] {
+        if (!h || !items || n_items <= 0) fail(BRIG_E_INVALID, "bad autotune arguments");
+        std::vector<brig::JoinIO> io((size_t)n_items);
+        for (int i = 0; i < n_items; ++i) {
+            const auto& it = items[i];
+            check_rel(it.r_key, it.r_val, it.n_r, "R");
+            check_rel(it.s_key, it.s_val, it.n_s, "S");
+            check_out(&it.out);
+            io[i] = brig::JoinIO{it.r_key, it.r_val, it.s_key, it.s_val, it.n_r, it.n_s, it.out};
+        }
+        const brig_join_config c = h->eng->autotune(io, static_cast<cudaStream_t>(stream));
+        if (chosen) *chosen = c;
+        h->last_kind = 2;
+        h->last_items = n_items;
+        return (int)BRIG_OK;
+    });
+}
+
 int brig_join_batch_counts(brig_join_t* h, int64_t* counts, int32_t n_items) {
     return guarded([&] {
         if (!h || !counts) fail(BRIG_E_INVALID, "null argument");

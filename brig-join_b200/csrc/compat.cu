@@ -1,0 +1,425 @@
+// compat.cu - the reference-named C++ entry points (include/brig_join_compat.h) over the engine.
+//
+// The partition entry points run the engine's own partition kernels in the reference's modulo
+// layout (partition_mode = BRIG_PART_MODULO with the global fan-outs) and then translate the
+// result into the reference's contract: tuples back into the caller's key/value arrays in place,
+// inclusive-end bucket indexes, local inclusive-end sub-bucket indexes. The probe entry point does
+// the reverse: it reads the caller's partitioned arrays and indexes into the engine's layout and
+// runs the engine's task builder and probe kernel. gpu_main is the whole local join over files.
+// Every helper here synchronises with the host where the reference does (its entry points are
+// blocking); failures print to stderr and leave outputs untouched instead of exiting.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include "../../include/brig_join.h"
+#include "../../include/brig_join_compat.h"
+#include "engine.h"
+
+int partition_size = 128;
+int second_partition_size = 67;
+int thread_no = 1024;
+int block_no = 31250;
+int block_size = 0;
+int chunk_size = 1024;
+
+// The reference's CPU check, used by gpu_main when the program links it (weak: optional).
+void run_sanity_check(const int* tableA, long long R, const int* tableB, long long S) __attribute__((weak));
+
+namespace brig {
+namespace {
+
+long long g_answer_capacity = (1ll << 62);
+
+// Workspace of the compat entry points (one per process; the reference's are not reentrant either).
+std::mutex g_mu;
+char* g_ws = nullptr;
+size_t g_ws_bytes = 0;
+
+char* compat_workspace(size_t bytes) {
+    if (bytes > g_ws_bytes) {
+        if (g_ws) cudaFree(g_ws);
+        g_ws = nullptr;
+        g_ws_bytes = 0;
+        cuda_check(cudaMalloc(&g_ws, bytes), "compat workspace");
+        g_ws_bytes = bytes;
+    }
+    return g_ws;
+}
+
+brig_join_config modulo_config() {
+    brig_join_config c;
+    brig_join_config_init(&c);
+    c.partition_mode = BRIG_PART_MODULO;
+    c.partition_size = partition_size;
+    c.second_partition_size = second_partition_size;
+    return c;
+}
+
+// A pipeline over one join laid out in the compat workspace; the descriptor image stays on the
+// host so the caller can read every buffer address.
+struct Prepared {
+    JoinPlan plan;
+    JoinOffs jo;
+    Shape sh;
+    std::vector<char> meta;
+    PipelineArgs a;
+    char* ws = nullptr;
+    const JoinDesc& desc() const { return *reinterpret_cast<const JoinDesc*>(meta.data()); }
+};
+
+void prepare(Prepared& p, const brig_join_config& cfg, const JoinIO& io) {
+    int dev = 0, sms = 148;
+    cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    p.plan = plan_join(cfg, io.nr, io.ns);
+    layout_for(cfg, &p.plan, 1, sms, &p.jo, p.sh);
+    p.ws = compat_workspace(p.sh.total);
+    p.meta.assign(p.sh.meta_bytes, 0);
+    fill_pipeline(cfg, &p.plan, &io, 1, p.sh, p.ws, p.meta.data(), sms, p.a);
+}
+
+void launch(Prepared& p, int stages, cudaStream_t st) {
+    cuda_check(cudaMemcpyAsync(p.ws + p.sh.meta, p.meta.data(), p.sh.meta_bytes, cudaMemcpyHostToDevice, st),
+               "descriptor upload");
+    cuda_check(cudaMemsetAsync(p.ws + p.sh.counters, 0, (size_t)kCntWords * 8, st), "counter reset");
+    p.a.stages = stages;
+    cuda_check(enqueue_pipeline(p.a, st), "pipeline launch");
+}
+
+// ---- layout translation kernels ----------------------------------------------------------------
+__global__ void k_unpack(const uint2* __restrict__ in, int* __restrict__ key, int* __restrict__ val, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint2 e = in[i];
+        key[i] = (int)e.x;
+        val[i] = (int)e.y;
+    }
+}
+__global__ void k_pack(const int* __restrict__ key, const int* __restrict__ val, uint2* __restrict__ out, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = make_uint2((uint32_t)key[i], (uint32_t)val[i]);
+}
+// Engine bounds -> reference indexes: blk[p] inclusive end of bucket p; sec[p*P2+q] inclusive end of
+// sub-bucket q relative to bucket p's start; prefix[p] bucket size; offset[p] bucket end.
+__global__ void k_to_ref_index(const int64_t* __restrict__ b1, const int64_t* __restrict__ bounds, int P1, int P2,
+                               long long* blk, long long* sec, long long* prefix, long long* offset) {
+    const int64_t nf = (int64_t)P1 * P2;
+    for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < nf; f += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = f / P2;
+        if (sec) sec[f] = bounds[f + 1] - b1[p];
+        if (f % P2 == 0) {
+            if (blk) blk[p] = b1[p + 1];
+            if (prefix) prefix[p] = b1[p + 1] - b1[p];
+            if (offset) offset[p] = b1[p + 1];
+        }
+    }
+}
+// Reference indexes -> engine bounds (start of every finest partition, plus the total).
+__global__ void k_from_ref_index(const long long* __restrict__ blk, const long long* __restrict__ sec, int P1, int P2,
+                                 int64_t* __restrict__ bounds) {
+    const int64_t nf = (int64_t)P1 * P2;
+    for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f <= nf; f += (int64_t)gridDim.x * blockDim.x) {
+        if (f == nf) {
+            bounds[f] = blk[P1 - 1];
+            continue;
+        }
+        const int64_t p = f / P2, q = f % P2;
+        bounds[f] = (p ? blk[p - 1] : 0) + (q ? sec[f - 1] : 0);
+    }
+}
+
+constexpr int kCompatGrid = 1184;
+
+// Partitions one relation (rel 0 = R from io.rk/rv, rel 1 = S from io.sk/sv) and translates the
+// result into the reference's contract.
+void partition_rel(int rel, int* d_data, int* d_val, int2* d_kv_out, long long* d_prefix, long long* d_block_index,
+                   long long* d_offset, long long* d_second_index, long long n, cudaStream_t st) {
+    if (partition_size <= 0 || second_partition_size <= 0) fail(BRIG_E_INVALID, "partition sizes must be positive");
+    const brig_join_config cfg = modulo_config();
+    JoinIO io{};
+    if (rel == 0) {
+        io.rk = reinterpret_cast<const uint32_t*>(d_data);
+        io.rv = reinterpret_cast<const uint32_t*>(d_val);
+        io.nr = n;
+    } else {
+        io.sk = reinterpret_cast<const uint32_t*>(d_data);
+        io.sv = reinterpret_cast<const uint32_t*>(d_val);
+        io.ns = n;
+    }
+    Prepared p;
+    prepare(p, cfg, io);
+    launch(p, rel == 0 ? kRunPartR : kRunPartS, st);
+    const JoinDesc& d = p.desc();
+    const RelPlan& R = d.rel[rel];
+    const uint2* fin = d.pf.P2 > 1 ? R.l2 : R.l1;
+    if (n > 0) {
+        k_unpack<<<kCompatGrid, 256, 0, st>>>(fin, d_data, d_val, n);
+        if (d_kv_out)
+            cuda_check(cudaMemcpyAsync(d_kv_out, fin, (size_t)n * 8, cudaMemcpyDeviceToDevice, st), "kv copy");
+    }
+    k_to_ref_index<<<kCompatGrid, 256, 0, st>>>(R.b1, R.bounds, (int)d.pf.P1, (int)d.pf.P2, d_block_index, d_second_index,
+                                                d_prefix, d_offset);
+    note_launches(n > 0 ? 2 : 1);
+    cuda_check(cudaGetLastError(), "translation launch");
+}
+
+void report(const Error& e, const char* where) { fprintf(stderr, "[brig compat] %s: %s\n", where, e.msg.c_str()); }
+
+}  // namespace
+}  // namespace brig
+
+using namespace brig;
+
+void brig_compat_set_answer_capacity(long long capacity) { g_answer_capacity = capacity < 0 ? 0 : capacity; }
+
+void split_tables(int device_num, int* const tableA, int* const tableB, int* const tableA_val, int* const tableB_val,
+                  long long* tableA_size, long long* tableB_size, int** tableA_split, int** tableB_split,
+                  int** tableA_val_split, int** tableB_val_split, const long long R, const long long S) {
+    const long long r = R / device_num, s = S / device_num;
+    for (int i = 0; i < device_num; ++i) {
+        tableA_split[i] = tableA + r * i;
+        tableB_split[i] = tableB + s * i;
+        tableA_val_split[i] = tableA_val + r * i;
+        tableB_val_split[i] = tableB_val + s * i;
+        tableA_size[i] = (i == device_num - 1) ? R - r * i : r;
+        tableB_size[i] = (i == device_num - 1) ? S - s * i : s;
+    }
+}
+
+void partial_jointable_gpu_partition_r_only(int* const d_adata, int* const, int* const d_a_val, int* const,
+                                            long long* const d_a_prefix_data, long long* const d_block_index_split_r,
+                                            long long* const d_a_offset, long long* const d_second_index_split_r,
+                                            const long long R, cudaStream_t gpu_stream) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    try {
+        partition_rel(0, d_adata, d_a_val, nullptr, d_a_prefix_data, d_block_index_split_r, d_a_offset,
+                      d_second_index_split_r, R, gpu_stream);
+        cuda_check(cudaStreamSynchronize(gpu_stream), "cudaStreamSynchronize");
+    } catch (const Error& e) {
+        report(e, "partial_jointable_gpu_partition_r_only");
+    }
+}
+
+void partial_jointable_gpu_partition_s_only(int* const d_bdata, int* const, int* const d_b_val, int* const,
+                                            int2* const d_b_kv_out, long long* const d_b_prefix_data,
+                                            long long* const d_block_index_split_s, long long* const d_b_offset,
+                                            long long* const d_second_index_split_s, int* const d_answer_num,
+                                            const long long S, cudaStream_t gpu_stream) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    try {
+        if (d_answer_num) cuda_check(cudaMemsetAsync(d_answer_num, 0, sizeof(int), gpu_stream), "memset");
+        partition_rel(1, d_bdata, d_b_val, d_b_kv_out, d_b_prefix_data, d_block_index_split_s, d_b_offset,
+                      d_second_index_split_s, S, gpu_stream);
+        cuda_check(cudaStreamSynchronize(gpu_stream), "cudaStreamSynchronize");
+    } catch (const Error& e) {
+        report(e, "partial_jointable_gpu_partition_s_only");
+    }
+}
+
+void partial_jointable_gpu_partition(const int* const d_adata, const int* const d_bdata, int* const d_oa_data,
+                                     int* const d_ob_data, int* const d_a_val, int* const d_b_val, int* const d_oa_val,
+                                     int* const d_ob_val, int2* const d_b_kv_out, long long* const d_a_prefix_data,
+                                     long long* const d_b_prefix_data, long long* const d_block_index_split_r,
+                                     long long* const d_block_index_split_s, long long* const d_a_offset,
+                                     long long* const d_b_offset, long long* const d_second_index_split_r,
+                                     long long* const d_second_index_split_s, int* const d_answer_num,
+                                     const long long R, const long long S, cudaStream_t gpu_stream, cudaEvent_t,
+                                     double& out_partition_sec, double& out_hist_sec, bool) {
+    const auto t0 = std::chrono::steady_clock::now();
+    // The reference partitions its (const-declared) input buffers in place as well.
+    partial_jointable_gpu_partition_r_only(const_cast<int*>(d_adata), d_oa_data, d_a_val, d_oa_val, d_a_prefix_data,
+                                           d_block_index_split_r, d_a_offset, d_second_index_split_r, R, gpu_stream);
+    partial_jointable_gpu_partition_s_only(const_cast<int*>(d_bdata), d_ob_data, d_b_val, d_ob_val, d_b_kv_out,
+                                           d_b_prefix_data, d_block_index_split_s, d_b_offset, d_second_index_split_s,
+                                           d_answer_num, S, gpu_stream);
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    out_partition_sec += sec;
+    out_hist_sec += 0.0;  // the histogram passes are inside the partition time here
+}
+
+void partial_jointable_gpu_partition_rs_split(
+    const int* const d_adata, const int* const d_bdata, int* const d_oa_data, int* const d_ob_data, int* const d_a_val,
+    int* const d_b_val, int* const d_oa_val, int* const d_ob_val, int2* const d_b_kv_out,
+    long long* const d_a_prefix_data, long long* const d_b_prefix_data, long long* const d_block_index_split_r,
+    long long* const d_block_index_split_s, long long* const d_a_offset, long long* const d_b_offset,
+    long long* const d_second_index_split_r, long long* const d_second_index_split_s, int* const d_answer_num,
+    const long long R, const long long S, cudaStream_t gpu_stream, cudaEvent_t, double& out_partition_sec,
+    double& out_partition_r_sec, double& out_partition_s_sec, double& out_hist_r_sec, double& out_hist_s_sec, bool) {
+    const auto t0 = std::chrono::steady_clock::now();
+    partial_jointable_gpu_partition_r_only(const_cast<int*>(d_adata), d_oa_data, d_a_val, d_oa_val, d_a_prefix_data,
+                                           d_block_index_split_r, d_a_offset, d_second_index_split_r, R, gpu_stream);
+    const auto t1 = std::chrono::steady_clock::now();
+    partial_jointable_gpu_partition_s_only(const_cast<int*>(d_bdata), d_ob_data, d_b_val, d_ob_val, d_b_kv_out,
+                                           d_b_prefix_data, d_block_index_split_s, d_b_offset, d_second_index_split_s,
+                                           d_answer_num, S, gpu_stream);
+    const auto t2 = std::chrono::steady_clock::now();
+    out_partition_r_sec += std::chrono::duration<double>(t1 - t0).count();
+    out_partition_s_sec += std::chrono::duration<double>(t2 - t1).count();
+    out_partition_sec += std::chrono::duration<double>(t2 - t0).count();
+    out_hist_r_sec += 0.0;
+    out_hist_s_sec += 0.0;
+}
+
+void partial_jointable_gpu_run_only_s(const int* const d_adata, const int* const d_bdata, const int* const d_a_val,
+                                      const int* const d_b_val, long long* const d_block_index_split_r,
+                                      long long* const d_block_index_split_s, long long* const d_second_index_split_r,
+                                      long long* const d_second_index_split_s, int* const d_answer,
+                                      int* const d_answer_val, int* const d_answer_s_val, int* const d_answer_num, int,
+                                      int* final_answer_number, cudaStream_t gpu_stream, cudaEvent_t,
+                                      int* const d_answer_write_idx) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    try {
+        cudaStream_t st = gpu_stream;
+        const int P1 = partition_size, P2 = second_partition_size;
+        if (P1 <= 0 || P2 <= 0) fail(BRIG_E_INVALID, "partition sizes must be positive");
+        long long nr = 0, ns = 0;
+        cuda_check(cudaMemcpyAsync(&nr, d_block_index_split_r + (P1 - 1), 8, cudaMemcpyDeviceToHost, st), "D2H");
+        cuda_check(cudaMemcpyAsync(&ns, d_block_index_split_s + (P1 - 1), 8, cudaMemcpyDeviceToHost, st), "D2H");
+        int wi = 0;
+        if (d_answer_write_idx)
+            cuda_check(cudaMemcpyAsync(&wi, d_answer_write_idx, 4, cudaMemcpyDeviceToHost, st), "D2H");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        brig_join_config cfg = modulo_config();
+        // the caller's layout fixes the fan-outs; keep them even when the planner would choose
+        // differently for these sizes
+        cfg.partition_size = P1;
+        cfg.second_partition_size = P2;
+        const int64_t base = std::max(0, wi);
+        const int64_t cap = std::max<int64_t>(0, g_answer_capacity - base);
+        brig_join_output out{reinterpret_cast<uint32_t*>(d_answer_val) + base,
+                             reinterpret_cast<uint32_t*>(d_answer_s_val) + base,
+                             d_answer ? reinterpret_cast<uint32_t*>(d_answer) + base : nullptr, cap, nullptr};
+        JoinIO io{reinterpret_cast<const uint32_t*>(d_adata), reinterpret_cast<const uint32_t*>(d_a_val),
+                  reinterpret_cast<const uint32_t*>(d_bdata), reinterpret_cast<const uint32_t*>(d_b_val), nr, ns, out};
+        Prepared p;
+        prepare(p, cfg, io);
+        const JoinDesc& d = p.desc();
+        for (int rel = 0; rel < 2; ++rel) {
+            const RelPlan& R = d.rel[rel];
+            uint2* fin = d.pf.P2 > 1 ? R.l2 : R.l1;
+            const int64_t n = rel ? ns : nr;
+            if (n > 0)
+                k_pack<<<kCompatGrid, 256, 0, st>>>(rel ? d_bdata : d_adata, rel ? d_b_val : d_a_val, fin, n);
+            k_from_ref_index<<<kCompatGrid, 256, 0, st>>>(rel ? d_block_index_split_s : d_block_index_split_r,
+                                                          rel ? d_second_index_split_s : d_second_index_split_r, P1, P2,
+                                                          R.bounds);
+            if (d.pf.P2 > 1)  // b1 is only read by level-2 kernels, which do not run here
+                cuda_check(cudaMemsetAsync(R.b1, 0, ((size_t)P1 + 1) * 8, st), "memset");
+            note_launches(n > 0 ? 2 : 1);
+        }
+        cuda_check(cudaGetLastError(), "translation launch");
+        launch(p, kRunProbe, st);
+        long long cnt = 0;
+        cuda_check(cudaMemcpyAsync(&cnt, d.counters + kCntMatches, 8, cudaMemcpyDeviceToHost, st), "D2H");
+        cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        const int c32 = (int)cnt;
+        if (d_answer_num) cuda_check(cudaMemcpy(d_answer_num, &c32, 4, cudaMemcpyHostToDevice), "H2D");
+        if (d_answer_write_idx) {
+            const int next = (int)(base + cnt);
+            cuda_check(cudaMemcpy(d_answer_write_idx, &next, 4, cudaMemcpyHostToDevice), "H2D");
+        }
+        if (final_answer_number) *final_answer_number = c32;
+    } catch (const Error& e) {
+        report(e, "partial_jointable_gpu_run_only_s");
+    }
+}
+
+void gpu_main(std::vector<int>*, std::vector<int>*, const std::string& r_inputPath, const std::string& s_inputPath,
+              long long R, long long S, int use_bf, bool use_nvlink, bool, double true_false_ratio, int s_chunks,
+              bool sanityCheck, int kernel_fusion, double redist_skew_threshold, long long override_num_bits,
+              int override_num_hashes, int, int override_partition_size, int override_second_partition_size, int,
+              int read_val, int r_shuffle_enable, double r_replicate_ratio, double answer_scale) {
+    if (use_nvlink || kernel_fusion || redist_skew_threshold > 0.0 || r_shuffle_enable || r_replicate_ratio >= 0.0)
+        fprintf(stderr, "[brig compat] one GPU: multi-GPU options (nvlink, fusion, redistribution, shuffle, "
+                        "replication) have no effect\n");
+    if (R < 0 || S < 0 || s_chunks < 1) {
+        fprintf(stderr, "[brig compat] gpu_main: bad sizes\n");
+        return;
+    }
+    std::vector<int> tk(R), tv(R), sk(S), sv(S);
+    {
+        std::ifstream rf(r_inputPath, std::ios::binary), sf(s_inputPath, std::ios::binary);
+        if (!rf.is_open() || !sf.is_open()) {
+            fprintf(stderr, "[brig compat] gpu_main: failed to open input files\n");
+            return;
+        }
+        rf.read(reinterpret_cast<char*>(tk.data()), (std::streamsize)(4 * R));
+        sf.read(reinterpret_cast<char*>(sk.data()), (std::streamsize)(4 * S));
+        if (read_val) {
+            rf.read(reinterpret_cast<char*>(tv.data()), (std::streamsize)(4 * R));
+            sf.read(reinterpret_cast<char*>(sv.data()), (std::streamsize)(4 * S));
+        } else {
+            for (long long i = 0; i < R; ++i) tv[i] = (int)i + 1;
+            for (long long i = 0; i < S; ++i) sv[i] = (int)i + 100000001;
+        }
+        if (!rf || !sf) {
+            fprintf(stderr, "[brig compat] gpu_main: input shorter than the given sizes\n");
+            return;
+        }
+    }
+    if (sanityCheck && run_sanity_check) run_sanity_check(tk.data(), R, sk.data(), S);
+    brig_join_config cfg;
+    brig_join_config_init(&cfg);
+    if (use_bf) {
+        cfg.use_bloom = 1;
+        const double ln2 = std::log(2.0);
+        const double bits = -(double)R * std::log(true_false_ratio) / (ln2 * ln2);
+        cfg.bloom_num_bits = override_num_bits >= 0 ? override_num_bits : (int64_t)bits;
+        cfg.bloom_num_hashes = override_num_hashes >= 0 ? override_num_hashes : std::max(1, (int)(bits / std::max<double>(R, 1) * ln2));
+        if (cfg.bloom_num_hashes > kMaxBloomK) cfg.bloom_num_hashes = kMaxBloomK;
+    }
+    if (override_partition_size >= 0 || override_second_partition_size >= 0) {
+        cfg.partition_mode = BRIG_PART_MODULO;
+        cfg.partition_size = override_partition_size > 0 ? override_partition_size : partition_size;
+        if (override_second_partition_size > 0) cfg.second_partition_size = override_second_partition_size;
+    }
+    const long long cap = (long long)((double)std::max(R, S) * std::max(1.0, answer_scale));
+    brig_join_t* h = nullptr;
+    if (brig_join_create(&cfg, &h) != BRIG_OK) {
+        fprintf(stderr, "[brig compat] gpu_main: %s\n", brig_join_last_error());
+        return;
+    }
+    uint32_t *dk = nullptr, *dv = nullptr, *dsk = nullptr, *dsv = nullptr, *o_r = nullptr, *o_s = nullptr;
+    const long long chunk = (S + s_chunks - 1) / s_chunks;
+    long long total = 0, overflow_tasks = 0;
+    bool ok = cudaMalloc(&dk, 4 * std::max(R, 1ll)) == cudaSuccess && cudaMalloc(&dv, 4 * std::max(R, 1ll)) == cudaSuccess &&
+              cudaMalloc(&dsk, 4 * std::max(chunk, 1ll)) == cudaSuccess &&
+              cudaMalloc(&dsv, 4 * std::max(chunk, 1ll)) == cudaSuccess &&
+              cudaMalloc(&o_r, 4 * std::max(cap, 1ll)) == cudaSuccess && cudaMalloc(&o_s, 4 * std::max(cap, 1ll)) == cudaSuccess;
+    const auto t0 = std::chrono::steady_clock::now();
+    if (ok) {
+        cudaMemcpy(dk, tk.data(), 4 * R, cudaMemcpyHostToDevice);
+        cudaMemcpy(dv, tv.data(), 4 * R, cudaMemcpyHostToDevice);
+        for (int c = 0; c < s_chunks && ok; ++c) {
+            const long long off = (long long)c * chunk, n = std::max(0ll, std::min(chunk, S - off));
+            if (n > 0) {
+                cudaMemcpy(dsk, sk.data() + off, 4 * n, cudaMemcpyHostToDevice);
+                cudaMemcpy(dsv, sv.data() + off, 4 * n, cudaMemcpyHostToDevice);
+            }
+            brig_join_output out{o_r, o_s, nullptr, cap, nullptr};
+            brig_join_stats st;
+            int rc = brig_join_run(h, dk, dv, R, dsk, dsv, n, &out, nullptr);
+            if (rc == BRIG_OK || rc == BRIG_E_OVERFLOW) rc = brig_join_get_stats(h, &st);
+            if (rc != BRIG_OK && rc != BRIG_E_OVERFLOW) {
+                fprintf(stderr, "[brig compat] gpu_main: %s\n", brig_join_last_error());
+                ok = false;
+                break;
+            }
+            total += st.count;
+            overflow_tasks += st.split_tasks;
+        }
+    } else {
+        fprintf(stderr, "[brig compat] gpu_main: device allocation failed\n");
+    }
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (ok) {
+        printf("[PE0] PE0 answer count: %lld\n", total);
+        printf("=== Grand Total Answer Count (all PEs): %lld ===\n", total);
+        printf("[PE0] Total (H2D + join) %.4f sec, split tasks %lld\n", sec, overflow_tasks);
+    }
+    for (uint32_t* p : {dk, dv, dsk, dsv, o_r, o_s})
+        if (p) cudaFree(p);
+    brig_join_destroy(h);
+}

@@ -48,7 +48,8 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
             // At most 512 level-1 partitions: every CTA keeps one open output run per partition,
             // and at 512 the runs of all CTAs (148 x 512 lines) stay resident in L2 until they are
             // completed, so DRAM sees whole lines. Anything finer goes to level 2.
-            b1 = bits <= 9 ? bits : 9;
+            const int cap = cfg.max_level1_bits > 0 ? std::min(cfg.max_level1_bits, 12) : 9;
+            b1 = bits <= cap ? bits : cap;
         }
         if (cfg.second_partition_size > 0) {
             if (!is_pow2(cfg.second_partition_size) || cfg.second_partition_size > kMaxP2)
@@ -444,6 +445,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     a.any_bloom = sh.any_bloom ? 1 : 0;
     a.num_sms = num_sms;
     a.stage_events = nullptr;
+    a.stages = kRunAll;
 }
 
 void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph) {
@@ -543,6 +545,55 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
     d_counters_ = counters;
     d_gwords_ = a.gwords;
     nj_ = nj;
+}
+
+brig_join_config Engine::autotune(const std::vector<JoinIO>& joins, cudaStream_t stream) {
+    // Candidates: shared-memory table capacity (build-chunk size, which also sets the partition
+    // count through the planner's fill target) x largest level-1 fan-out.
+    const int tables[] = {2048, 4096, 8192};
+    const int l1bits[] = {8, 9, 10};
+    const brig_join_config base = cfg_;
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+    float best = -1.f;
+    brig_join_config best_cfg = base;
+    try {
+        for (int t : tables) {
+            for (int b : l1bits) {
+                cfg_ = base;
+                cfg_.table_capacity = t;
+                cfg_.max_level1_bits = b;
+                cfg_.profile_stages = 0;
+                run(joins, stream, false);  // warm-up (sizes the workspace)
+                cuda_check(cudaEventRecord(e0, stream), "cudaEventRecord");
+                run(joins, stream, false);
+                cuda_check(cudaEventRecord(e1, stream), "cudaEventRecord");
+                cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+                float ms = 0.f;
+                cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+                if (best < 0.f || ms < best) {
+                    best = ms;
+                    best_cfg = cfg_;
+                }
+            }
+        }
+    } catch (...) {
+        cfg_ = base;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    best_cfg.profile_stages = base.profile_stages;
+    cfg_ = best_cfg;
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+        graph_key_.clear();
+    }
+    return cfg_;
 }
 
 void Engine::sync_counters(std::vector<int64_t>& counters, int64_t& errors) {

@@ -89,6 +89,8 @@ public:
 
     // Enqueues all joins on `stream` (asynchronous).
     void run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph);
+    // Times candidate configurations on `joins`, keeps the fastest in the handle and returns it.
+    brig_join_config autotune(const std::vector<JoinIO>& joins, cudaStream_t stream);
     // Waits for the last run; copies per-join counters.
     void sync_counters(std::vector<int64_t>& counters, int64_t& errors);
     const std::vector<JoinPlan>& last_plans() const { return plans_; }

@@ -1044,9 +1044,10 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     k_fill_word<<<1, 1, 0, st>>>(a.gwords + kGErrors, 0ull);
     launches += 2;
 
-    // ---- R: level 1 -------------------------------------------------------------------------
+    // ---- R, then S: level 1 and level 2 (the Bloom build sits between them) -----------------
     for (int rel = 0; rel < 2; ++rel) {
-        if (rel == 1 && a.any_bloom && a.total_bloom_groups > 0) {
+        const bool part = (a.stages & (rel == 0 ? kRunPartR : kRunPartS)) != 0;
+        if (rel == 1 && (a.stages & kRunBloom) && a.any_bloom && a.total_bloom_groups > 0) {
             // Bloom filter over the final R partitions, before S's first pass probes it.
             k_bloom_build<<<grid_for(a.total_bloom_groups, sms, 4), kThreads,
                             (size_t)a.bloom_smem_words * 4, st>>>(a.J, a.nj, a.bloom_prefix,
@@ -1055,6 +1056,10 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
         }
         if (rel == 1) mark(5);
         const int m0 = rel == 0 ? 1 : 6;  // first stage mark of this relation
+        if (!part) {
+            for (int m = m0; m < m0 + 4; ++m) mark(m);
+            continue;
+        }
         if (a.total_slices[rel] > 0) {
             k_l1_hist<<<grid_for(a.total_slices[rel], sms, 4), kThreads, (size_t)a.max_p1 * 4, st>>>(
                 a.J, a.nj, rel, a.slice_prefix[rel], a.hist, a.gwords);
@@ -1084,6 +1089,12 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
         mark(m0 + 3);
     }
     // ---- tasks --------------------------------------------------------------------------------
+    if (!(a.stages & kRunProbe)) {
+        mark(10);
+        mark(11);
+        note_launches(launches);
+        return cudaGetLastError();
+    }
     {
         const int64_t n = a.total_domains + 1;
         const int blocks = (int)std::min<int64_t>((n + 127) / 128, (int64_t)sms * 8);

@@ -40,7 +40,11 @@ struct PipelineArgs {
     int any_bloom;
     int num_sms;
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
+    int stages;                       // kRunPartR | kRunBloom | kRunPartS | kRunProbe
 };
+
+// Pipeline parts (a full join runs all four; the reference-named entry points run subsets).
+enum RunPart : int { kRunPartR = 1, kRunBloom = 2, kRunPartS = 4, kRunProbe = 8, kRunAll = 15 };
 
 constexpr int kNumStages = 11;
 constexpr int kBloomSmemWords = 12288;  // 48 KB of Bloom segments per build CTA

@@ -80,7 +80,9 @@ typedef struct brig_join_config {
                                        level-1 partition's filter segments stay in L2 (needs two
                                        partition levels); 0 = auto: 1 while the whole filter fits
                                        comfortably in L2, else 2 */
-    int32_t reserved[5];
+    int32_t max_level1_bits;        /* largest automatic level-1 fan-out, as radix bits (hash mode);
+                                       0 = 9 (512 partitions) */
+    int32_t reserved[4];
 } brig_join_config;
 
 /* Output of one join. Pairs are written in an unspecified order; the multiset is exact. When the
@@ -190,6 +192,14 @@ int brig_join_run_batch(brig_join_t* h, const brig_join_batch_item* items, int32
 /* Waits for the last batch and copies its per-join exact counts into counts[n_items]. Returns
  * BRIG_E_OVERFLOW if any join exceeded its capacity. */
 int brig_join_batch_counts(brig_join_t* h, int64_t* counts, int32_t n_items);
+
+/* Times candidate configurations (shared-memory table capacity x level-1 fan-out) on the given
+ * batch and keeps the fastest in the handle; the chosen configuration is copied to *chosen when
+ * not NULL. Runs the batch 2 x 9 times; results of those runs are discarded (outputs are
+ * overwritten). The reference has no autotuner; its sizing is fixed heuristics
+ * (src/hash_kernel.cu:198-284). */
+int brig_join_autotune(brig_join_t* h, const brig_join_batch_item* items, int32_t n_items, void* stream,
+                       brig_join_config* chosen);
 
 /* ---- Served joins: continuous batching under an HBM budget ------------------------------------
  * No reference counterpart. Requests are admitted while their device footprint fits the budget;

@@ -114,3 +114,15 @@ def test_generator_rejects_bad_arguments(bj):
     assert L.brig_gen_host(1, -5, 10, 0.1, 0.0, None, None, None, None) == bj.BRIG_E_INVALID
     assert L.brig_gen_host(1, 10, 10, 1.5, 0.0, None, None, None, None) == bj.BRIG_E_INVALID
     assert L.brig_gen_host(1, 1 << 31, 10, 0.1, 0.0, None, None, None, None) == bj.BRIG_E_UNSUPPORTED
+
+
+def test_compat_symbols_exported(bj):
+    """The reference-named C++ entry points of include/brig_join_compat.h are exported."""
+    out = subprocess.run(["nm", "-DC", "--defined-only", bj.LIB_PATH], capture_output=True, text=True).stdout
+    for name in ["gpu_main(", "split_tables(", "partial_jointable_gpu_partition(",
+                 "partial_jointable_gpu_partition_rs_split(", "partial_jointable_gpu_partition_r_only(",
+                 "partial_jointable_gpu_partition_s_only(", "partial_jointable_gpu_run_only_s(",
+                 "brig_compat_set_answer_capacity("]:
+        assert name in out, name
+    for g in ["partition_size", "second_partition_size", "thread_no", "block_no", "chunk_size"]:
+        assert any(line.split()[-1] == g for line in out.splitlines() if line.strip()), g
