@@ -29,6 +29,7 @@ constexpr int kMaxBloomK = 16;
 constexpr int kThreads = 512;         // threads per CTA of every partition and probe kernel
 constexpr int kTile = 4096;           // tuples per scatter tile staged in shared memory
 constexpr int kWarpBuf = 128;         // output pairs staged per warp before a global flush
+constexpr int64_t kL2Slice = 32 * kTile;  // tuples per level-2 slice (131072)
 
 // Per-join device counters (int64 each).
 enum Counter : int {
@@ -149,8 +150,7 @@ struct RelPlan {
     int64_t* bounds;       // [P1*P2 + 1] start of each finest partition in the final buffer
                            // (equal to b1 when P2 == 1)
     uint32_t* slice_cnt;   // [nslices] survivors per slice (S with a level-1 Bloom probe)
-    uint32_t* fine_cnt;    // [P1*P2] tuples per finest partition when the final buffer has gaps
-                           // (S with a level-2 Bloom probe), else nullptr: size = bounds[f+1]-bounds[f]
+    int64_t h2_base;       // offset of this relation's [P1][P2][slices] level-2 histogram in hist2
 };
 
 struct JoinDesc {
@@ -198,7 +198,8 @@ enum GlobalWord : int {
     kGQueue = 0,           // next task index to hand out
     kGTasks = 1,           // total tasks (written by the task builder)
     kGErrors = 2,          // device-side consistency failures
-    kGWords = 4
+    kGL2Slices = 3,        // level-2 slices of R (word 3) and of S (word 4)
+    kGWords = 8
 };
 
 }  // namespace brig

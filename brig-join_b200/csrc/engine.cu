@@ -162,8 +162,8 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
             if (r == 1 && p.bloom) {
                 ro.cmp = L.take((size_t)std::max<int64_t>(n[r], 1) * 8);
                 if (p.bloom_level == 1) ro.slice_cnt = L.take((size_t)ro.nslices * 4);
-                else ro.fine_cnt = L.take((size_t)p.nfine * 4);
             }
+            if (two) sh.l2_slice_cap[r] += (int64_t)p.pf.P1 + n[r] / kL2Slice + 1;
             ro.hist_base = sh.hist_len[0] + sh.hist_len[1];  // provisional, fixed below
             sh.total_slices[r] += ro.nslices;
         }
@@ -193,14 +193,35 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
         }
         sh.hist_len[r] = base - ((r == 0) ? 0 : sh.hist_len[0]);
     }
+    // Level-2 histograms [p][q][slice] per join, sized by the slice bound P1 + n / kL2Slice + 1.
+    for (int r = 0; r < 2; ++r) {
+        int64_t base = (r == 0) ? 0 : sh.h2_len[0];
+        for (int j = 0; j < nj; ++j) {
+            const JoinPlan& p = plans[j];
+            RelOffs& ro = sh.jo[j].rel[r];
+            ro.h2_base = base;
+            if (p.pf.P2 > 1) {
+                const int64_t n = r == 0 ? p.nr : p.ns;
+                base += ((int64_t)p.pf.P1 + n / kL2Slice + 1) * p.pf.P2 + 1;
+            }
+        }
+        sh.h2_len[r] = base - ((r == 0) ? 0 : sh.h2_len[0]);
+    }
+    const int64_t h2_total = std::max<int64_t>(1, sh.h2_len[0] + sh.h2_len[1]);
+    sh.hist2 = L.take((size_t)h2_total * 4);
+    sh.hist2_scan = L.take((size_t)h2_total * 8);
+    sh.seg_ns = L.take(((size_t)sh.total_segs + 1) * 4);
+    sh.seg_off = L.take(((size_t)sh.total_segs + 1) * 8);
+    sh.slice_cnt2 = L.take((size_t)std::max<int64_t>(1, std::max(sh.l2_slice_cap[0], sh.l2_slice_cap[1])) * 4);
     const int64_t hist_total = sh.hist_len[0] + sh.hist_len[1];
     sh.hist = L.take((size_t)hist_total * 4);
     sh.hist_scan = L.take((size_t)hist_total * 8);
     sh.tcount = L.take(((size_t)sh.total_domains + 1) * 4);
     sh.toff = L.take(((size_t)sh.total_domains + 1) * 8);
     sh.tasks = L.take((size_t)sh.task_cap * sizeof(Task));
-    sh.scan_tmp_len = std::max(scan_tmp_words(std::max(sh.hist_len[0], sh.hist_len[1])),
-                               scan_tmp_words(sh.total_domains + 1));
+    sh.scan_tmp_len = std::max({scan_tmp_words(std::max(sh.hist_len[0], sh.hist_len[1])),
+                                scan_tmp_words(sh.total_domains + 1), scan_tmp_words(sh.total_segs + 1),
+                                scan_tmp_words(std::max(sh.h2_len[0], sh.h2_len[1]))});
     sh.scan_tmp = L.take((size_t)sh.scan_tmp_len * 8);
     sh.gwords = L.take(kGWords * 8);
     sh.counters = L.take((size_t)nj * kCntWords * 8);
@@ -379,7 +400,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
             R.b1 = reinterpret_cast<int64_t*>(ws + ro.b1);
             R.bounds = p.pf.P2 > 1 ? reinterpret_cast<int64_t*>(ws + ro.bounds) : R.b1;
             R.slice_cnt = ro.slice_cnt ? reinterpret_cast<uint32_t*>(ws + ro.slice_cnt) : nullptr;
-            R.fine_cnt = ro.fine_cnt ? reinterpret_cast<uint32_t*>(ws + ro.fine_cnt) : nullptr;
+            R.h2_base = ro.h2_base;
         }
         d.pf = p.pf;
         d.out_r = io.out.r_val;
@@ -446,6 +467,17 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     a.num_sms = num_sms;
     a.stage_events = nullptr;
     a.stages = kRunAll;
+    a.seg_ns = reinterpret_cast<uint32_t*>(ws + sh.seg_ns);
+    a.seg_off = reinterpret_cast<int64_t*>(ws + sh.seg_off);
+    a.hist2 = reinterpret_cast<uint32_t*>(ws + sh.hist2);
+    a.hist2_scan = reinterpret_cast<int64_t*>(ws + sh.hist2_scan);
+    a.h2_begin[0] = 0;
+    a.h2_len[0] = sh.h2_len[0];
+    a.h2_begin[1] = sh.h2_len[0];
+    a.h2_len[1] = sh.h2_len[1];
+    a.slice_cnt2 = reinterpret_cast<uint32_t*>(ws + sh.slice_cnt2);
+    a.l2_slice_cap[0] = sh.l2_slice_cap[0];
+    a.l2_slice_cap[1] = sh.l2_slice_cap[1];
 }
 
 void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph) {

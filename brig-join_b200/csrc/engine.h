@@ -46,7 +46,8 @@ struct JoinIO {
 
 // Byte offsets of one relation's buffers inside a pipeline workspace.
 struct RelOffs {
-    size_t l1 = 0, l2 = 0, cmp = 0, b1 = 0, bounds = 0, slice_cnt = 0, fine_cnt = 0;
+    size_t l1 = 0, l2 = 0, cmp = 0, b1 = 0, bounds = 0, slice_cnt = 0;
+    int64_t h2_base = 0;
     int64_t slice_len = 0;
     int32_t nslices = 0;
     int64_t hist_base = 0;
@@ -66,6 +67,9 @@ struct Shape {
     int64_t task_cap = 0;
     size_t hist = 0, hist_scan = 0, tcount = 0, toff = 0, tasks = 0, scan_tmp = 0, gwords = 0,
            counters = 0, meta = 0;
+    size_t seg_ns = 0, seg_off = 0, hist2 = 0, hist2_scan = 0, slice_cnt2 = 0;
+    int64_t h2_len[2] = {0, 0};
+    int64_t l2_slice_cap[2] = {0, 0};
     int64_t scan_tmp_len = 0;
     size_t meta_bytes = 0;      // descriptor image: nj JoinDesc + 5 prefix arrays of nj+1 int64
     size_t total = 0;           // workspace bytes

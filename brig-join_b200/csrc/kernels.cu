@@ -39,6 +39,7 @@ namespace brig {
 namespace {
 
 __device__ __forceinline__ int64_t min_i64(int64_t a, int64_t b) { return a < b ? a : b; }
+__device__ __forceinline__ int64_t max_i64(int64_t a, int64_t b) { return a > b ? a : b; }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -476,39 +477,81 @@ __global__ void k_bounds_l1(const JoinDesc* __restrict__ J, int nj, int rel, con
     }
 }
 
-// Level 2: one CTA per (join, level-1 partition). Counts the partition by its level-2 id, writes
-// the finest-partition bounds, then scatters the partition from l1 into l2 in the same range.
-__global__ void __launch_bounds__(kThreads)
-k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
-               unsigned long long* gwords, int max_bins) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    unsigned char* inbuf = smem;                                                // 2 tile buffers
-    uint2* stage = reinterpret_cast<uint2*>(smem + 2 * kTileBuf);               // [kTile]
-    int64_t* cursor = reinterpret_cast<int64_t*>(stage + kTile);                // [max_bins]
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(cursor + max_bins);             // [max_bins]
-    __shared__ uint32_t tmp[kThreads / 32];
-    __shared__ uint32_t s_surv;
-    __shared__ __align__(8) uint64_t bars[2];
-    init_bars(bars);
-    uint32_t ph = 0;
+// ---- Level 2 ------------------------------------------------------------------------------------
+// Every level-1 partition p is cut into slices of kL2Slice tuples, planned on the device
+// (k_l2_plan + a scan of the slice counts). Slices are handed to CTAs in (join, p, slice) order,
+// so the CTAs running at any moment work on a few adjacent partitions: their output runs and, for
+// a level-2 Bloom probe, their filter segments stay in L2. Per join the level-2 histogram is laid
+// out [p][q][slice]; one exclusive scan of it gives every (p, q, slice) its output run, the same
+// trick as level 1. Survivors of a level-2 Bloom probe are compacted per slice, so the level-2
+// output is dense (survivors only) like the level-1 output.
+// A global level-2 slice t decoded into its join, level-1 partition and slice within it.
+struct L2Slice {
+    int j;
+    int64_t g;          // global segment index (seg_prefix[j] + p)
+    uint32_t p;
+    uint32_t ns;        // slices of this segment
+    int64_t sl;         // slice within the segment
+    int64_t local_off;  // slices of earlier segments of the same join
+};
+
+__device__ __forceinline__ L2Slice l2_decode(const int64_t* __restrict__ seg_prefix, int nj,
+                                             const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns,
+                                             int64_t total_segs, int64_t t) {
+    L2Slice x;
+    // largest g with seg_off[g] <= t (seg_off is non-decreasing; empty segments have one slice)
+    int64_t lo = 0, hi = total_segs;
+    while (hi - lo > 1) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (seg_off[mid] <= t) lo = mid; else hi = mid;
+    }
+    x.g = lo;
+    x.j = find_owner(seg_prefix, nj, lo);
+    x.p = (uint32_t)(lo - seg_prefix[x.j]);
+    x.ns = seg_ns[lo];
+    x.sl = t - seg_off[lo];
+    x.local_off = seg_off[lo] - seg_off[seg_prefix[x.j]];
+    return x;
+}
+
+// Slices per level-1 partition (at least one, so every partition owns a histogram region).
+__global__ void k_l2_plan(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
+                          uint32_t* __restrict__ seg_ns) {
     const int64_t total = seg_prefix[nj];
-    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= total; g += (int64_t)gridDim.x * blockDim.x) {
+        if (g == total) { seg_ns[g] = 0; continue; }
         const int j = find_owner(seg_prefix, nj, g);
-        const JoinDesc& d = J[j];
+        const RelPlan& R = J[j].rel[rel];
+        const int64_t p = g - seg_prefix[j];
+        const int64_t len = R.b1[p + 1] - R.b1[p];
+        seg_ns[g] = (uint32_t)max_i64(1, (len + kL2Slice - 1) / kL2Slice);
+    }
+}
+
+// Level-2 histogram of one slice: counts by level-2 id, or (S with a level-2 Bloom probe) tests
+// every key and compacts the survivors into cmp[slice begin, + survivors).
+__global__ void __launch_bounds__(kThreads)
+k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
+          const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
+          uint32_t* __restrict__ hist2, uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords) {
+    extern __shared__ uint32_t cnt[];  // [max P2]
+    __shared__ uint32_t s_surv;
+    const int lane = threadIdx.x & 31;
+    const int64_t total = (int64_t)gwords[kGL2Slices + rel];
+    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const L2Slice x = l2_decode(seg_prefix, nj, seg_off, seg_ns, total_segs, t);
+        const JoinDesc& d = J[x.j];
         const RelPlan& R = d.rel[rel];
-        const uint32_t p = (uint32_t)(g - seg_prefix[j]);
-        const uint32_t P2 = d.pf.P2, P1 = d.pf.P1;
-        const int64_t begin = R.b1[p], end = R.b1[p + 1];
+        const uint32_t P2 = d.pf.P2;
+        const int64_t begin = R.b1[x.p] + x.sl * kL2Slice;
+        const int64_t end = min_i64(R.b1[x.p + 1], begin + kL2Slice);
         const Bin2 bin{d.pf};
         const bool bloom = rel == 1 && d.bloom != nullptr && d.bloom_level == 2;
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cnt[q] = 0;
         if (threadIdx.x == 0) s_surv = 0;
         __syncthreads();
-        int64_t src_end = end;
-        const uint2* src = R.l1;
+        const uint2* __restrict__ l1 = R.l1;
         if (!bloom) {
-            // eight independent loads in flight per thread
-            const uint2* __restrict__ l1 = R.l1;
             for (int64_t i0 = begin + threadIdx.x; i0 < end; i0 += 8 * kThreads) {
                 uint32_t kk[8];
 #pragma unroll
@@ -521,23 +564,20 @@ k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* _
                     if (i0 + u * kThreads < end) atomicAdd(&cnt[bin(kk[u])], 1u);
             }
         } else {
-            // Bloom probe fused into the level-2 pass: this level-1 partition's filter segments are
-            // contiguous and stay in L2 while the CTA works on it. Survivors are compacted into
-            // cmp[begin, begin + survivors) and counted by level-2 id.
-            const int lane = threadIdx.x & 31;
+            // the filter segments of this level-1 partition are shared by every CTA working on it
             for (int64_t i0 = begin; i0 < end; i0 += kProbeILP * kThreads) {
                 uint2 e[kProbeILP];
                 uint4 w0[kProbeILP], w1[kProbeILP];
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    e[u] = i < end ? __ldcs(&R.l1[i]) : make_uint2(0u, 0u);
+                    e[u] = i < end ? __ldcs(&l1[i]) : make_uint2(0u, 0u);
                 }
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
                     if (i < end) {
-                        const uint4* blk = bloom_block(d, p * P2 + bin(e[u].x), e[u].x);
+                        const uint4* blk = bloom_block(d, x.p * P2 + bin(e[u].x), e[u].x);
                         w0[u] = __ldg(blk);
                         w1[u] = __ldg(blk + 1);
                     }
@@ -560,30 +600,74 @@ k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* _
                     }
                 }
             }
-            // the survivors are read back below by bulk copies (async proxy)
-            asm volatile("fence.proxy.async.global;" ::: "memory");
-            __syncthreads();
-            src_end = begin + s_surv;
-            src = R.cmp;
-            if (threadIdx.x == 0)
-                atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSurvivors]),
-                          (unsigned long long)s_surv);
         }
         __syncthreads();
-        for (uint32_t q = threadIdx.x; q < P2; q += kThreads) {
-            const uint32_t c = cnt[q];
-            if (R.fine_cnt) R.fine_cnt[(int64_t)p * P2 + q] = c;
+        uint32_t* H = hist2 + R.h2_base + x.local_off * P2;
+        for (uint32_t q = threadIdx.x; q < P2; q += kThreads) H[(int64_t)q * x.ns + x.sl] = cnt[q];
+        if (threadIdx.x == 0 && bloom) {
+            slice_cnt2[t] = s_surv;
+            atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSurvivors]), (unsigned long long)s_surv);
         }
         __syncthreads();
-        block_scan_excl(cnt, (int)P2, tmp);
-        for (uint32_t q = threadIdx.x; q < P2; q += kThreads) {
-            cursor[q] = begin + cnt[q];
-            R.bounds[(int64_t)p * P2 + q] = begin + cnt[q];
-        }
-        if (threadIdx.x == 0 && p == P1 - 1) R.bounds[(int64_t)P1 * P2] = end;
+    }
+}
+
+// Level-2 scatter of one slice into its private runs of the level-2 buffer.
+__global__ void __launch_bounds__(kThreads)
+k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
+             const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
+             const int64_t* __restrict__ scan2, const uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords,
+             int max_bins) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned char* inbuf = smem;                                                // 2 tile buffers
+    uint2* stage = reinterpret_cast<uint2*>(smem + 2 * kTileBuf);               // [kTile]
+    int64_t* cursor = reinterpret_cast<int64_t*>(stage + kTile);                // [max_bins]
+    uint32_t* cnt = reinterpret_cast<uint32_t*>(cursor + max_bins);             // [max_bins]
+    __shared__ uint32_t tmp[kThreads / 32];
+    __shared__ __align__(8) uint64_t bars[2];
+    init_bars(bars);
+    uint32_t ph = 0;
+    const int64_t total = (int64_t)gwords[kGL2Slices + rel];
+    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const L2Slice x = l2_decode(seg_prefix, nj, seg_off, seg_ns, total_segs, t);
+        const JoinDesc& d = J[x.j];
+        const RelPlan& R = d.rel[rel];
+        const uint32_t P2 = d.pf.P2;
+        const int64_t begin = R.b1[x.p] + x.sl * kL2Slice;
+        const bool bloom = rel == 1 && d.bloom != nullptr && d.bloom_level == 2;
+        const int64_t end = bloom ? begin + slice_cnt2[t] : min_i64(R.b1[x.p + 1], begin + kL2Slice);
+        const int64_t* S2 = scan2 + R.h2_base;
+        const int64_t s0 = S2[0];
+        const int64_t* Sx = S2 + x.local_off * P2;
+        for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
         __syncthreads();
-        scatter_tiles(TileIn{src, nullptr, nullptr, false}, begin, src_end, bin, (int)P2, R.l2, src_end, cursor,
-                      cnt, tmp, stage, inbuf, bars, ph, &gwords[kGErrors]);
+        scatter_tiles(TileIn{bloom ? R.cmp : R.l1, nullptr, nullptr, false}, begin, end, Bin2{d.pf}, (int)P2, R.l2,
+                      R.n, cursor, cnt, tmp, stage, inbuf, bars, ph, &gwords[kGErrors]);
+    }
+}
+
+// Finest-partition starts from the level-2 scan: bounds[p*P2+q] = start of (p, q); bounds[P1*P2] =
+// the relation's level-2 total. One grid row per join.
+__global__ void k_l2_bounds(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
+                            const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns,
+                            const int64_t* __restrict__ scan2) {
+    for (int j = blockIdx.y; j < nj; j += gridDim.y) {
+        const JoinDesc& d = J[j];
+        if (d.pf.P2 <= 1) continue;
+        const RelPlan& R = d.rel[rel];
+        const int64_t P2 = d.pf.P2, nf = (int64_t)d.pf.P1 * P2;
+        const int64_t* S2 = scan2 + R.h2_base;
+        const int64_t s0 = S2[0];
+        const int64_t g0 = seg_prefix[j];
+        for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f <= nf; f += (int64_t)gridDim.x * blockDim.x) {
+            if (f == nf) {
+                const int64_t local_total = seg_off[seg_prefix[j + 1]] - seg_off[g0];
+                R.bounds[f] = S2[local_total * P2] - s0;
+                continue;
+            }
+            const int64_t g = g0 + f / P2, q = f % P2;
+            R.bounds[f] = S2[(seg_off[g] - seg_off[g0]) * P2 + q * (int64_t)seg_ns[g]] - s0;
+        }
     }
 }
 
@@ -595,7 +679,7 @@ k_l2_partition(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* _
 __global__ void __launch_bounds__(kThreads)
 k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ bloom_prefix,
               int smem_words, unsigned long long* gwords) {
-    extern __shared__ uint32_t seg[];
+    extern __shared__ __align__(16) uint32_t seg[];
     const int64_t total = bloom_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(bloom_prefix, nj, g);
@@ -632,10 +716,15 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
                 }
                 BloomKey bk;
                 bloom_key(kk[u], d.seg_blocks, k, bk);
-                uint32_t* blk = dst + local * nw + (int64_t)bk.block * 8;
+                // a 32-byte block is four 64-bit words: at most four atomics per key
+                unsigned long long* blk =
+                    reinterpret_cast<unsigned long long*>(dst + local * nw + (int64_t)bk.block * 8);
 #pragma unroll
-                for (int w = 0; w < 8; ++w)
-                    if (bk.mask[w]) atomicOr(blk + w, bk.mask[w]);
+                for (int w = 0; w < 4; ++w) {
+                    const unsigned long long m =
+                        (unsigned long long)bk.mask[2 * w] | ((unsigned long long)bk.mask[2 * w + 1] << 32);
+                    if (m) atomicOr(blk + w, m);
+                }
             }
         }
         __syncthreads();
@@ -658,7 +747,7 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
 // (src/kernel_functions.cu:356-395).
 __device__ __forceinline__ void fine_range(const RelPlan& R, int64_t f, int64_t& begin, int64_t& n) {
     begin = R.bounds[f];
-    n = R.fine_cnt ? (int64_t)R.fine_cnt[f] : R.bounds[f + 1] - begin;
+    n = R.bounds[f + 1] - begin;
 }
 
 // Walks domain `dom` of join d and calls emit(b_begin, b_len, p_begin, p_len, split, build_s)
@@ -1028,7 +1117,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     cudaError_t err;
     if (!attrs_done) {
         if ((err = set_smem_attr((const void*)k_l1_scatter, scatter_smem(kMaxP1))) != cudaSuccess) return err;
-        if ((err = set_smem_attr((const void*)k_l2_partition, scatter_smem(kMaxP2))) != cudaSuccess) return err;
+        if ((err = set_smem_attr((const void*)k_l2_scatter, scatter_smem(kMaxP2))) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_bloom_build, kBloomSmemWords * 4)) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_probe, probe_smem_bytes(kMaxTable, 1))) != cudaSuccess)
             return err;
@@ -1082,9 +1171,27 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             ++launches;
         }
         if (a.total_segs > 0) {
-            k_l2_partition<<<grid_for(a.total_segs, sms, 2), kThreads, scatter_smem(a.max_p2), st>>>(
-                a.J, a.nj, rel, a.seg_prefix, a.gwords, a.max_p2);
+            const int pb = (int)std::min<int64_t>((a.total_segs + 1 + 255) / 256, (int64_t)sms * 8);
+            k_l2_plan<<<pb, 256, 0, st>>>(a.J, a.nj, rel, a.seg_prefix, a.seg_ns);
             ++launches;
+            if ((err = enqueue_scan(a.seg_ns, a.seg_off, a.total_segs + 1, a.scan_tmp,
+                                    reinterpret_cast<int64_t*>(a.gwords + kGL2Slices + rel), st)) != cudaSuccess)
+                return err;
+            uint32_t* h2 = a.hist2 + a.h2_begin[rel];
+            if ((err = cudaMemsetAsync(h2, 0, (size_t)a.h2_len[rel] * 4, st)) != cudaSuccess) return err;
+            k_l2_hist<<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4, st>>>(
+                a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2, a.gwords);
+            ++launches;
+            if ((err = enqueue_scan(h2, a.hist2_scan + a.h2_begin[rel], a.h2_len[rel], a.scan_tmp, nullptr, st)) !=
+                cudaSuccess)
+                return err;
+            k_l2_scatter<<<grid_for(a.l2_slice_cap[rel], sms, 2), kThreads, scatter_smem(a.max_p2), st>>>(
+                a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2_scan, a.slice_cnt2, a.gwords,
+                a.max_p2);
+            dim3 grid((unsigned)std::min<int64_t>(((int64_t)a.max_p1 * a.max_p2 + 1 + 255) / 256, 4096),
+                      (unsigned)std::min(a.nj, 65535));
+            k_l2_bounds<<<grid, 256, 0, st>>>(a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.hist2_scan);
+            launches += 2;
         }
         mark(m0 + 3);
     }

@@ -41,6 +41,14 @@ struct PipelineArgs {
     int num_sms;
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
     int stages;                       // kRunPartR | kRunBloom | kRunPartS | kRunProbe
+    // level 2 (planned on the device)
+    uint32_t* seg_ns;                 // [total_segs + 1] slices per level-1 partition
+    int64_t* seg_off;                 // [total_segs + 1] their exclusive scan
+    uint32_t* hist2;                  // level-2 histograms of both relations
+    int64_t* hist2_scan;              // their exclusive scan
+    int64_t h2_begin[2], h2_len[2];   // range of each relation in hist2
+    uint32_t* slice_cnt2;             // [max slices] survivors per slice (level-2 Bloom probe)
+    int64_t l2_slice_cap[2];          // upper bound of level-2 slices per relation
 };
 
 // Pipeline parts (a full join runs all four; the reference-named entry points run subsets).
