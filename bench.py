@@ -356,6 +356,11 @@ def main():
     ap.add_argument("--bloom", type=int, default=None, help="override Bloom on/off")
     ap.add_argument("--bloom-level", type=int, default=0,
                     help="S pass that probes the filter (1 first, 2 second, 0 planner's choice)")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="override |R| = |S| (a smaller case of the same generator, e.g. for ncu)")
+    ap.add_argument("--p1", type=int, default=0, help="override the level-1 fan-out")
+    ap.add_argument("--p2", type=int, default=0, help="override the level-2 fan-out")
+    ap.add_argument("--table", type=int, default=0, help="override table_capacity")
     args = ap.parse_args()
     if args.steps > 64:
         ap.error("--steps above 64: per-stage events keep the last 64 runs")
@@ -366,6 +371,10 @@ def main():
     wl = dict(WORKLOADS[args.workload])
     if args.bloom is not None:
         wl["bloom"] = args.bloom
+    if args.rows > 0:
+        wl["n_r"] = wl["n_s"] = args.rows
+        wl["name"] = f"join {args.rows} x {args.rows}, 10% match" + (
+            f", Bloom {wl['bpk']:g} bits/key k={wl['k']}" if wl["bloom"] else "")
     if args.impl == "reference":
         return run_reference_arm(args, wl)
 
@@ -397,7 +406,8 @@ def main():
     out_r = torch.empty(cap, dtype=i32, device="cuda")
     out_s = torch.empty(cap, dtype=i32, device="cuda")
     j = bj.Join(use_bloom=wl["bloom"], bloom_bits_per_key=wl["bpk"], bloom_num_hashes=wl["k"],
-                bloom_probe_level=args.bloom_level, use_cuda_graph=1, profile_stages=1)
+                bloom_probe_level=args.bloom_level, use_cuda_graph=1, profile_stages=1,
+                partition_size=args.p1, second_partition_size=args.p2, table_capacity=args.table)
 
     def step():
         j.run(rk, rv, nr, sk, sv, ns, out_r, out_s, cap, stream=sp)
@@ -498,7 +508,8 @@ def main():
                        "bloom_bits_per_key": wl["bpk"] if wl["bloom"] else 0,
                        "bloom_hashes": st.bloom_num_hashes, "partition_size": st.partition_size,
                        "second_partition_size": st.second_partition_size,
-                       "l2": "no flush: each step streams 10+ GB of inputs, far above the 126 MB L2",
+                       "l2": f"no flush: each step streams {8 * (nr + ns) / 1e9:.2f} GB of inputs"
+                             + (", far above the 126 MB L2" if 8 * (nr + ns) > 4 * 126e6 else ""),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},

@@ -21,7 +21,7 @@ namespace brig {
 constexpr int kMaxP1 = 4096;          // first-level fan-out (the reference caps at PARTITION_MAX=2048,
                                       // src/kernel_functions.h:15)
 constexpr int kMaxP2 = 1024;          // second-level fan-out (SECOND_PASS_MAX=4096, :14)
-constexpr int kMaxTable = 8192;       // build-side tuples per shared-memory table (largest allowed)
+constexpr int kMaxTable = 4096;       // build-side tuples per shared-memory table (largest allowed)
 constexpr int kDefaultTable = 4096;   // default table capacity
 constexpr int kDefaultChunk = 65536;  // default streamed tuples per probe task
 constexpr int kMinTable = 256;
@@ -121,17 +121,24 @@ struct BloomKey {
 
 BRIG_HD uint64_t bloom_hash(uint32_t key) { return mix64((uint64_t)key ^ 0x6a09e667f3bcc909ull); }
 
+// Bits 40..63 of the hash pick the block (24-bit multiply-shift range reduction).
+BRIG_HD uint32_t bloom_block_of(uint64_t g, uint32_t seg_blocks) {
+    return (uint32_t)(((g >> 40) * (uint64_t)seg_blocks) >> 24);
+}
+// Bits to set/test in word w (0..7) of the block: hash i < k sets one bit of word i % 8, at the
+// bit position given by 5 hash bits (bits 5w.. of g for i < 8, of g2 = mix64(g) for i >= 8).
+BRIG_HD uint32_t bloom_word_mask(uint64_t g, uint64_t g2, int k, int w) {
+    uint32_t m = (w < k) ? (1u << ((uint32_t)(g >> (5 * w)) & 31u)) : 0u;
+    if (w + 8 < k) m |= 1u << ((uint32_t)(g2 >> (5 * w)) & 31u);
+    return m;
+}
+
 BRIG_HD void bloom_key(uint32_t key, uint32_t seg_blocks, int k, BloomKey& bk) {
     const uint64_t g = bloom_hash(key);
-    // bits 40..63 pick the block (24-bit multiply-shift range reduction), bits 0..39 the word bits
-    bk.block = (uint32_t)(((g >> 40) * (uint64_t)seg_blocks) >> 24);
+    bk.block = bloom_block_of(g, seg_blocks);
     const uint64_t g2 = k > 8 ? mix64(g) : 0ull;
 #pragma unroll
-    for (int w = 0; w < 8; ++w) {
-        uint32_t m = (w < k) ? (1u << ((uint32_t)(g >> (5 * w)) & 31u)) : 0u;
-        if (w + 8 < k) m |= 1u << ((uint32_t)(g2 >> (5 * w)) & 31u);
-        bk.mask[w] = m;
-    }
+    for (int w = 0; w < 8; ++w) bk.mask[w] = bloom_word_mask(g, g2, k, w);
 }
 
 // ---- per-join descriptor (device resident) ------------------------------------------------------

@@ -365,7 +365,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
     const int C = cfg.s_chunk > 0 ? cfg.s_chunk : kDefaultChunk;
     if (T < kMinTable || T > kMaxTable || !is_pow2(T))
-        fail(BRIG_E_INVALID, "table_capacity must be a power of two in [256, 8192]");
+        fail(BRIG_E_INVALID, "table_capacity must be a power of two in [256, 4096]");
     if (C < 1) fail(BRIG_E_INVALID, "s_chunk must be >= 1");
     JoinDesc* hJ = reinterpret_cast<JoinDesc*>(meta_host);
     int64_t* hpre = reinterpret_cast<int64_t*>(meta_host + (size_t)nj * sizeof(JoinDesc));
@@ -582,7 +582,7 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
 brig_join_config Engine::autotune(const std::vector<JoinIO>& joins, cudaStream_t stream) {
     // Candidates: shared-memory table capacity (build-chunk size, which also sets the partition
     // count through the planner's fill target) x largest level-1 fan-out.
-    const int tables[] = {2048, 4096, 8192};
+    const int tables[] = {1024, 2048, 4096};
     const int l1bits[] = {8, 9, 10};
     const brig_join_config base = cfg_;
     cudaEvent_t e0, e1;

@@ -192,6 +192,8 @@ struct TileIn {
     bool bulk_kv;
 };
 constexpr size_t kTileBuf = (size_t)(kTile + 2) * 8;  // one input buffer
+constexpr int kProbeChunk = kMaxTable;                      // tuples per probe item (build or stream)
+constexpr size_t kProbeBuf = (size_t)(kProbeChunk + 2) * 8; // one probe item buffer
 
 __device__ __forceinline__ uint32_t tile_mis(const TileIn& in, int64_t t0) {
     return in.p ? (uint32_t)((((uintptr_t)(in.p + t0)) & 15) ? 1 : 0) : 0u;
@@ -202,6 +204,10 @@ __device__ __forceinline__ void tile_issue(const TileIn& in, int64_t t0, int tn,
     if (in.p) {
         const uint32_t mis = tile_mis(in, t0);
         const uint32_t bytes = (((uint32_t)tn + mis) * 8u + 15u) & ~15u;
+        if (bytes == 0) {
+            mbar_arrive(bar);
+            return;
+        }
         mbar_arrive_tx(bar, bytes);
         bulk_g2s(buf, in.p + t0 - mis, bytes, bar);
     } else if (in.bulk_kv && (tn & ~3) > 0) {
@@ -714,15 +720,16 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
                     atomicAdd(&gwords[kGErrors], 1ull);
                     continue;
                 }
-                BloomKey bk;
-                bloom_key(kk[u], d.seg_blocks, k, bk);
-                // a 32-byte block is four 64-bit words: at most four atomics per key
-                unsigned long long* blk =
-                    reinterpret_cast<unsigned long long*>(dst + local * nw + (int64_t)bk.block * 8);
+                const uint64_t g = bloom_hash(kk[u]);
+                const uint64_t g2 = k > 8 ? mix64(g) : 0ull;
+                uint32_t* blk = dst + local * nw + (int64_t)bloom_block_of(g, d.seg_blocks) * 8;
+                // Lane l starts at word l % 8 of its block, so the lanes of one atomic instruction
+                // touch different words and mostly different shared-memory banks (all lanes on
+                // the same word would be an 8-way bank conflict, since blocks are 8 words).
 #pragma unroll
-                for (int w = 0; w < 4; ++w) {
-                    const unsigned long long m =
-                        (unsigned long long)bk.mask[2 * w] | ((unsigned long long)bk.mask[2 * w + 1] << 32);
+                for (int t = 0; t < 8; ++t) {
+                    const int w = (t + (int)threadIdx.x) & 7;
+                    const uint32_t m = bloom_word_mask(g, g2, k, w);
                     if (m) atomicOr(blk + w, m);
                 }
             }
@@ -750,20 +757,27 @@ __device__ __forceinline__ void fine_range(const RelPlan& R, int64_t f, int64_t&
     n = R.bounds[f + 1] - begin;
 }
 
-// Walks domain `dom` of join d and calls emit(b_begin, b_len, p_begin, p_len, split, build_s)
-// for every task, in order.
+// Walks domain `dom` of join d with one warp and calls emit(b_begin, b_len, p_begin, p_len, split,
+// build_s) for every task, in order, on every lane (the grouping state is warp-uniform). Lanes load
+// 32 partitions' bounds at a time; the greedy grouping then steps through them with shuffles.
 template <class Emit>
 __device__ void walk_domain(const JoinDesc& d, int64_t dom, Emit&& emit) {
+    const int lane = threadIdx.x & 31;
     const int64_t P2 = d.pf.P2;
     const int64_t f_first = P2 > 1 ? dom * P2 : 0;
     const int64_t f_last = P2 > 1 ? f_first + P2 : (int64_t)d.pf.P1;
     int64_t tot_r = 0, tot_s = 0;
-    for (int64_t f = f_first; f < f_last; ++f) {
+    for (int64_t f = f_first + lane; f < f_last; f += 32) {
         int64_t b, n;
         fine_range(d.rel[0], f, b, n);
         tot_r += n;
         fine_range(d.rel[1], f, b, n);
         tot_s += n;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        tot_r += __shfl_xor_sync(0xffffffffu, tot_r, o);
+        tot_s += __shfl_xor_sync(0xffffffffu, tot_s, o);
     }
     if (tot_r == 0 || tot_s == 0) return;
     const bool bs = tot_s < tot_r;
@@ -778,69 +792,90 @@ __device__ void walk_domain(const JoinDesc& d, int64_t dom, Emit&& emit) {
         nb = 0;
         np = 0;
     };
-    for (int64_t f = f_first; f < f_last; ++f) {
-        int64_t bb, bn, pb, pn;
-        fine_range(B, f, bb, bn);
-        fine_range(P, f, pb, pn);
-        if (bn > T) {
-            close();
-            if (pn > 0)
-                for (int64_t c = 0; c * T < bn; ++c) emit(bb + c * T, min_i64(T, bn - c * T), pb, pn, true, bs);
-            continue;
+    for (int64_t f0 = f_first; f0 < f_last; f0 += 32) {
+        int64_t mb = 0, mbn = 0, mp = 0, mpn = 0;
+        if (f0 + lane < f_last) {
+            fine_range(B, f0 + lane, mb, mbn);
+            fine_range(P, f0 + lane, mp, mpn);
         }
-        if (nb + bn > T) close();
-        if (gb0 < 0) {
-            gb0 = bb;
-            gp0 = pb;
+        const int cnt = (int)min_i64(32, f_last - f0);
+        for (int l = 0; l < cnt; ++l) {
+            const int64_t bb = __shfl_sync(0xffffffffu, mb, l), bn = __shfl_sync(0xffffffffu, mbn, l);
+            const int64_t pb = __shfl_sync(0xffffffffu, mp, l), pn = __shfl_sync(0xffffffffu, mpn, l);
+            if (bn > T) {
+                close();
+                if (pn > 0)
+                    for (int64_t c = 0; c * T < bn; ++c) emit(bb + c * T, min_i64(T, bn - c * T), pb, pn, true, bs);
+                continue;
+            }
+            if (nb + bn > T) close();
+            if (gb0 < 0) {
+                gb0 = bb;
+                gp0 = pb;
+            }
+            nb += bn;
+            np += pn;
         }
-        nb += bn;
-        np += pn;
     }
     close();
 }
 
-__global__ void k_tasks_count(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ dom_prefix,
-                              uint32_t* __restrict__ tcount) {
+constexpr int kTaskWarps = 8;  // warps (domains) per task-builder CTA
+
+__global__ void __launch_bounds__(kTaskWarps * 32)
+k_tasks_count(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ dom_prefix,
+              uint32_t* __restrict__ tcount) {
     const int64_t total = dom_prefix[nj];
-    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= total;
-         g += (int64_t)gridDim.x * blockDim.x) {
-        if (g == total) { tcount[g] = 0; continue; }
+    const int64_t warp0 = (int64_t)blockIdx.x * kTaskWarps + (threadIdx.x >> 5);
+    for (int64_t g = warp0; g <= total; g += (int64_t)gridDim.x * kTaskWarps) {
+        if (g == total) {
+            if ((threadIdx.x & 31) == 0) tcount[g] = 0;
+            continue;
+        }
         const int j = find_owner(dom_prefix, nj, g);
         uint32_t n = 0;
         walk_domain(J[j], g - dom_prefix[j], [&](int64_t, int64_t, int64_t, int64_t, bool, bool) { ++n; });
-        tcount[g] = n;
+        if ((threadIdx.x & 31) == 0) tcount[g] = n;
     }
 }
 
-__global__ void k_tasks_write(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ dom_prefix,
-                              const int64_t* __restrict__ toff, Task* __restrict__ tasks, int64_t task_cap,
-                              unsigned long long* gwords) {
+__global__ void __launch_bounds__(kTaskWarps * 32)
+k_tasks_write(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ dom_prefix,
+              const int64_t* __restrict__ toff, Task* __restrict__ tasks, int64_t task_cap,
+              unsigned long long* gwords) {
     const int64_t total = dom_prefix[nj];
-    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < total;
-         g += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp0 = (int64_t)blockIdx.x * kTaskWarps + (threadIdx.x >> 5);
+    for (int64_t g = warp0; g < total; g += (int64_t)gridDim.x * kTaskWarps) {
         const int j = find_owner(dom_prefix, nj, g);
         const JoinDesc& d = J[j];
         int64_t t = toff[g];
         int64_t n = 0, nsplit = 0;
         walk_domain(d, g - dom_prefix[j], [&](int64_t b0, int64_t bn, int64_t p0, int64_t pn, bool split, bool bs) {
-            if (t < 0 || t >= task_cap) {
-                atomicAdd(&gwords[kGErrors], 1ull);
-                return;
+            if (lane == 0) {
+                if (t < 0 || t >= task_cap) {
+                    atomicAdd(&gwords[kGErrors], 1ull);
+                } else {
+                    Task tk;
+                    tk.join = j;
+                    tk.flags = (bs ? kTaskBuildS : 0u) | (split ? kTaskSplit : 0u);
+                    tk.b_begin = b0;
+                    tk.b_len = (uint32_t)bn;
+                    tk.p_begin = p0;
+                    tk.p_len = (uint32_t)pn;
+                    tasks[t] = tk;
+                }
             }
-            Task tk;
-            tk.join = j;
-            tk.flags = (bs ? kTaskBuildS : 0u) | (split ? kTaskSplit : 0u);
-            tk.b_begin = b0;
-            tk.b_len = (uint32_t)bn;
-            tk.p_begin = p0;
-            tk.p_len = (uint32_t)pn;
-            tasks[t++] = tk;
+            ++t;
             ++n;
             nsplit += split ? 1 : 0;
         });
-        if (n) atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntTasks]), (unsigned long long)n);
-        if (nsplit)
-            atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSplitTasks]), (unsigned long long)nsplit);
+        if (lane == 0) {
+            if (n) atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntTasks]), (unsigned long long)n);
+            if (nsplit)
+                atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSplitTasks]),
+                          (unsigned long long)nsplit);
+        }
     }
 }
 
@@ -868,28 +903,77 @@ __device__ __forceinline__ void warp_flush(const JoinDesc& d, const uint32_t* wr
     __syncwarp();
 }
 
-// Persistent probe kernel. Each CTA repeatedly takes the next task, builds a bucketised table of
-// the task's build chunk in shared memory (count per bucket, exclusive scan, place), then streams
-// the other side through it: the streamed tuples arrive in chunks of kChunk by bulk copy (the next
-// chunk in flight while the current one is probed), every streamed tuple scans its bucket, and
-// every key-equal entry is a match. After placement off[b] holds the end of bucket b, so bucket b
-// spans [off[b-1], off[b]).
-constexpr int kChunk = 2048;                                // streamed tuples per bulk copy
-constexpr size_t kChunkBuf = (size_t)(kChunk + 2) * 8;      // one chunk buffer (alignment slack)
+// Persistent probe kernel. A task's build chunk and its streamed chunks reach shared memory as a
+// sequence of bulk copies ("items": build, chunk 0, chunk 1, ...; then the next task's items) through
+// a ring of two buffers: item i lives in buffer i % 2, and when the CTA has finished with item i
+// thread 0 issues item i + 2, so one item is always in flight while the other is processed. Tasks
+// are taken from the global queue one ahead of their use. Per task the CTA builds a bucketised
+// table of the build chunk (count per bucket, exclusive scan, place; after placement off[b] holds
+// the end of bucket b, so bucket b spans [off[b-1], off[b])), then streams every chunk through it:
+// each streamed tuple scans its bucket and every key-equal entry is a match.
+constexpr int kRing = 4;  // tasks held by a CTA: the one being processed and the ones being loaded
 
-__global__ void __launch_bounds__(kThreads, 2)
+__device__ __forceinline__ int task_items(const Task& t) {
+    return 1 + (int)((t.p_len + (uint32_t)kProbeChunk - 1) / (uint32_t)kProbeChunk);
+}
+// Source and length of item k of task t (0 = build chunk, 1.. = streamed chunks).
+__device__ __forceinline__ const uint2* item_src(const JoinDesc& d, const Task& t, int k, int& n) {
+    const bool bs = (t.flags & kTaskBuildS) != 0;
+    if (k == 0) {
+        n = (int)min_i64(kProbeChunk, (int64_t)t.b_len);  // b_len <= table_cap <= kProbeChunk by construction
+        return final_buf(d, bs ? 1 : 0) + t.b_begin;
+    }
+    const int64_t c0 = (int64_t)(k - 1) * kProbeChunk;
+    n = (int)min_i64(kProbeChunk, (int64_t)t.p_len - c0);
+    return final_buf(d, bs ? 0 : 1) + t.p_begin + c0;
+}
+
+struct ProbeShared {
+    Task ring[kRing];
+    int valid[kRing];
+    int ps, pi;               // next item to issue: ring slot and item index
+    long long issued;         // items issued so far
+};
+
+// Thread 0: dequeues the next task into ring slot `slot`.
+__device__ __forceinline__ void dequeue(ProbeShared& sh, int slot, const Task* __restrict__ tasks,
+                                        unsigned long long* gwords, long long ntasks) {
+    const long long t = (long long)atomicAdd(&gwords[kGQueue], 1ull);
+    sh.valid[slot] = t < ntasks;
+    if (t < ntasks) sh.ring[slot] = tasks[t];
+}
+
+// Thread 0: issues the next item of the sequence into buffer (issued % 2), dequeuing tasks as the
+// sequence reaches them. Past the last task nothing is issued.
+__device__ __forceinline__ void produce(ProbeShared& sh, const JoinDesc* __restrict__ J, const Task* __restrict__ tasks,
+                                        unsigned long long* gwords, long long ntasks, unsigned char* bufs,
+                                        uint64_t* bars) {
+    if (!sh.valid[sh.ps]) return;
+    const Task& t = sh.ring[sh.ps];
+    int n;
+    const uint2* src = item_src(J[t.join], t, sh.pi, n);
+    const int b = (int)(sh.issued & 1);
+    tile_issue(TileIn{src, nullptr, nullptr, false}, 0, n, bufs + b * kProbeBuf, &bars[b]);
+    ++sh.issued;
+    if (++sh.pi == task_items(t)) {
+        sh.pi = 0;
+        sh.ps = (sh.ps + 1) % kRing;
+        dequeue(sh, sh.ps, tasks, gwords, ntasks);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
 k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned long long* gwords,
         int table_cap, int emit_key) {
     extern __shared__ __align__(16) unsigned char smem[];
-    unsigned char* sbuf = smem;                                                     // 2 chunk buffers
-    uint2* table = reinterpret_cast<uint2*>(smem + 2 * kChunkBuf);                  // [table_cap]
+    unsigned char* bufs = smem;                                                     // 2 item buffers
+    uint2* table = reinterpret_cast<uint2*>(smem + 2 * kProbeBuf);                  // [table_cap]
     uint32_t* off = reinterpret_cast<uint32_t*>(table + table_cap);                 // [table_cap] (+pad)
     uint32_t* wbuf = off + table_cap + 4;
     __shared__ uint32_t tmp[kThreads / 32];
-    __shared__ long long s_task;
+    __shared__ ProbeShared sh;
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
-    uint32_t ph = 0;
     unsigned long long* errors = &gwords[kGErrors];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int words_per_warp = kWarpBuf * (emit_key ? 3 : 2);
@@ -899,12 +983,19 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     int wcount = 0;
     int cur = -1;
     const long long ntasks = (long long)gwords[kGTasks];
-    for (;;) {
-        if (threadIdx.x == 0) s_task = (long long)atomicAdd(&gwords[kGQueue], 1ull);
-        __syncthreads();
-        const long long t = s_task;
-        if (t >= ntasks) break;
-        const Task tk = tasks[t];
+    if (threadIdx.x == 0) {
+        sh.ps = 0;
+        sh.pi = 0;
+        sh.issued = 0;
+        dequeue(sh, 0, tasks, gwords, ntasks);
+        produce(sh, J, tasks, gwords, ntasks, bufs, bars);
+        produce(sh, J, tasks, gwords, ntasks, bufs, bars);
+    }
+    __syncthreads();
+    long long consumed = 0;
+    for (int cs = 0;; cs = (cs + 1) % kRing) {
+        if (!sh.valid[cs]) break;
+        const Task tk = sh.ring[cs];
         if (tk.join != cur) {
             if (cur >= 0 && wcount > 0) warp_flush(J[cur], wr, ws, wk, wcount, lane);
             wcount = 0;
@@ -912,40 +1003,44 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         }
         const JoinDesc& d = J[tk.join];
         const bool bs = (tk.flags & kTaskBuildS) != 0;
-        const uint2* __restrict__ Bb = final_buf(d, bs ? 1 : 0) + tk.b_begin;   // build side
-        const uint2* Pb = final_buf(d, bs ? 0 : 1) + tk.p_begin;                // streamed side
-        const uint32_t nr = min(tk.b_len, (uint32_t)table_cap);
-        if (tk.b_len > (uint32_t)table_cap && threadIdx.x == 0) atomicAdd(errors, 1ull);
-        const uint32_t np = tk.p_len;
-        const int nchunks = (int)((np + kChunk - 1) / kChunk);
-        // first streamed chunk flies while the table is built
-        const TileIn pin{Pb, nullptr, nullptr, false};
-        if (threadIdx.x == 0 && nchunks > 0) tile_issue(pin, 0, (int)min(np, (uint32_t)kChunk), sbuf, &bars[0]);
+        const int nitems = task_items(tk);
+        // ---- item 0: build the table
+        int nr;
+        const uint2* bsrc = item_src(d, tk, 0, nr);
+        if (nr > table_cap) {
+            if (threadIdx.x == 0) atomicAdd(errors, 1ull);
+            nr = table_cap;
+        }
         uint32_t nb = 32;
-        while (nb < nr) nb <<= 1;
+        while (nb < (uint32_t)nr) nb <<= 1;
         const uint32_t mask = nb - 1;
         for (uint32_t i = threadIdx.x; i < nb; i += kThreads) off[i] = 0;
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < nr; i += kThreads)
-            atomicAdd(&off[bucket_of(__ldg(&Bb[i].x), mask)], 1u);
-        __syncthreads();
-        block_scan_excl(off, (int)nb, tmp);
-        for (uint32_t i = threadIdx.x; i < nr; i += kThreads) {
-            const uint2 e = __ldg(&Bb[i]);
-            const uint32_t pos = atomicAdd(&off[bucket_of(e.x, mask)], 1u);
-            table[pos] = e;
+        {
+            const int b = (int)(consumed & 1);
+            mbar_wait(&bars[b], (uint32_t)((consumed >> 1) & 1), errors);
+            __syncthreads();
+            const uint2* in = reinterpret_cast<const uint2*>(bufs + b * kProbeBuf) +
+                              tile_mis(TileIn{bsrc, nullptr, nullptr, false}, 0);
+            for (int i = threadIdx.x; i < nr; i += kThreads) atomicAdd(&off[bucket_of(in[i].x, mask)], 1u);
+            __syncthreads();
+            block_scan_excl(off, (int)nb, tmp);
+            for (int i = threadIdx.x; i < nr; i += kThreads) {
+                const uint2 e = in[i];
+                table[atomicAdd(&off[bucket_of(e.x, mask)], 1u)] = e;
+            }
+            __syncthreads();
+            ++consumed;
+            if (threadIdx.x == 0) produce(sh, J, tasks, gwords, ntasks, bufs, bars);
+            __syncthreads();
         }
-        __syncthreads();
-        for (int c = 0; c < nchunks; ++c) {
-            const int b = c & 1;
-            const int64_t c0 = (int64_t)c * kChunk;
-            const int cn = (int)min((int64_t)kChunk, (int64_t)np - c0);
-            if (threadIdx.x == 0 && c + 1 < nchunks)
-                tile_issue(pin, c0 + kChunk, (int)min((int64_t)kChunk, (int64_t)np - c0 - kChunk),
-                           sbuf + (b ^ 1) * kChunkBuf, &bars[b ^ 1]);
-            mbar_wait(&bars[b], (ph >> b) & 1u, errors);
-            ph ^= 1u << b;
-            const uint2* chunk = reinterpret_cast<const uint2*>(sbuf + b * kChunkBuf) + tile_mis(pin, c0);
+        // ---- items 1..: stream the other side through the table
+        for (int k = 1; k < nitems; ++k) {
+            int cn;
+            const uint2* csrc = item_src(d, tk, k, cn);
+            const int b = (int)(consumed & 1);
+            mbar_wait(&bars[b], (uint32_t)((consumed >> 1) & 1), errors);
+            const uint2* chunk = reinterpret_cast<const uint2*>(bufs + b * kProbeBuf) +
+                                 tile_mis(TileIn{csrc, nullptr, nullptr, false}, 0);
             for (int base = 0; base < cn; base += kThreads) {
                 const int i = base + (int)threadIdx.x;
                 uint2 e = make_uint2(0u, 0u);
@@ -983,7 +1078,10 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
                     }
                 }
             }
-            __syncthreads();  // chunk buffer b is free for the copy issued next iteration
+            __syncthreads();  // buffer b is free: refill it with item consumed + 2
+            ++consumed;
+            if (threadIdx.x == 0) produce(sh, J, tasks, gwords, ntasks, bufs, bars);
+            __syncthreads();  // ring updates by produce() visible before the next task is read
         }
     }
     if (cur >= 0 && wcount > 0) warp_flush(J[cur], wr, ws, wk, wcount, lane);
@@ -1093,7 +1191,7 @@ cudaError_t enqueue_scan(const uint32_t* in, int64_t* out, int64_t n, int64_t* t
 }
 
 size_t probe_smem_bytes(int table_cap, int emit_key) {
-    return 2 * kChunkBuf + (size_t)table_cap * 8 + ((size_t)table_cap + 4) * 4 +
+    return 2 * kProbeBuf + (size_t)table_cap * 8 + ((size_t)table_cap + 4) * 4 +
            (size_t)(kThreads / 32) * kWarpBuf * (emit_key ? 3 : 2) * 4;
 }
 
@@ -1204,14 +1302,14 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     }
     {
         const int64_t n = a.total_domains + 1;
-        const int blocks = (int)std::min<int64_t>((n + 127) / 128, (int64_t)sms * 8);
-        k_tasks_count<<<blocks, 128, 0, st>>>(a.J, a.nj, a.dom_prefix, a.tcount);
+        const int blocks = (int)std::min<int64_t>((n + kTaskWarps - 1) / kTaskWarps, (int64_t)sms * 16);
+        k_tasks_count<<<blocks, kTaskWarps * 32, 0, st>>>(a.J, a.nj, a.dom_prefix, a.tcount);
         ++launches;
         if ((err = enqueue_scan(a.tcount, a.toff, n, a.scan_tmp,
                                 reinterpret_cast<int64_t*>(a.gwords + kGTasks), st)) != cudaSuccess)
             return err;
-        k_tasks_write<<<blocks, 128, 0, st>>>(a.J, a.nj, a.dom_prefix, a.toff, a.tasks, a.task_cap,
-                                              a.gwords);
+        k_tasks_write<<<blocks, kTaskWarps * 32, 0, st>>>(a.J, a.nj, a.dom_prefix, a.toff, a.tasks, a.task_cap,
+                                                          a.gwords);
         ++launches;
     }
     mark(10);

@@ -63,7 +63,7 @@ typedef struct brig_join_config {
     double  bloom_bits_per_key;     /* filter size when bloom_num_bits == 0; default 10 */
     int64_t bloom_num_bits;         /* total filter bits (--num_bits); 0 = bits_per_key * |R| */
     int32_t table_capacity;         /* max build-side tuples per shared-memory table, power of two
-                                       in [256, 8192]; 0 = 4096 (the reference's HT_SIZE is 10007,
+                                       in [256, 4096]; 0 = 4096 (the reference's HT_SIZE is 10007,
                                        src/common.h:15) */
     int32_t s_chunk;                /* max streamed tuples per probe task; 0 = 65536 */
     int32_t emit_key;               /* 1 = also write the key of each pair (GPU_answer array,

@@ -51,7 +51,7 @@ def test_modulo_mode(bj, oracle, torch_cuda, p1, p2, bloom):
             second_partition_size=p2, use_bloom=bloom)
 
 
-@pytest.mark.parametrize("table", [256, 1024, 8192])
+@pytest.mark.parametrize("table", [256, 1024, 4096])
 def test_duplicates_and_split_path(bj, oracle, torch_cuda, table):
     rng = np.random.default_rng(table)
     rk = rng.integers(0, 300, 20_000, dtype=np.uint32)     # heavy duplicates in R
