@@ -163,6 +163,22 @@ def run_reference_arm(args, wl):
     return 0
 
 
+# ---- multi-rank aggregation (replicas: one independent join per GPU) -------------------------------
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest x over all ranks (the job's time is its slowest rank's); x itself on one rank."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(world: int, steps: int, nr: int, ns: int, ms_total: float) -> float:
+    """Tuples per second over all ranks: every rank joins its own |R| + |S| tuples per step."""
+    return world * steps * (nr + ns) / (ms_total / 1e3)
+
+
 # ---- per-stage algorithmic bytes ------------------------------------------------------------------
 def stage_bytes(nr, ns, surv, matches, bloom_bits):
     """Minimum bytes each stage must move (read inputs once, write outputs once)."""
@@ -447,12 +463,9 @@ def main():
     launches = bj.kernel_launches() - launches0
     ms_total = ev0.elapsed_time(ev1)
     st = j.stats()
-    if dist:
-        t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(ms_total, dist, "cuda")
     ms_step = ms_total / args.steps
-    value = world * args.steps * (nr + ns) / (ms_total / 1e3)
+    value = whole_job_value(world, args.steps, nr, ns, ms_total)
 
     peak, peak_kind = peaks()
     avg = stages

@@ -75,6 +75,7 @@ struct Shape {
     size_t total = 0;           // workspace bytes
     int max_p1 = 1, max_p2 = 1, max_seg_words = 0, bloom_smem_words = 0;
     bool any_bloom = false;
+    bool any_bloom_l1 = false;
 };
 
 // Lays out `nj` joins in one workspace; fills jo[0..nj) and sh. Allocates nothing.

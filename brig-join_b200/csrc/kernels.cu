@@ -179,54 +179,59 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, unsign
         if (mbar_try_wait(bar, parity)) return;
 }
 
-// Where the tuples of a tile come from: packed tuples in an engine buffer (p), or the caller's
-// separate key/value arrays (k, v). Packed tiles are copied from the 16-byte boundary at or below
-// their first tuple (engine buffers are padded, so reading up to 8 bytes past either end stays
-// inside the workspace). Key/value tiles are bulk-copied when both arrays are 16-byte aligned at
-// tile starts; the last (tn mod 4) tuples of a tile, or every tuple of unaligned arrays, are
-// read with ordinary loads, so nothing outside the caller's arrays is read.
-struct TileIn {
-    const uint2* p;
-    const uint32_t* k;
-    const uint32_t* v;
-    bool bulk_kv;
-};
+// Where the tuples of a tile come from. PackedTiles: (key, value) pairs in an engine buffer; a tile
+// is copied from the 16-byte boundary at or below its first tuple (engine buffers are padded, so
+// reading up to 8 bytes past either end stays inside the workspace). KvTiles: the caller's separate
+// key and value arrays, bulk-copied when both are 16-byte aligned at tile starts; the last
+// (tn mod 4) tuples of a tile, or every tuple of unaligned arrays, are read with ordinary loads, so
+// nothing outside the caller's arrays is read. issue() is called by one thread and arms `bar`
+// (with no bytes when nothing is copied); item() reads tuple i of the tile.
 constexpr size_t kTileBuf = (size_t)(kTile + 2) * 8;  // one input buffer
-constexpr int kProbeChunk = kMaxTable;                      // tuples per probe item (build or stream)
-constexpr size_t kProbeBuf = (size_t)(kProbeChunk + 2) * 8; // one probe item buffer
 
-__device__ __forceinline__ uint32_t tile_mis(const TileIn& in, int64_t t0) {
-    return in.p ? (uint32_t)((((uintptr_t)(in.p + t0)) & 15) ? 1 : 0) : 0u;
-}
-// Thread 0: starts the copy of tuples [t0, t0 + tn) into buf and arms bar.
-__device__ __forceinline__ void tile_issue(const TileIn& in, int64_t t0, int tn, unsigned char* buf, uint64_t* bar) {
-    fence_proxy_async();
-    if (in.p) {
-        const uint32_t mis = tile_mis(in, t0);
-        const uint32_t bytes = (((uint32_t)tn + mis) * 8u + 15u) & ~15u;
-        if (bytes == 0) {
+struct PackedTiles {
+    const uint2* p;
+    __device__ __forceinline__ uint32_t mis(int64_t t0) const {
+        return (((uintptr_t)(p + t0)) & 15) ? 1u : 0u;
+    }
+    __device__ __forceinline__ void issue(int64_t t0, int tn, unsigned char* buf, uint64_t* bar) const {
+        fence_proxy_async();
+        const uint32_t m = mis(t0);
+        const uint32_t bytes = (((uint32_t)tn + m) * 8u + 15u) & ~15u;
+        if (tn <= 0) {
             mbar_arrive(bar);
             return;
         }
         mbar_arrive_tx(bar, bytes);
-        bulk_g2s(buf, in.p + t0 - mis, bytes, bar);
-    } else if (in.bulk_kv && (tn & ~3) > 0) {
-        const uint32_t bytes = (uint32_t)(tn & ~3) * 4u;
-        mbar_arrive_tx(bar, 2 * bytes);
-        bulk_g2s(buf, in.k + t0, bytes, bar);
-        bulk_g2s(buf + (size_t)kTile * 4, in.v + t0, bytes, bar);
-    } else {
-        mbar_arrive(bar);
+        bulk_g2s(buf, p + t0 - m, bytes, bar);
     }
-}
-__device__ __forceinline__ uint2 tile_item(const TileIn& in, const unsigned char* buf, int64_t t0, int i, int tn,
-                                           uint32_t mis) {
-    if (in.p) return reinterpret_cast<const uint2*>(buf)[i + mis];
-    if (in.bulk_kv && i < (tn & ~3))
-        return make_uint2(reinterpret_cast<const uint32_t*>(buf)[i],
-                          reinterpret_cast<const uint32_t*>(buf + (size_t)kTile * 4)[i]);
-    return make_uint2(__ldcs(in.k + t0 + i), __ldcs(in.v + t0 + i));
-}
+    __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t, int i, int, uint32_t m) const {
+        return reinterpret_cast<const uint2*>(buf)[i + m];
+    }
+};
+
+struct KvTiles {
+    const uint32_t* k;
+    const uint32_t* v;
+    bool bulk;
+    __device__ __forceinline__ uint32_t mis(int64_t) const { return 0u; }
+    __device__ __forceinline__ void issue(int64_t t0, int tn, unsigned char* buf, uint64_t* bar) const {
+        fence_proxy_async();
+        if (bulk && (tn & ~3) > 0) {
+            const uint32_t bytes = (uint32_t)(tn & ~3) * 4u;
+            mbar_arrive_tx(bar, 2 * bytes);
+            bulk_g2s(buf, k + t0, bytes, bar);
+            bulk_g2s(buf + (size_t)kTile * 4, v + t0, bytes, bar);
+        } else {
+            mbar_arrive(bar);
+        }
+    }
+    __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t t0, int i, int tn, uint32_t) const {
+        if (bulk && i < (tn & ~3))
+            return make_uint2(reinterpret_cast<const uint32_t*>(buf)[i],
+                              reinterpret_cast<const uint32_t*>(buf + (size_t)kTile * 4)[i]);
+        return make_uint2(__ldcs(k + t0 + i), __ldcs(v + t0 + i));
+    }
+};
 
 struct Bin1 {
     PartFn f;
@@ -238,63 +243,94 @@ struct Bin2 {
 };
 
 // Scatters tuples [begin, end) of `in` into `out`. cursor[b] is the next output position of bin
-// b; it advances as tiles are written. Each tile of kTile tuples arrives by bulk copy (the next
-// one is in flight meanwhile), is counted by bin, reordered by bin in shared memory (stage) and
-// written so that consecutive threads store consecutive positions of one bin's run.
+// b; it advances as tiles are written. Each tile of kTile tuples arrives by bulk copy into one of
+// the two input buffers while the previous tile is processed. Per tile every thread holds its
+// kTile / kThreads tuples in registers, takes a rank inside its tuple's bin with one shared-memory
+// atomic, and after a scan of the bin counts writes the tuple to its bin-ordered position in
+// `stage` (the tile's own input buffer, free once the tuples are in registers) with its bin in
+// `sbin`. The write pass then stores consecutive staged positions from consecutive threads, i.e.
+// runs of one bin to consecutive addresses; delta[b] = cursor[b] - (first staged position of b)
+// turns a staged position into its output position with one add.
 // `inbuf` holds two tile buffers, `bars` their mbarriers, `ph` the parity of each barrier.
-template <class Bin>
-__device__ void scatter_tiles(const TileIn& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
-                              uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, uint32_t* cnt,
-                              uint32_t* tmp, uint2* stage, unsigned char* inbuf, uint64_t* bars, uint32_t& ph,
-                              unsigned long long* errors) {
+template <class In, class Bin>
+__device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
+                              uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, int64_t* delta,
+                              uint32_t* cnt, uint16_t* sbin, uint32_t* tmp, unsigned char* inbuf, uint64_t* bars,
+                              uint32_t& ph, unsigned long long* errors) {
     constexpr int kItems = kTile / kThreads;
     const int64_t ntiles = (end - begin + kTile - 1) / kTile;
     if (ntiles <= 0) return;
-    if (threadIdx.x == 0) tile_issue(in, begin, (int)min_i64(kTile, end - begin), inbuf, &bars[0]);
+    for (int x = threadIdx.x; x < nbins; x += kThreads) cnt[x] = 0;
+    if (threadIdx.x == 0) in.issue(begin, (int)min_i64(kTile, end - begin), inbuf, &bars[0]);
     for (int64_t t = 0; t < ntiles; ++t) {
         const int64_t t0 = begin + t * kTile;
         const int tn = (int)min_i64(kTile, end - t0);
         const int b = (int)(t & 1);
-        if (threadIdx.x == 0 && t + 1 < ntiles)
-            tile_issue(in, t0 + kTile, (int)min_i64(kTile, end - t0 - kTile), inbuf + (b ^ 1) * kTileBuf,
-                       &bars[b ^ 1]);
-        for (int x = threadIdx.x; x < nbins; x += kThreads) cnt[x] = 0;
         mbar_wait(&bars[b], (ph >> b) & 1u, errors);
         ph ^= 1u << b;
+        // Every thread is past the previous tile's write pass, which read buffer b ^ 1 as `stage`
+        // (and cnt is zero again): the next tile may now be copied into b ^ 1.
         __syncthreads();
-        const unsigned char* buf = inbuf + b * kTileBuf;
-        const uint32_t mis = tile_mis(in, t0);
+        if (threadIdx.x == 0 && t + 1 < ntiles)
+            in.issue(t0 + kTile, (int)min_i64(kTile, end - t0 - kTile), inbuf + (b ^ 1) * kTileBuf, &bars[b ^ 1]);
+        unsigned char* buf = inbuf + b * kTileBuf;
+        const uint32_t mis = in.mis(t0);
+        uint2 it[kItems];
         uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const int i = k * kThreads + threadIdx.x;
             if (i < tn) {
-                const uint32_t bb = bin(tile_item(in, buf, t0, i, tn, mis).x);
+                it[k] = in.item(buf, t0, i, tn, mis);
+                const uint32_t bb = bin(it[k].x);
                 br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
             }
         }
         __syncthreads();
         block_scan_excl(cnt, nbins, tmp);  // cnt[b] = first staged position of bin b
+        for (int x = threadIdx.x; x < nbins; x += kThreads) {
+            const uint32_t e0 = cnt[x];
+            const uint32_t e1 = (x + 1 < nbins) ? cnt[x + 1] : (uint32_t)tn;
+            const int64_t c = cursor[x];
+            delta[x] = c - (int64_t)e0;
+            cursor[x] = c + (int64_t)(e1 - e0);
+        }
+        uint2* stage = reinterpret_cast<uint2*>(buf);
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const int i = k * kThreads + threadIdx.x;
-            if (i < tn) stage[cnt[br[k] >> 16] + (br[k] & 0xffffu)] = tile_item(in, buf, t0, i, tn, mis);
+            if (i < tn) {
+                const uint32_t bb = br[k] >> 16;
+                const uint32_t pos = cnt[bb] + (br[k] & 0xffffu);
+                stage[pos] = it[k];
+                sbin[pos] = (uint16_t)bb;
+            }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < tn; i += kThreads) {
-            const uint2 e = stage[i];
-            const uint32_t bb = bin(e.x);
-            const int64_t dst = cursor[bb] + (int64_t)(i - (int)cnt[bb]);
-            if (dst >= 0 && dst < out_limit) out[dst] = e;
-            else atomicAdd(errors, 1ull);
+        for (int x = threadIdx.x; x < nbins; x += kThreads) cnt[x] = 0;  // for the next tile
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const int i = k * kThreads + threadIdx.x;
+            if (i < tn) {
+                const int64_t dst = delta[sbin[i]] + i;
+                if ((uint64_t)dst < (uint64_t)out_limit) out[dst] = stage[i];
+                else atomicAdd(errors, 1ull);
+            }
         }
-        __syncthreads();
-        for (int x = threadIdx.x; x < nbins; x += kThreads) {
-            const uint32_t nxt = (x + 1 < nbins) ? cnt[x + 1] : (uint32_t)tn;
-            cursor[x] += (int64_t)(nxt - cnt[x]);
-        }
-        __syncthreads();
     }
+    __syncthreads();  // the last write pass is done with the buffers, cursor and cnt
+}
+
+// Shared-memory layout of the scatter kernels: two tile buffers, then cursor and delta (int64 per
+// bin), the bin counts (uint32 per bin) and the staged bins (uint16 per tile position).
+__device__ __forceinline__ void scatter_carve(unsigned char* smem, int max_bins, unsigned char*& inbuf,
+                                              int64_t*& cursor, int64_t*& delta, uint32_t*& cnt,
+                                              uint16_t*& sbin) {
+    inbuf = smem;
+    cursor = reinterpret_cast<int64_t*>(smem + 2 * kTileBuf);
+    delta = cursor + max_bins;
+    cnt = reinterpret_cast<uint32_t*>(delta + max_bins);
+    sbin = reinterpret_cast<uint16_t*>(cnt + max_bins);
 }
 
 __device__ __forceinline__ void init_bars(uint64_t* bars) {
@@ -308,11 +344,6 @@ __device__ __forceinline__ void init_bars(uint64_t* bars) {
 
 // Bloom probe, split in two so a thread can have several block loads in flight: the address of a
 // key's 32-byte block in the segment of its finest partition f, then the test of the loaded words.
-__device__ __forceinline__ const uint4* bloom_block(const JoinDesc& d, uint32_t f, uint32_t key) {
-    BloomKey bk;
-    bloom_key(key, d.seg_blocks, d.bloom_k, bk);
-    return reinterpret_cast<const uint4*>(d.bloom + ((int64_t)f * d.seg_blocks + bk.block) * 8);
-}
 __device__ __forceinline__ bool bloom_words_pass(uint32_t key, uint32_t seg_blocks, int k, uint4 w0, uint4 w1) {
     BloomKey bk;
     bloom_key(key, seg_blocks, k, bk);
@@ -321,6 +352,20 @@ __device__ __forceinline__ bool bloom_words_pass(uint32_t key, uint32_t seg_bloc
            ((w1.x & bk.mask[4]) == bk.mask[4]) && ((w1.y & bk.mask[5]) == bk.mask[5]) &&
            ((w1.z & bk.mask[6]) == bk.mask[6]) && ((w1.w & bk.mask[7]) == bk.mask[7]);
 }
+__device__ __forceinline__ const uint4* bloom_block(const JoinDesc& d, uint32_t f, uint64_t g) {
+    return reinterpret_cast<const uint4*>(d.bloom + ((int64_t)f * d.seg_blocks + bloom_block_of(g, d.seg_blocks)) * 8);
+}
+// Tests the key with hash g (key itself for k > 8) against its loaded block words w0, w1: for
+// k <= 8 word w must have bit (g >> 5w) & 31 set for every w < k.
+__device__ __forceinline__ bool bloom_pass(uint64_t g, uint32_t key, uint32_t seg_blocks, int k, uint4 w0, uint4 w1) {
+    if (k > 8) return bloom_words_pass(key, seg_blocks, k, w0, w1);
+    const uint32_t wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+    uint32_t ok = 1u;
+#pragma unroll
+    for (int w = 0; w < 8; ++w)
+        if (w < k) ok &= wv[w] >> ((uint32_t)(g >> (5 * w)) & 31u);
+    return (ok & 1u) != 0;
+}
 constexpr int kProbeILP = 4;  // keys per thread with their filter blocks in flight together
 
 // ---------------------------------------------------------------------------------------------
@@ -328,7 +373,7 @@ constexpr int kProbeILP = 4;  // keys per thread with their filter blocks in fli
 // Bloom probe + survivor compaction + histogram (S with Bloom).
 // hist layout per relation: [p * nslices + s], plus one trailing zero (sentinel) so that the
 // exclusive scan of entry P1*nslices is the relation's total.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
           uint32_t* __restrict__ hist, unsigned long long* gwords) {
     extern __shared__ uint32_t sh_cnt[];  // [max P1]
@@ -352,6 +397,20 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t* __restrict__ key = R.key;
             if ((((uintptr_t)(key + b)) & 15) == 0) {
                 int64_t i = b + 4 * (int64_t)threadIdx.x;
+                // four 16-byte loads in flight per thread
+                for (; i + 12 * kThreads + 3 < e; i += 16 * kThreads) {
+                    uint4 k4[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        k4[u] = __ldcs(reinterpret_cast<const uint4*>(key + i + 4 * u * kThreads));
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        atomicAdd(&sh_cnt[part1(pf, k4[u].x)], 1u);
+                        atomicAdd(&sh_cnt[part1(pf, k4[u].y)], 1u);
+                        atomicAdd(&sh_cnt[part1(pf, k4[u].z)], 1u);
+                        atomicAdd(&sh_cnt[part1(pf, k4[u].w)], 1u);
+                    }
+                }
                 for (; i + 3 < e; i += 4 * kThreads) {
                     const uint4 k4 = __ldcs(reinterpret_cast<const uint4*>(key + i));
                     atomicAdd(&sh_cnt[part1(pf, k4.x)], 1u);
@@ -372,8 +431,10 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             // compacted (key, value) into R.cmp[b, b + count) and counted per level-1 partition.
             const uint32_t* __restrict__ key = R.key;
             const uint32_t* __restrict__ val = R.val;
+            const int bk = d.bloom_k;
             for (int64_t i0 = b; i0 < e; i0 += kProbeILP * kThreads) {
-                uint32_t kk[kProbeILP];
+                uint32_t kk[kProbeILP], p1[kProbeILP];
+                uint64_t gg[kProbeILP];
                 uint4 w0[kProbeILP], w1[kProbeILP];
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
@@ -383,8 +444,10 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
+                    p1[u] = part1(pf, kk[u]);
+                    gg[u] = bloom_hash(kk[u]);
                     if (i < e) {
-                        const uint4* blk = bloom_block(d, part1(pf, kk[u]) * pf.P2 + part2(pf, kk[u]), kk[u]);
+                        const uint4* blk = bloom_block(d, p1[u] * pf.P2 + part2(pf, kk[u]), gg[u]);
                         w0[u] = __ldg(blk);
                         w1[u] = __ldg(blk + 1);
                     }
@@ -392,14 +455,14 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    const bool pass = i < e && bloom_words_pass(kk[u], d.seg_blocks, d.bloom_k, w0[u], w1[u]);
+                    const bool pass = i < e && bloom_pass(gg[u], kk[u], d.seg_blocks, bk, w0[u], w1[u]);
                     const uint32_t m = __ballot_sync(0xffffffffu, pass);
                     if (m) {
                         uint32_t base = 0;
                         if (lane == 0) base = atomicAdd(&s_cursor, (uint32_t)__popc(m));
                         base = __shfl_sync(0xffffffffu, base, 0);
                         if (pass) {
-                            atomicAdd(&sh_cnt[part1(pf, kk[u])], 1u);
+                            atomicAdd(&sh_cnt[p1[u]], 1u);
                             const int64_t dst = b + base + __popc(m & lanemask_lt());
                             if (dst < e) R.cmp[dst] = make_uint2(kk[u], __ldg(val + i));
                             else atomicAdd(&gwords[kGErrors], 1ull);
@@ -428,14 +491,19 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 
 // Level 1, pass 2: scatter each slice into its private runs. cursor[p] = scan[p][s] - scan[0][0]
 // of this relation, i.e. the partition's start plus the counts of all earlier slices.
-__global__ void __launch_bounds__(kThreads)
+// kPacked selects the slices this launch handles: false = tuples from the caller's key/value arrays,
+// true = S survivors of a level-1 Bloom probe, packed in cmp. One instantiation per input form keeps
+// each kernel within the 64 registers that two CTAs per SM allow.
+template <bool kPacked>
+__global__ void __launch_bounds__(kThreads, 2)
 k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
              const int64_t* __restrict__ scan, unsigned long long* gwords, int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
-    unsigned char* inbuf = smem;                                                // 2 tile buffers
-    uint2* stage = reinterpret_cast<uint2*>(smem + 2 * kTileBuf);               // [kTile]
-    int64_t* cursor = reinterpret_cast<int64_t*>(stage + kTile);                // [max_bins]
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(cursor + max_bins);             // [max_bins]
+    unsigned char* inbuf;
+    int64_t *cursor, *delta;
+    uint32_t* cnt;
+    uint16_t* sbin;
+    scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
     __shared__ uint32_t tmp[kThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
@@ -448,6 +516,7 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const int s = (int)(g - slice_prefix[j]);
         const int64_t b = (int64_t)s * R.slice_len;
         const bool bloom = (rel == 1) && d.bloom != nullptr && d.bloom_level == 1;
+        if (bloom != kPacked) continue;  // the other instantiation's slice (block-uniform)
         const int64_t e = bloom ? b + R.slice_cnt[s] : min(b + R.slice_len, R.n);
         const uint32_t P1 = d.pf.P1;
         const int64_t* S = scan + R.hist_base;
@@ -456,15 +525,14 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
             cursor[p] = S[(int64_t)p * R.nslices + s] - s0;
         __syncthreads();
         const Bin1 bin{d.pf};
-        TileIn in;
-        if (bloom) {
-            in = TileIn{R.cmp, nullptr, nullptr, false};
+        if constexpr (kPacked) {
+            scatter_tiles(PackedTiles{R.cmp}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf,
+                          bars, ph, &gwords[kGErrors]);
         } else {
             const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 15) == 0;
-            in = TileIn{nullptr, R.key, R.val, al};
+            scatter_tiles(KvTiles{R.key, R.val, al}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp,
+                          inbuf, bars, ph, &gwords[kGErrors]);
         }
-        scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, tmp, stage, inbuf, bars, ph,
-                      &gwords[kGErrors]);
     }
 }
 
@@ -536,7 +604,7 @@ __global__ void k_l2_plan(const JoinDesc* __restrict__ J, int nj, int rel, const
 
 // Level-2 histogram of one slice: counts by level-2 id, or (S with a level-2 Bloom probe) tests
 // every key and compacts the survivors into cmp[slice begin, + survivors).
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
           const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
           uint32_t* __restrict__ hist2, uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords) {
@@ -571,8 +639,11 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             }
         } else {
             // the filter segments of this level-1 partition are shared by every CTA working on it
+            const int bk = d.bloom_k;
             for (int64_t i0 = begin; i0 < end; i0 += kProbeILP * kThreads) {
                 uint2 e[kProbeILP];
+                uint32_t q[kProbeILP];
+                uint64_t gg[kProbeILP];
                 uint4 w0[kProbeILP], w1[kProbeILP];
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
@@ -582,8 +653,10 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
+                    q[u] = bin(e[u].x);
+                    gg[u] = bloom_hash(e[u].x);
                     if (i < end) {
-                        const uint4* blk = bloom_block(d, x.p * P2 + bin(e[u].x), e[u].x);
+                        const uint4* blk = bloom_block(d, x.p * P2 + q[u], gg[u]);
                         w0[u] = __ldg(blk);
                         w1[u] = __ldg(blk + 1);
                     }
@@ -591,14 +664,14 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    const bool pass = i < end && bloom_words_pass(e[u].x, d.seg_blocks, d.bloom_k, w0[u], w1[u]);
+                    const bool pass = i < end && bloom_pass(gg[u], e[u].x, d.seg_blocks, bk, w0[u], w1[u]);
                     const uint32_t m = __ballot_sync(0xffffffffu, pass);
                     if (m) {
                         uint32_t base = 0;
                         if (lane == 0) base = atomicAdd(&s_surv, (uint32_t)__popc(m));
                         base = __shfl_sync(0xffffffffu, base, 0);
                         if (pass) {
-                            atomicAdd(&cnt[bin(e[u].x)], 1u);
+                            atomicAdd(&cnt[q[u]], 1u);
                             const int64_t dst = begin + base + __popc(m & lanemask_lt());
                             if (dst < end) R.cmp[dst] = e[u];
                             else atomicAdd(&gwords[kGErrors], 1ull);
@@ -619,16 +692,17 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 }
 
 // Level-2 scatter of one slice into its private runs of the level-2 buffer.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
              const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
              const int64_t* __restrict__ scan2, const uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords,
              int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
-    unsigned char* inbuf = smem;                                                // 2 tile buffers
-    uint2* stage = reinterpret_cast<uint2*>(smem + 2 * kTileBuf);               // [kTile]
-    int64_t* cursor = reinterpret_cast<int64_t*>(stage + kTile);                // [max_bins]
-    uint32_t* cnt = reinterpret_cast<uint32_t*>(cursor + max_bins);             // [max_bins]
+    unsigned char* inbuf;
+    int64_t *cursor, *delta;
+    uint32_t* cnt;
+    uint16_t* sbin;
+    scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
     __shared__ uint32_t tmp[kThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
@@ -647,8 +721,8 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const int64_t* Sx = S2 + x.local_off * P2;
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
         __syncthreads();
-        scatter_tiles(TileIn{bloom ? R.cmp : R.l1, nullptr, nullptr, false}, begin, end, Bin2{d.pf}, (int)P2, R.l2,
-                      R.n, cursor, cnt, tmp, stage, inbuf, bars, ph, &gwords[kGErrors]);
+        scatter_tiles(PackedTiles{bloom ? R.cmp : R.l1}, begin, end, Bin2{d.pf}, (int)P2, R.l2,
+                      R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph, &gwords[kGErrors]);
     }
 }
 
@@ -677,6 +751,13 @@ __global__ void k_l2_bounds(const JoinDesc* __restrict__ J, int nj, int rel, con
     }
 }
 
+// The low 40 bits of g rotated right by s (0 <= s < 40).
+__device__ __forceinline__ uint64_t rot40(uint64_t g, uint32_t s) {
+    constexpr uint64_t kM = (1ull << 40) - 1;
+    const uint64_t x = g & kM;
+    return s ? (((x >> s) | (x << (40 - s))) & kM) : x;
+}
+
 // Bloom build: one CTA per group of G consecutive finest partitions of a Bloom-enabled join
 // (G = JoinDesc::bloom_group, chosen so the group's segments fit in shared memory). The group's R
 // tuples are contiguous in the final R buffer; every key sets its bits with 32-bit atomicOr in the
@@ -700,6 +781,7 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
         const int64_t words = (f1 - f0) * (int64_t)nw;
         uint32_t* gseg = d.bloom + f0 * (int64_t)nw;
         const int k = d.bloom_k;
+        const uint32_t l8 = threadIdx.x & 7u, rs = 5u * l8;
         const bool in_smem = words <= smem_words;
         uint32_t* dst = in_smem ? seg : gseg;
         for (int64_t w = threadIdx.x; w < words; w += kThreads) dst[w] = 0;
@@ -721,16 +803,27 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
                     continue;
                 }
                 const uint64_t g = bloom_hash(kk[u]);
-                const uint64_t g2 = k > 8 ? mix64(g) : 0ull;
                 uint32_t* blk = dst + local * nw + (int64_t)bloom_block_of(g, d.seg_blocks) * 8;
                 // Lane l starts at word l % 8 of its block, so the lanes of one atomic instruction
                 // touch different words and mostly different shared-memory banks (all lanes on
-                // the same word would be an 8-way bank conflict, since blocks are 8 words).
+                // the same word would be an 8-way bank conflict, since blocks are 8 words). For
+                // k <= 8 the 40 bits of word positions are rotated once by 5 * (l % 8) bits so
+                // that step t reads its position with a constant shift.
+                if (k <= 8) {
+                    const uint64_t r = rot40(g, rs);
 #pragma unroll
-                for (int t = 0; t < 8; ++t) {
-                    const int w = (t + (int)threadIdx.x) & 7;
-                    const uint32_t m = bloom_word_mask(g, g2, k, w);
-                    if (m) atomicOr(blk + w, m);
+                    for (int t = 0; t < 8; ++t) {
+                        const uint32_t w = ((uint32_t)t + l8) & 7u;
+                        if (w < (uint32_t)k) atomicOr(blk + w, 1u << ((uint32_t)(r >> (5 * t)) & 31u));
+                    }
+                } else {
+                    const uint64_t g2 = mix64(g);
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const int w = (int)(((uint32_t)t + l8) & 7u);
+                        const uint32_t m = bloom_word_mask(g, g2, k, w);
+                        if (m) atomicOr(blk + w, m);
+                    }
                 }
             }
         }
@@ -903,77 +996,28 @@ __device__ __forceinline__ void warp_flush(const JoinDesc& d, const uint32_t* wr
     __syncwarp();
 }
 
-// Persistent probe kernel. A task's build chunk and its streamed chunks reach shared memory as a
-// sequence of bulk copies ("items": build, chunk 0, chunk 1, ...; then the next task's items) through
-// a ring of two buffers: item i lives in buffer i % 2, and when the CTA has finished with item i
-// thread 0 issues item i + 2, so one item is always in flight while the other is processed. Tasks
-// are taken from the global queue one ahead of their use. Per task the CTA builds a bucketised
-// table of the build chunk (count per bucket, exclusive scan, place; after placement off[b] holds
-// the end of bucket b, so bucket b spans [off[b-1], off[b])), then streams every chunk through it:
-// each streamed tuple scans its bucket and every key-equal entry is a match.
-constexpr int kRing = 4;  // tasks held by a CTA: the one being processed and the ones being loaded
+// Persistent probe kernel, two CTAs per SM. Each CTA takes tasks from the global queue (the next
+// task index is fetched while the current task runs). Per task the CTA
+//   * loads the build chunk (at most table_cap tuples) into registers, kTable / kThreads per thread,
+//     counts it per bucket with one shared-memory atomic per tuple (the atomic's result is the
+//     tuple's rank in its bucket), scans the counts into bucket starts (off[nb] = the chunk size)
+//     and places every tuple at off[bucket] + rank: a bucketised table, bucket b = [off[b], off[b+1]);
+//   * streams the other side straight from global memory, kProbeU coalesced tuples per thread in
+//     flight; a streamed tuple scans its bucket and every key-equal entry is a match. The lanes of a
+//     warp scan their buckets in lock step and matches are compacted with ballot/popc into the
+//     warp's shared-memory staging buffer, which is written out with one global atomic per flush.
+constexpr int kProbeU = 4;                     // streamed tuples per thread in flight
+constexpr int kBuildPer = kMaxTable / kThreads;  // build tuples per thread
 
-__device__ __forceinline__ int task_items(const Task& t) {
-    return 1 + (int)((t.p_len + (uint32_t)kProbeChunk - 1) / (uint32_t)kProbeChunk);
-}
-// Source and length of item k of task t (0 = build chunk, 1.. = streamed chunks).
-__device__ __forceinline__ const uint2* item_src(const JoinDesc& d, const Task& t, int k, int& n) {
-    const bool bs = (t.flags & kTaskBuildS) != 0;
-    if (k == 0) {
-        n = (int)min_i64(kProbeChunk, (int64_t)t.b_len);  // b_len <= table_cap <= kProbeChunk by construction
-        return final_buf(d, bs ? 1 : 0) + t.b_begin;
-    }
-    const int64_t c0 = (int64_t)(k - 1) * kProbeChunk;
-    n = (int)min_i64(kProbeChunk, (int64_t)t.p_len - c0);
-    return final_buf(d, bs ? 0 : 1) + t.p_begin + c0;
-}
-
-struct ProbeShared {
-    Task ring[kRing];
-    int valid[kRing];
-    int ps, pi;               // next item to issue: ring slot and item index
-    long long issued;         // items issued so far
-};
-
-// Thread 0: dequeues the next task into ring slot `slot`.
-__device__ __forceinline__ void dequeue(ProbeShared& sh, int slot, const Task* __restrict__ tasks,
-                                        unsigned long long* gwords, long long ntasks) {
-    const long long t = (long long)atomicAdd(&gwords[kGQueue], 1ull);
-    sh.valid[slot] = t < ntasks;
-    if (t < ntasks) sh.ring[slot] = tasks[t];
-}
-
-// Thread 0: issues the next item of the sequence into buffer (issued % 2), dequeuing tasks as the
-// sequence reaches them. Past the last task nothing is issued.
-__device__ __forceinline__ void produce(ProbeShared& sh, const JoinDesc* __restrict__ J, const Task* __restrict__ tasks,
-                                        unsigned long long* gwords, long long ntasks, unsigned char* bufs,
-                                        uint64_t* bars) {
-    if (!sh.valid[sh.ps]) return;
-    const Task& t = sh.ring[sh.ps];
-    int n;
-    const uint2* src = item_src(J[t.join], t, sh.pi, n);
-    const int b = (int)(sh.issued & 1);
-    tile_issue(TileIn{src, nullptr, nullptr, false}, 0, n, bufs + b * kProbeBuf, &bars[b]);
-    ++sh.issued;
-    if (++sh.pi == task_items(t)) {
-        sh.pi = 0;
-        sh.ps = (sh.ps + 1) % kRing;
-        dequeue(sh, sh.ps, tasks, gwords, ntasks);
-    }
-}
-
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
 k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned long long* gwords,
         int table_cap, int emit_key) {
     extern __shared__ __align__(16) unsigned char smem[];
-    unsigned char* bufs = smem;                                                     // 2 item buffers
-    uint2* table = reinterpret_cast<uint2*>(smem + 2 * kProbeBuf);                  // [table_cap]
-    uint32_t* off = reinterpret_cast<uint32_t*>(table + table_cap);                 // [table_cap] (+pad)
+    uint2* table = reinterpret_cast<uint2*>(smem);                    // [table_cap]
+    uint32_t* off = reinterpret_cast<uint32_t*>(table + table_cap);   // [table_cap + 1] (+pad)
     uint32_t* wbuf = off + table_cap + 4;
     __shared__ uint32_t tmp[kThreads / 32];
-    __shared__ ProbeShared sh;
-    __shared__ __align__(8) uint64_t bars[2];
-    init_bars(bars);
+    __shared__ long long s_task[2];
     unsigned long long* errors = &gwords[kGErrors];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int words_per_warp = kWarpBuf * (emit_key ? 3 : 2);
@@ -983,19 +1027,13 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     int wcount = 0;
     int cur = -1;
     const long long ntasks = (long long)gwords[kGTasks];
-    if (threadIdx.x == 0) {
-        sh.ps = 0;
-        sh.pi = 0;
-        sh.issued = 0;
-        dequeue(sh, 0, tasks, gwords, ntasks);
-        produce(sh, J, tasks, gwords, ntasks, bufs, bars);
-        produce(sh, J, tasks, gwords, ntasks, bufs, bars);
-    }
+    if (threadIdx.x == 0) s_task[0] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
     __syncthreads();
-    long long consumed = 0;
-    for (int cs = 0;; cs = (cs + 1) % kRing) {
-        if (!sh.valid[cs]) break;
-        const Task tk = sh.ring[cs];
+    for (int slot = 0;; slot ^= 1) {
+        const long long t = s_task[slot];
+        if (t >= ntasks) break;
+        if (threadIdx.x == 0) s_task[slot ^ 1] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
+        const Task& tk = tasks[t];
         if (tk.join != cur) {
             if (cur >= 0 && wcount > 0) warp_flush(J[cur], wr, ws, wk, wcount, lane);
             wcount = 0;
@@ -1003,10 +1041,9 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         }
         const JoinDesc& d = J[tk.join];
         const bool bs = (tk.flags & kTaskBuildS) != 0;
-        const int nitems = task_items(tk);
-        // ---- item 0: build the table
-        int nr;
-        const uint2* bsrc = item_src(d, tk, 0, nr);
+        const uint2* __restrict__ bsrc = final_buf(d, bs ? 1 : 0) + tk.b_begin;
+        const uint2* __restrict__ psrc = final_buf(d, bs ? 0 : 1) + tk.p_begin;
+        int nr = (int)tk.b_len;
         if (nr > table_cap) {
             if (threadIdx.x == 0) atomicAdd(errors, 1ull);
             nr = table_cap;
@@ -1014,49 +1051,61 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         uint32_t nb = 32;
         while (nb < (uint32_t)nr) nb <<= 1;
         const uint32_t mask = nb - 1;
-        for (uint32_t i = threadIdx.x; i < nb; i += kThreads) off[i] = 0;
+        // the previous task's probe is done with table and off (and s_task[slot ^ 1] is written)
+        for (uint32_t i = threadIdx.x; i <= nb; i += kThreads) off[i] = 0;
+        __syncthreads();
+        // ---- build
+        // keys first (counted), values after the scan (placed): fewer live registers
+        uint32_t br[kBuildPer];  // bucket << 16 | rank in bucket
         {
-            const int b = (int)(consumed & 1);
-            mbar_wait(&bars[b], (uint32_t)((consumed >> 1) & 1), errors);
-            __syncthreads();
-            const uint2* in = reinterpret_cast<const uint2*>(bufs + b * kProbeBuf) +
-                              tile_mis(TileIn{bsrc, nullptr, nullptr, false}, 0);
-            for (int i = threadIdx.x; i < nr; i += kThreads) atomicAdd(&off[bucket_of(in[i].x, mask)], 1u);
-            __syncthreads();
-            block_scan_excl(off, (int)nb, tmp);
-            for (int i = threadIdx.x; i < nr; i += kThreads) {
-                const uint2 e = in[i];
-                table[atomicAdd(&off[bucket_of(e.x, mask)], 1u)] = e;
+            uint32_t bkey[kBuildPer];
+#pragma unroll
+            for (int k = 0; k < kBuildPer; ++k) {
+                const int i = k * kThreads + threadIdx.x;
+                if (i < nr) bkey[k] = __ldg(&bsrc[i].x);
             }
-            __syncthreads();
-            ++consumed;
-            if (threadIdx.x == 0) produce(sh, J, tasks, gwords, ntasks, bufs, bars);
-            __syncthreads();
+#pragma unroll
+            for (int k = 0; k < kBuildPer; ++k) {
+                const int i = k * kThreads + threadIdx.x;
+                if (i < nr) {
+                    const uint32_t bk = bucket_of(bkey[k], mask);
+                    br[k] = (bk << 16) | atomicAdd(&off[bk], 1u);
+                }
+            }
         }
-        // ---- items 1..: stream the other side through the table
-        for (int k = 1; k < nitems; ++k) {
-            int cn;
-            const uint2* csrc = item_src(d, tk, k, cn);
-            const int b = (int)(consumed & 1);
-            mbar_wait(&bars[b], (uint32_t)((consumed >> 1) & 1), errors);
-            const uint2* chunk = reinterpret_cast<const uint2*>(bufs + b * kProbeBuf) +
-                                 tile_mis(TileIn{csrc, nullptr, nullptr, false}, 0);
-            for (int base = 0; base < cn; base += kThreads) {
-                const int i = base + (int)threadIdx.x;
-                uint2 e = make_uint2(0u, 0u);
+        __syncthreads();
+        block_scan_excl(off, (int)nb + 1, tmp);  // off[b] = start of bucket b, off[nb] = nr
+#pragma unroll
+        for (int k = 0; k < kBuildPer; ++k) {
+            const int i = k * kThreads + threadIdx.x;
+            if (i < nr) table[off[br[k] >> 16] + (br[k] & 0xffffu)] = __ldg(bsrc + i);
+        }
+        __syncthreads();
+        // ---- probe
+        const uint32_t pn = tk.p_len;
+        for (uint32_t base = 0; base < pn; base += (uint32_t)(kProbeU * kThreads)) {
+            uint2 e[kProbeU];
+#pragma unroll
+            for (int u = 0; u < kProbeU; ++u) {
+                const uint32_t i = base + u * kThreads + threadIdx.x;
+                e[u] = i < pn ? __ldcs(psrc + i) : make_uint2(0u, 0u);
+            }
+#pragma unroll
+            for (int u = 0; u < kProbeU; ++u) {
+                if (base + u * kThreads >= pn) break;  // warp-uniform: nothing left for any lane
+                const uint32_t i = base + u * kThreads + threadIdx.x;
                 uint32_t lo = 0, hi = 0;
-                if (i < cn) {
-                    e = chunk[i];
-                    const uint32_t bk = bucket_of(e.x, mask);
-                    lo = bk ? off[bk - 1] : 0u;
-                    hi = off[bk];
+                if (i < pn) {
+                    const uint32_t bk = bucket_of(e[u].x, mask);
+                    lo = off[bk];
+                    hi = off[bk + 1];
                 }
                 while (__any_sync(0xffffffffu, lo < hi)) {
                     bool m = false;
                     uint32_t rv = 0;
                     if (lo < hi) {
                         const uint2 cc = table[lo];
-                        m = (cc.x == e.x);
+                        m = (cc.x == e[u].x);
                         rv = cc.y;
                         ++lo;
                     }
@@ -1069,20 +1118,17 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
                         }
                         if (m) {
                             const int pos = wcount + __popc(mm & lanemask_lt());
-                            wr[pos] = bs ? e.y : rv;
-                            ws[pos] = bs ? rv : e.y;
-                            if (emit_key) wk[pos] = e.x;
+                            wr[pos] = bs ? e[u].y : rv;
+                            ws[pos] = bs ? rv : e[u].y;
+                            if (emit_key) wk[pos] = e[u].x;
                         }
                         wcount += n;
                         __syncwarp();
                     }
                 }
             }
-            __syncthreads();  // buffer b is free: refill it with item consumed + 2
-            ++consumed;
-            if (threadIdx.x == 0) produce(sh, J, tasks, gwords, ntasks, bufs, bars);
-            __syncthreads();  // ring updates by produce() visible before the next task is read
         }
+        __syncthreads();
     }
     if (cur >= 0 && wcount > 0) warp_flush(J[cur], wr, ws, wk, wcount, lane);
 }
@@ -1191,14 +1237,14 @@ cudaError_t enqueue_scan(const uint32_t* in, int64_t* out, int64_t n, int64_t* t
 }
 
 size_t probe_smem_bytes(int table_cap, int emit_key) {
-    return 2 * kProbeBuf + (size_t)table_cap * 8 + ((size_t)table_cap + 4) * 4 +
+    return (size_t)table_cap * 8 + ((size_t)table_cap + 4) * 4 +
            (size_t)(kThreads / 32) * kWarpBuf * (emit_key ? 3 : 2) * 4;
 }
 
 // Shared memory of the scatter kernels: two bulk-copy tile buffers, the reordered tile, and a
 // cursor and a count per bin.
 static size_t scatter_smem(int max_bins) {
-    return 2 * kTileBuf + (size_t)kTile * 8 + (size_t)max_bins * 12;
+    return 2 * kTileBuf + (size_t)max_bins * (8 + 8 + 4) + (size_t)kTile * 2;
 }
 
 static cudaError_t set_smem_attr(const void* fn, size_t bytes) {
@@ -1214,7 +1260,8 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     static thread_local bool attrs_done = false;
     cudaError_t err;
     if (!attrs_done) {
-        if ((err = set_smem_attr((const void*)k_l1_scatter, scatter_smem(kMaxP1))) != cudaSuccess) return err;
+        if ((err = set_smem_attr((const void*)k_l1_scatter<false>, scatter_smem(kMaxP1))) != cudaSuccess) return err;
+        if ((err = set_smem_attr((const void*)k_l1_scatter<true>, scatter_smem(kMaxP1))) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_l2_scatter, scatter_smem(kMaxP2))) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_bloom_build, kBloomSmemWords * 4)) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_probe, probe_smem_bytes(kMaxTable, 1))) != cudaSuccess)
@@ -1258,9 +1305,14 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             return err;
         mark(m0 + 1);
         if (a.total_slices[rel] > 0) {
-            k_l1_scatter<<<grid_for(a.total_slices[rel], sms, 2), kThreads, scatter_smem(a.max_p1), st>>>(
+            k_l1_scatter<false><<<grid_for(a.total_slices[rel], sms, 2), kThreads, scatter_smem(a.max_p1), st>>>(
                 a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
             ++launches;
+            if (rel == 1 && a.any_bloom_l1) {
+                k_l1_scatter<true><<<grid_for(a.total_slices[rel], sms, 2), kThreads, scatter_smem(a.max_p1), st>>>(
+                    a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
+                ++launches;
+            }
         }
         mark(m0 + 2);
         {

@@ -38,6 +38,7 @@ struct PipelineArgs {
     int table_cap;                    // probe table capacity (tuples)
     int emit_key;
     int any_bloom;
+    int any_bloom_l1;                 // some join probes its filter in S's first pass
     int num_sms;
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
     int stages;                       // kRunPartR | kRunBloom | kRunPartS | kRunProbe
