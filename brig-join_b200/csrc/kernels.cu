@@ -7,7 +7,9 @@
 //   gpu_make_simple_prefix (src/kernel_functions.cu:461-492)          -> k_scan_* (device-wide)
 //   gpu_make_sorted_table_for_both (src/kernel_functions.cu:95-133)    -> k_l1_scatter
 //   gpu_run_hist_second_pass + gpu_build_table_second_pass_kv (src/kernel_functions.cu:163-281)
-//                                                                      -> k_l2_partition
+//                                     -> k_l2_plan + k_l2_hist + k_l2_scatter + k_l2_bounds
+//   queryAndCompactKernelPartitioned, alternatively fused into S's level-2 histogram pass
+//                                                                            -> k_l2_hist (Bloom)
 //   insertKernelPartitioned (src/bloom.cu:698-722)                     -> k_bloom_build
 //   gpu_probe_with_second_pass / gpu_fused_probe_transfer local part
 //   (src/kernel_functions.cu:294-454, 612-789), including the split path (:356-395)
