@@ -1000,33 +1000,95 @@ __device__ __forceinline__ void warp_flush(const JoinDesc& d, const uint32_t* wr
 
 // Persistent probe kernel, two CTAs per SM. Each CTA takes tasks from the global queue (the next
 // task index is fetched while the current task runs). Per task the CTA
-//   * loads the build chunk (at most table_cap tuples) into registers, kTable / kThreads per thread,
-//     counts it per bucket with one shared-memory atomic per tuple (the atomic's result is the
-//     tuple's rank in its bucket), scans the counts into bucket starts (off[nb] = the chunk size)
-//     and places every tuple at off[bucket] + rank: a bucketised table, bucket b = [off[b], off[b+1]);
+//   * loads the build chunk (at most table_cap tuples) into registers, kBuildPer per thread, counts
+//     it per bucket with one shared-memory atomic per tuple (the atomic's result is the tuple's rank
+//     in its bucket), scans the counts into bucket starts (off[nb] = the chunk size) and places
+//     every tuple at off[bucket] + rank: a bucketised table, bucket b = [off[b], off[b+1]). Every
+//     build key also sets one bit of a 65536-bit presence bitmap;
 //   * streams the other side straight from global memory, kProbeU coalesced tuples per thread in
-//     flight; a streamed tuple scans its bucket and every key-equal entry is a match. The lanes of a
-//     warp scan their buckets in lock step and matches are compacted with ballot/popc into the
-//     warp's shared-memory staging buffer, which is written out with one global atomic per flush.
-constexpr int kProbeU = 4;                     // streamed tuples per thread in flight
-constexpr int kBuildPer = kMaxTable / kThreads;  // build tuples per thread
+//     flight. A streamed tuple whose bitmap bit is clear cannot match (at most 4096 keys set at
+//     most 6% of the bits); the others are compacted with ballot/popc into the warp's candidate
+//     queue in shared memory. Every 32 queued candidates the warp scans their buckets in lock step,
+//     one candidate per lane, and compacts matches into the warp's output staging buffer, which is
+//     written out with one global atomic per flush. So the bucket scans, whose cost is the longest
+//     bucket among the lanes, run only on full warps of likely matches.
+// The bitmap index is a multiplicative hash of the key, independent of the partition bits (the
+// keys of one task share the top bits of mix32) and of the bucket bits.
+constexpr int kProbeU = 4;                        // streamed tuples per thread in flight
+constexpr int kBuildPer = kMaxTable / kThreads;   // build tuples per thread
+constexpr int kBitmapWords = 2048;                // 65536-bit presence bitmap
+constexpr int kQueue = 64;                        // candidates queued per warp
+
+__device__ __forceinline__ uint32_t presence_bit(uint32_t key) { return (key * 0x9E3779B1u) >> 16; }
+
+// Output staging of one warp: the pairs found so far for join `d`.
+struct WarpOut {
+    uint32_t* wr;
+    uint32_t* ws;
+    uint32_t* wk;
+    int count;
+};
+
+// The warp scans the buckets of candidates q[0, n) (n <= 32), one per lane, and stages every match.
+__device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2* q, int n, const uint2* table,
+                                                 const uint32_t* off, uint32_t mask, bool bs, int emit_key,
+                                                 int lane, WarpOut& o) {
+    uint2 e = make_uint2(0u, 0u);
+    uint32_t lo = 0, hi = 0;
+    if (lane < n) {
+        e = q[lane];
+        const uint32_t bk = bucket_of(e.x, mask);
+        lo = off[bk];
+        hi = off[bk + 1];
+    }
+    while (__any_sync(0xffffffffu, lo < hi)) {
+        bool m = false;
+        uint32_t rv = 0;
+        if (lo < hi) {
+            const uint2 cc = table[lo];
+            m = (cc.x == e.x);
+            rv = cc.y;
+            ++lo;
+        }
+        const uint32_t mm = __ballot_sync(0xffffffffu, m);
+        if (mm) {
+            const int c = __popc(mm);
+            if (o.count + c > kWarpBuf) {
+                warp_flush(d, o.wr, o.ws, o.wk, o.count, lane);
+                o.count = 0;
+            }
+            if (m) {
+                const int pos = o.count + __popc(mm & lanemask_lt());
+                o.wr[pos] = bs ? e.y : rv;
+                o.ws[pos] = bs ? rv : e.y;
+                if (emit_key) o.wk[pos] = e.x;
+            }
+            o.count += c;
+            __syncwarp();
+        }
+    }
+}
 
 __global__ void __launch_bounds__(kThreads, 2)
 k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned long long* gwords,
         int table_cap, int emit_key) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint2* table = reinterpret_cast<uint2*>(smem);                    // [table_cap]
-    uint32_t* off = reinterpret_cast<uint32_t*>(table + table_cap);   // [table_cap + 1] (+pad)
+    uint2* table = reinterpret_cast<uint2*>(smem);                              // [table_cap]
+    uint2* queue = table + table_cap;                                           // [warps][kQueue]
+    uint32_t* bitmap = reinterpret_cast<uint32_t*>(queue + (kThreads / 32) * kQueue);  // [kBitmapWords]
+    uint32_t* off = bitmap + kBitmapWords;                                      // [table_cap + 1] (+pad)
     uint32_t* wbuf = off + table_cap + 4;
     __shared__ uint32_t tmp[kThreads / 32];
     __shared__ long long s_task[2];
     unsigned long long* errors = &gwords[kGErrors];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int words_per_warp = kWarpBuf * (emit_key ? 3 : 2);
-    uint32_t* wr = wbuf + wid * words_per_warp;
-    uint32_t* ws = wr + kWarpBuf;
-    uint32_t* wk = ws + kWarpBuf;
-    int wcount = 0;
+    WarpOut o;
+    o.wr = wbuf + wid * words_per_warp;
+    o.ws = o.wr + kWarpBuf;
+    o.wk = o.ws + kWarpBuf;
+    o.count = 0;
+    uint2* q = queue + wid * kQueue;
     int cur = -1;
     const long long ntasks = (long long)gwords[kGTasks];
     if (threadIdx.x == 0) s_task[0] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
@@ -1037,8 +1099,8 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         if (threadIdx.x == 0) s_task[slot ^ 1] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
         const Task& tk = tasks[t];
         if (tk.join != cur) {
-            if (cur >= 0 && wcount > 0) warp_flush(J[cur], wr, ws, wk, wcount, lane);
-            wcount = 0;
+            if (cur >= 0 && o.count > 0) warp_flush(J[cur], o.wr, o.ws, o.wk, o.count, lane);
+            o.count = 0;
             cur = tk.join;
         }
         const JoinDesc& d = J[tk.join];
@@ -1053,11 +1115,11 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         uint32_t nb = 32;
         while (nb < (uint32_t)nr) nb <<= 1;
         const uint32_t mask = nb - 1;
-        // the previous task's probe is done with table and off (and s_task[slot ^ 1] is written)
+        // the previous task's probe is done with table, off and bitmap (and s_task[slot ^ 1] is written)
         for (uint32_t i = threadIdx.x; i <= nb; i += kThreads) off[i] = 0;
+        for (int i = threadIdx.x; i < kBitmapWords; i += kThreads) bitmap[i] = 0;
         __syncthreads();
-        // ---- build
-        // keys first (counted), values after the scan (placed): fewer live registers
+        // ---- build: keys first (counted, bitmap bits set), values after the scan (placed)
         uint32_t br[kBuildPer];  // bucket << 16 | rank in bucket
         {
             uint32_t bkey[kBuildPer];
@@ -1072,6 +1134,8 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
                 if (i < nr) {
                     const uint32_t bk = bucket_of(bkey[k], mask);
                     br[k] = (bk << 16) | atomicAdd(&off[bk], 1u);
+                    const uint32_t pb = presence_bit(bkey[k]);
+                    atomicOr(&bitmap[pb >> 5], 1u << (pb & 31u));
                 }
             }
         }
@@ -1085,6 +1149,7 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         __syncthreads();
         // ---- probe
         const uint32_t pn = tk.p_len;
+        int qn = 0;  // candidates in this warp's queue (warp-uniform)
         for (uint32_t base = 0; base < pn; base += (uint32_t)(kProbeU * kThreads)) {
             uint2 e[kProbeU];
 #pragma unroll
@@ -1094,45 +1159,34 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
             }
 #pragma unroll
             for (int u = 0; u < kProbeU; ++u) {
-                if (base + u * kThreads >= pn) break;  // warp-uniform: nothing left for any lane
                 const uint32_t i = base + u * kThreads + threadIdx.x;
-                uint32_t lo = 0, hi = 0;
+                bool cand = false;
                 if (i < pn) {
-                    const uint32_t bk = bucket_of(e[u].x, mask);
-                    lo = off[bk];
-                    hi = off[bk + 1];
+                    const uint32_t pb = presence_bit(e[u].x);
+                    cand = (bitmap[pb >> 5] >> (pb & 31u)) & 1u;
                 }
-                while (__any_sync(0xffffffffu, lo < hi)) {
-                    bool m = false;
-                    uint32_t rv = 0;
-                    if (lo < hi) {
-                        const uint2 cc = table[lo];
-                        m = (cc.x == e[u].x);
-                        rv = cc.y;
-                        ++lo;
-                    }
-                    const uint32_t mm = __ballot_sync(0xffffffffu, m);
-                    if (mm) {
-                        const int n = __popc(mm);
-                        if (wcount + n > kWarpBuf) {
-                            warp_flush(d, wr, ws, wk, wcount, lane);
-                            wcount = 0;
-                        }
-                        if (m) {
-                            const int pos = wcount + __popc(mm & lanemask_lt());
-                            wr[pos] = bs ? e[u].y : rv;
-                            ws[pos] = bs ? rv : e[u].y;
-                            if (emit_key) wk[pos] = e[u].x;
-                        }
-                        wcount += n;
+                const uint32_t cm = __ballot_sync(0xffffffffu, cand);
+                if (cm) {
+                    if (cand) q[qn + __popc(cm & lanemask_lt())] = e[u];
+                    qn += __popc(cm);
+                    __syncwarp();
+                    if (qn >= 32) {
+                        probe_candidates(d, q, 32, table, off, mask, bs, emit_key, lane, o);
+                        // move the overflow (fewer than 32) to the front of the queue
+                        const uint2 rest = lane < qn - 32 ? q[32 + lane] : make_uint2(0u, 0u);
+                        __syncwarp();
+                        if (lane < qn - 32) q[lane] = rest;
+                        qn -= 32;
                         __syncwarp();
                     }
                 }
             }
         }
+        if (qn > 0) probe_candidates(d, q, qn, table, off, mask, bs, emit_key, lane, o);
+        __syncwarp();
         __syncthreads();
     }
-    if (cur >= 0 && wcount > 0) warp_flush(J[cur], wr, ws, wk, wcount, lane);
+    if (cur >= 0 && o.count > 0) warp_flush(J[cur], o.wr, o.ws, o.wk, o.count, lane);
 }
 
 // Copies each join's match count to the caller's device int64 (if requested).
@@ -1239,7 +1293,8 @@ cudaError_t enqueue_scan(const uint32_t* in, int64_t* out, int64_t n, int64_t* t
 }
 
 size_t probe_smem_bytes(int table_cap, int emit_key) {
-    return (size_t)table_cap * 8 + ((size_t)table_cap + 4) * 4 +
+    return (size_t)table_cap * 8 + (size_t)(kThreads / 32) * kQueue * 8 + (size_t)kBitmapWords * 4 +
+           ((size_t)table_cap + 4) * 4 +
            (size_t)(kThreads / 32) * kWarpBuf * (emit_key ? 3 : 2) * 4;
 }
 
