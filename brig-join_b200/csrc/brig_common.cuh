@@ -53,7 +53,7 @@ BRIG_HD uint32_t mix32(uint32_t x) {
 }
 
 // SplitMix64 finaliser (Steele, Lea, Flood, "Fast splittable pseudorandom number generators",
-// OOPSLA 2014). Used for the Bloom filter's block and bit positions and by the input generator.
+// OOPSLA 2014). Used by the input generator and for Bloom hashes beyond the eighth.
 BRIG_HD uint64_t mix64(uint64_t x) {
     x ^= x >> 30; x *= 0xbf58476d1ce4e5b9ull;
     x ^= x >> 27; x *= 0x94d049bb133111ebull;
@@ -119,7 +119,10 @@ struct BloomKey {
     uint32_t mask[8];   // bits to set/test in the block's 8 words
 };
 
-BRIG_HD uint64_t bloom_hash(uint32_t key) { return mix64((uint64_t)key ^ 0x6a09e667f3bcc909ull); }
+// The Bloom hash is mix32(key) (which the partition functions compute anyway) times an odd 64-bit
+// constant: multiplication by an odd constant is a bijection modulo every power of two, so each
+// field of the product is uniform when mix32(key) is, and the top bits depend on every input bit.
+BRIG_HD uint64_t bloom_hash(uint32_t key) { return (uint64_t)mix32(key) * 0x9e3779b97f4a7c15ull; }
 
 // Bits 40..63 of the hash pick the block (24-bit multiply-shift range reduction).
 BRIG_HD uint32_t bloom_block_of(uint64_t g, uint32_t seg_blocks) {

@@ -354,8 +354,10 @@ __device__ __forceinline__ bool bloom_words_pass(uint32_t key, uint32_t seg_bloc
            ((w1.x & bk.mask[4]) == bk.mask[4]) && ((w1.y & bk.mask[5]) == bk.mask[5]) &&
            ((w1.z & bk.mask[6]) == bk.mask[6]) && ((w1.w & bk.mask[7]) == bk.mask[7]);
 }
-__device__ __forceinline__ const uint4* bloom_block(const JoinDesc& d, uint32_t f, uint64_t g) {
-    return reinterpret_cast<const uint4*>(d.bloom + ((int64_t)f * d.seg_blocks + bloom_block_of(g, d.seg_blocks)) * 8);
+// The 32-byte block of a key with hash g in the segment of finest partition f.
+__device__ __forceinline__ const uint4* bloom_block(const uint32_t* __restrict__ bloom, uint32_t seg_blocks, uint32_t f,
+                                                    uint64_t g) {
+    return reinterpret_cast<const uint4*>(bloom + ((int64_t)f * seg_blocks + bloom_block_of(g, seg_blocks)) * 8);
 }
 // Tests the key with hash g (key itself for k > 8) against its loaded block words w0, w1: for
 // k <= 8 word w must have bit (g >> 5w) & 31 set for every w < k.
@@ -433,10 +435,14 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             // compacted (key, value) into R.cmp[b, b + count) and counted per level-1 partition.
             const uint32_t* __restrict__ key = R.key;
             const uint32_t* __restrict__ val = R.val;
+            // descriptor fields in registers: the stores below could alias the descriptor, so
+            // fields read through `d` inside the loop would be reloaded after every store
             const int bk = d.bloom_k;
+            const uint32_t seg_blocks = d.seg_blocks;
+            const uint32_t* __restrict__ bloom = d.bloom;
+            uint2* __restrict__ cmp = R.cmp;
             for (int64_t i0 = b; i0 < e; i0 += kProbeILP * kThreads) {
-                uint32_t kk[kProbeILP], p1[kProbeILP];
-                uint64_t gg[kProbeILP];
+                uint32_t kk[kProbeILP];
                 uint4 w0[kProbeILP], w1[kProbeILP];
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
@@ -446,10 +452,8 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    p1[u] = part1(pf, kk[u]);
-                    gg[u] = bloom_hash(kk[u]);
                     if (i < e) {
-                        const uint4* blk = bloom_block(d, p1[u] * pf.P2 + part2(pf, kk[u]), gg[u]);
+                        const uint4* blk = bloom_block(bloom, seg_blocks, part_fine(pf, kk[u]), bloom_hash(kk[u]));
                         w0[u] = __ldg(blk);
                         w1[u] = __ldg(blk + 1);
                     }
@@ -457,16 +461,16 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    const bool pass = i < e && bloom_pass(gg[u], kk[u], d.seg_blocks, bk, w0[u], w1[u]);
+                    const bool pass = i < e && bloom_pass(bloom_hash(kk[u]), kk[u], seg_blocks, bk, w0[u], w1[u]);
                     const uint32_t m = __ballot_sync(0xffffffffu, pass);
                     if (m) {
                         uint32_t base = 0;
                         if (lane == 0) base = atomicAdd(&s_cursor, (uint32_t)__popc(m));
                         base = __shfl_sync(0xffffffffu, base, 0);
                         if (pass) {
-                            atomicAdd(&sh_cnt[p1[u]], 1u);
+                            atomicAdd(&sh_cnt[part1(pf, kk[u])], 1u);  // survivors only
                             const int64_t dst = b + base + __popc(m & lanemask_lt());
-                            if (dst < e) R.cmp[dst] = make_uint2(kk[u], __ldg(val + i));
+                            if (dst < e) cmp[dst] = make_uint2(kk[u], __ldg(val + i));
                             else atomicAdd(&gwords[kGErrors], 1ull);
                         }
                     }
@@ -642,6 +646,10 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         } else {
             // the filter segments of this level-1 partition are shared by every CTA working on it
             const int bk = d.bloom_k;
+            const uint32_t seg_blocks = d.seg_blocks;
+            const uint32_t* __restrict__ bloom = d.bloom;
+            uint2* __restrict__ cmp = R.cmp;
+            const uint32_t fbase = x.p * P2;
             for (int64_t i0 = begin; i0 < end; i0 += kProbeILP * kThreads) {
                 uint2 e[kProbeILP];
                 uint32_t q[kProbeILP];
@@ -658,7 +666,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                     q[u] = bin(e[u].x);
                     gg[u] = bloom_hash(e[u].x);
                     if (i < end) {
-                        const uint4* blk = bloom_block(d, x.p * P2 + q[u], gg[u]);
+                        const uint4* blk = bloom_block(bloom, seg_blocks, fbase + q[u], gg[u]);
                         w0[u] = __ldg(blk);
                         w1[u] = __ldg(blk + 1);
                     }
@@ -666,7 +674,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    const bool pass = i < end && bloom_pass(gg[u], e[u].x, d.seg_blocks, bk, w0[u], w1[u]);
+                    const bool pass = i < end && bloom_pass(gg[u], e[u].x, seg_blocks, bk, w0[u], w1[u]);
                     const uint32_t m = __ballot_sync(0xffffffffu, pass);
                     if (m) {
                         uint32_t base = 0;
@@ -675,7 +683,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                         if (pass) {
                             atomicAdd(&cnt[q[u]], 1u);
                             const int64_t dst = begin + base + __popc(m & lanemask_lt());
-                            if (dst < end) R.cmp[dst] = e[u];
+                            if (dst < end) cmp[dst] = e[u];
                             else atomicAdd(&gwords[kGErrors], 1ull);
                         }
                     }
@@ -782,7 +790,11 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
         const uint32_t nw = d.seg_blocks * 8;
         const int64_t words = (f1 - f0) * (int64_t)nw;
         uint32_t* gseg = d.bloom + f0 * (int64_t)nw;
+        // descriptor fields in registers: the atomics below may write global memory (segments too
+        // large for shared memory), so fields read through `d` would be reloaded after each one
         const int k = d.bloom_k;
+        const PartFn pf = d.pf;
+        const uint32_t seg_blocks = d.seg_blocks;
         const uint32_t l8 = threadIdx.x & 7u, rs = 5u * l8;
         const bool in_smem = words <= smem_words;
         uint32_t* dst = in_smem ? seg : gseg;
@@ -799,13 +811,13 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
             for (int u = 0; u < kProbeILP; ++u) {
                 const int64_t i = i0 + u * kThreads + threadIdx.x;
                 if (i >= end) continue;
-                const int64_t local = (int64_t)part_fine(d.pf, kk[u]) - f0;
+                const int64_t local = (int64_t)part_fine(pf, kk[u]) - f0;
                 if (local < 0 || local >= f1 - f0) {
                     atomicAdd(&gwords[kGErrors], 1ull);
                     continue;
                 }
                 const uint64_t g = bloom_hash(kk[u]);
-                uint32_t* blk = dst + local * nw + (int64_t)bloom_block_of(g, d.seg_blocks) * 8;
+                uint32_t* blk = dst + local * nw + (int64_t)bloom_block_of(g, seg_blocks) * 8;
                 // Lane l starts at word l % 8 of its block, so the lanes of one atomic instruction
                 // touch different words and mostly different shared-memory banks (all lanes on
                 // the same word would be an 8-way bank conflict, since blocks are 8 words). For
