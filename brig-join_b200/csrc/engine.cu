@@ -171,6 +171,7 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
             o.bloom = L.take((size_t)p.nfine * p.seg_blocks * 32);
             sh.any_bloom = true;
             if (p.bloom_level == 1) sh.any_bloom_l1 = true;
+            if (p.bloom_level == 2) sh.any_bloom_l2 = true;
             sh.total_bloom_groups += (p.nfine + p.bloom_group - 1) / p.bloom_group;
             const int64_t nw = (int64_t)p.seg_blocks * 8;
             sh.max_seg_words = std::max<int>(sh.max_seg_words, (int)nw);
@@ -466,6 +467,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
         if (joins[j].out.key) a.emit_key = 1;
     a.any_bloom = sh.any_bloom ? 1 : 0;
     a.any_bloom_l1 = sh.any_bloom_l1 ? 1 : 0;
+    a.any_bloom_l2 = sh.any_bloom_l2 ? 1 : 0;
     a.num_sms = num_sms;
     a.stage_events = nullptr;
     a.stages = kRunAll;

@@ -76,6 +76,7 @@ struct Shape {
     int max_p1 = 1, max_p2 = 1, max_seg_words = 0, bloom_smem_words = 0;
     bool any_bloom = false;
     bool any_bloom_l1 = false;
+    bool any_bloom_l2 = false;
 };
 
 // Lays out `nj` joins in one workspace; fills jo[0..nj) and sh. Allocates nothing.

@@ -371,6 +371,7 @@ __device__ __forceinline__ bool bloom_pass(uint64_t g, uint32_t key, uint32_t se
     return (ok & 1u) != 0;
 }
 constexpr int kProbeILP = 4;  // keys per thread with their filter blocks in flight together
+constexpr int kL2ProbeILP = 3;  // the level-2 probe reads L2-resident blocks: shorter latency, fewer registers
 
 // ---------------------------------------------------------------------------------------------
 // Level 1, pass 1: per-slice histogram over P1 partitions (R, or S without Bloom), or the fused
@@ -610,6 +611,9 @@ __global__ void k_l2_plan(const JoinDesc* __restrict__ J, int nj, int rel, const
 
 // Level-2 histogram of one slice: counts by level-2 id, or (S with a level-2 Bloom probe) tests
 // every key and compacts the survivors into cmp[slice begin, + survivors).
+// kBloom selects the slices this launch handles (S slices of joins probing their filter at level 2,
+// or all others); one instantiation per form keeps each within 64 registers.
+template <bool kBloom>
 __global__ void __launch_bounds__(kThreads, 2)
 k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
           const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
@@ -627,11 +631,12 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         const int64_t end = min_i64(R.b1[x.p + 1], begin + kL2Slice);
         const Bin2 bin{d.pf};
         const bool bloom = rel == 1 && d.bloom != nullptr && d.bloom_level == 2;
+        if (bloom != kBloom) continue;  // the other instantiation's slice (block-uniform)
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cnt[q] = 0;
         if (threadIdx.x == 0) s_surv = 0;
         __syncthreads();
         const uint2* __restrict__ l1 = R.l1;
-        if (!bloom) {
+        if constexpr (!kBloom) {
             for (int64_t i0 = begin + threadIdx.x; i0 < end; i0 += 8 * kThreads) {
                 uint32_t kk[8];
 #pragma unroll
@@ -650,38 +655,37 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t* __restrict__ bloom = d.bloom;
             uint2* __restrict__ cmp = R.cmp;
             const uint32_t fbase = x.p * P2;
-            for (int64_t i0 = begin; i0 < end; i0 += kProbeILP * kThreads) {
-                uint2 e[kProbeILP];
-                uint32_t q[kProbeILP];
-                uint64_t gg[kProbeILP];
-                uint4 w0[kProbeILP], w1[kProbeILP];
+            for (int64_t i0 = begin; i0 < end; i0 += kL2ProbeILP * kThreads) {
+                // only the tuples and their filter blocks are held per key (the hashes are cheap
+                // to recompute, registers are not)
+                uint2 e[kL2ProbeILP];
+                uint4 w0[kL2ProbeILP], w1[kL2ProbeILP];
 #pragma unroll
-                for (int u = 0; u < kProbeILP; ++u) {
+                for (int u = 0; u < kL2ProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
                     e[u] = i < end ? __ldcs(&l1[i]) : make_uint2(0u, 0u);
                 }
 #pragma unroll
-                for (int u = 0; u < kProbeILP; ++u) {
+                for (int u = 0; u < kL2ProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    q[u] = bin(e[u].x);
-                    gg[u] = bloom_hash(e[u].x);
                     if (i < end) {
-                        const uint4* blk = bloom_block(bloom, seg_blocks, fbase + q[u], gg[u]);
+                        const uint4* blk = bloom_block(bloom, seg_blocks, fbase + bin(e[u].x), bloom_hash(e[u].x));
                         w0[u] = __ldg(blk);
                         w1[u] = __ldg(blk + 1);
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < kProbeILP; ++u) {
+                for (int u = 0; u < kL2ProbeILP; ++u) {
                     const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    const bool pass = i < end && bloom_pass(gg[u], e[u].x, seg_blocks, bk, w0[u], w1[u]);
+                    const bool pass =
+                        i < end && bloom_pass(bloom_hash(e[u].x), e[u].x, seg_blocks, bk, w0[u], w1[u]);
                     const uint32_t m = __ballot_sync(0xffffffffu, pass);
                     if (m) {
                         uint32_t base = 0;
                         if (lane == 0) base = atomicAdd(&s_surv, (uint32_t)__popc(m));
                         base = __shfl_sync(0xffffffffu, base, 0);
                         if (pass) {
-                            atomicAdd(&cnt[q[u]], 1u);
+                            atomicAdd(&cnt[bin(e[u].x)], 1u);
                             const int64_t dst = begin + base + __popc(m & lanemask_lt());
                             if (dst < end) cmp[dst] = e[u];
                             else atomicAdd(&gwords[kGErrors], 1ull);
@@ -1017,8 +1021,10 @@ __device__ __forceinline__ void warp_flush(const JoinDesc& d, const uint32_t* wr
 //     in its bucket), scans the counts into bucket starts (off[nb] = the chunk size) and places
 //     every tuple at off[bucket] + rank: a bucketised table, bucket b = [off[b], off[b+1]). Every
 //     build key also sets one bit of a 65536-bit presence bitmap;
-//   * streams the other side straight from global memory, kProbeU coalesced tuples per thread in
-//     flight. A streamed tuple whose bitmap bit is clear cannot match (at most 4096 keys set at
+//   * streams the other side: its first kProbeFirst tuples from shared memory, where a bulk copy
+//     issued at the start of the task has put them while the table was built, the rest straight
+//     from global memory with kProbeU coalesced tuples per thread in flight. (The build side is
+//     loaded once, into registers.) A streamed tuple whose bitmap bit is clear cannot match (at most 4096 keys set at
 //     most 6% of the bits); the others are compacted with ballot/popc into the warp's candidate
 //     queue in shared memory. Every 32 queued candidates the warp scans their buckets in lock step,
 //     one candidate per lane, and compacts matches into the warp's output staging buffer, which is
@@ -1030,6 +1036,7 @@ constexpr int kProbeU = 4;                        // streamed tuples per thread 
 constexpr int kBuildPer = kMaxTable / kThreads;   // build tuples per thread
 constexpr int kBitmapWords = 2048;                // 65536-bit presence bitmap
 constexpr int kQueue = 64;                        // candidates queued per warp
+constexpr int kProbeFirst = 2048;                 // first probe-side tuples of a task, bulk-copied
 
 __device__ __forceinline__ uint32_t presence_bit(uint32_t key) { return (key * 0x9E3779B1u) >> 16; }
 
@@ -1081,17 +1088,61 @@ __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2*
     }
 }
 
+// Streams tuples [0, n) of `src` (shared memory when kShared, else global) through the filter and
+// the warp's candidate queue; full warps of candidates are probed as they form.
+template <bool kShared, int U>
+__device__ __forceinline__ void probe_stream(const JoinDesc& d, const uint2* __restrict__ src, uint32_t n,
+                                             const uint32_t* bitmap, uint2* q, int& qn, const uint2* table,
+                                             const uint32_t* off, uint32_t mask, bool bs, int emit_key, int lane,
+                                             WarpOut& o) {
+    for (uint32_t base = 0; base < n; base += (uint32_t)(U * kThreads)) {
+        uint2 e[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t i = base + u * kThreads + threadIdx.x;
+            if (kShared) e[u] = i < n ? src[i] : make_uint2(0u, 0u);
+            else e[u] = i < n ? __ldcs(src + i) : make_uint2(0u, 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t i = base + u * kThreads + threadIdx.x;
+            bool cand = false;
+            if (i < n) {
+                const uint32_t pb = presence_bit(e[u].x);
+                cand = (bitmap[pb >> 5] >> (pb & 31u)) & 1u;
+            }
+            const uint32_t cm = __ballot_sync(0xffffffffu, cand);
+            if (cm) {
+                if (cand) q[qn + __popc(cm & lanemask_lt())] = e[u];
+                qn += __popc(cm);
+                __syncwarp();
+                if (qn >= 32) {
+                    probe_candidates(d, q, 32, table, off, mask, bs, emit_key, lane, o);
+                    // move the overflow (fewer than 32) to the front of the queue
+                    const uint2 rest = lane < qn - 32 ? q[32 + lane] : make_uint2(0u, 0u);
+                    __syncwarp();
+                    if (lane < qn - 32) q[lane] = rest;
+                    qn -= 32;
+                    __syncwarp();
+                }
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 2)
 k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned long long* gwords,
         int table_cap, int emit_key) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2* table = reinterpret_cast<uint2*>(smem);                              // [table_cap]
-    uint2* queue = table + table_cap;                                           // [warps][kQueue]
+    uint2* pbuf = table + table_cap;                                            // [kProbeFirst + 2]
+    uint2* queue = pbuf + kProbeFirst + 2;                                      // [warps][kQueue]
     uint32_t* bitmap = reinterpret_cast<uint32_t*>(queue + (kThreads / 32) * kQueue);  // [kBitmapWords]
     uint32_t* off = bitmap + kBitmapWords;                                      // [table_cap + 1] (+pad)
     uint32_t* wbuf = off + table_cap + 4;
     __shared__ uint32_t tmp[kThreads / 32];
     __shared__ long long s_task[2];
+    __shared__ __align__(8) uint64_t bar;
     unsigned long long* errors = &gwords[kGErrors];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int words_per_warp = kWarpBuf * (emit_key ? 3 : 2);
@@ -1102,23 +1153,34 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     o.count = 0;
     uint2* q = queue + wid * kQueue;
     int cur = -1;
+    uint32_t ph = 0;
     const long long ntasks = (long long)gwords[kGTasks];
-    if (threadIdx.x == 0) s_task[0] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
+    if (threadIdx.x == 0) {
+        s_task[0] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
     __syncthreads();
     for (int slot = 0;; slot ^= 1) {
         const long long t = s_task[slot];
         if (t >= ntasks) break;
-        if (threadIdx.x == 0) s_task[slot ^ 1] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
         const Task& tk = tasks[t];
+        const JoinDesc& d = J[tk.join];
+        const bool bs = (tk.flags & kTaskBuildS) != 0;
+        const uint2* __restrict__ bsrc = final_buf(d, bs ? 1 : 0) + tk.b_begin;
+        const uint2* __restrict__ psrc = final_buf(d, bs ? 0 : 1) + tk.p_begin;
+        const uint32_t pn = tk.p_len;
+        const uint32_t first = pn < (uint32_t)kProbeFirst ? pn : (uint32_t)kProbeFirst;
+        // the first probe chunk is copied into shared memory while the table is built
+        if (threadIdx.x == 0) {
+            s_task[slot ^ 1] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
+            PackedTiles{psrc}.issue(0, (int)first, reinterpret_cast<unsigned char*>(pbuf), &bar);
+        }
         if (tk.join != cur) {
             if (cur >= 0 && o.count > 0) warp_flush(J[cur], o.wr, o.ws, o.wk, o.count, lane);
             o.count = 0;
             cur = tk.join;
         }
-        const JoinDesc& d = J[tk.join];
-        const bool bs = (tk.flags & kTaskBuildS) != 0;
-        const uint2* __restrict__ bsrc = final_buf(d, bs ? 1 : 0) + tk.b_begin;
-        const uint2* __restrict__ psrc = final_buf(d, bs ? 0 : 1) + tk.p_begin;
         int nr = (int)tk.b_len;
         if (nr > table_cap) {
             if (threadIdx.x == 0) atomicAdd(errors, 1ull);
@@ -1127,28 +1189,26 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         uint32_t nb = 32;
         while (nb < (uint32_t)nr) nb <<= 1;
         const uint32_t mask = nb - 1;
-        // the previous task's probe is done with table, off and bitmap (and s_task[slot ^ 1] is written)
+        // the previous task's probe is done with table, off, bitmap and pbuf
         for (uint32_t i = threadIdx.x; i <= nb; i += kThreads) off[i] = 0;
         for (int i = threadIdx.x; i < kBitmapWords; i += kThreads) bitmap[i] = 0;
+        // ---- build: count per bucket (the atomic's result is the rank), set the bitmap bits
+        uint2 bt[kBuildPer];
+#pragma unroll
+        for (int k = 0; k < kBuildPer; ++k) {
+            const int i = k * kThreads + threadIdx.x;
+            if (i < nr) bt[k] = __ldg(bsrc + i);
+        }
         __syncthreads();
-        // ---- build: keys first (counted, bitmap bits set), values after the scan (placed)
         uint32_t br[kBuildPer];  // bucket << 16 | rank in bucket
-        {
-            uint32_t bkey[kBuildPer];
 #pragma unroll
-            for (int k = 0; k < kBuildPer; ++k) {
-                const int i = k * kThreads + threadIdx.x;
-                if (i < nr) bkey[k] = __ldg(&bsrc[i].x);
-            }
-#pragma unroll
-            for (int k = 0; k < kBuildPer; ++k) {
-                const int i = k * kThreads + threadIdx.x;
-                if (i < nr) {
-                    const uint32_t bk = bucket_of(bkey[k], mask);
-                    br[k] = (bk << 16) | atomicAdd(&off[bk], 1u);
-                    const uint32_t pb = presence_bit(bkey[k]);
-                    atomicOr(&bitmap[pb >> 5], 1u << (pb & 31u));
-                }
+        for (int k = 0; k < kBuildPer; ++k) {
+            const int i = k * kThreads + threadIdx.x;
+            if (i < nr) {
+                const uint32_t bk = bucket_of(bt[k].x, mask);
+                br[k] = (bk << 16) | atomicAdd(&off[bk], 1u);
+                const uint32_t pb = presence_bit(bt[k].x);
+                atomicOr(&bitmap[pb >> 5], 1u << (pb & 31u));
             }
         }
         __syncthreads();
@@ -1156,44 +1216,17 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
 #pragma unroll
         for (int k = 0; k < kBuildPer; ++k) {
             const int i = k * kThreads + threadIdx.x;
-            if (i < nr) table[off[br[k] >> 16] + (br[k] & 0xffffu)] = __ldg(bsrc + i);
+            if (i < nr) table[off[br[k] >> 16] + (br[k] & 0xffffu)] = bt[k];
         }
+        mbar_wait(&bar, ph, errors);
+        ph ^= 1u;
         __syncthreads();
-        // ---- probe
-        const uint32_t pn = tk.p_len;
+        // ---- probe: the first chunk from shared memory, the rest straight from global memory
         int qn = 0;  // candidates in this warp's queue (warp-uniform)
-        for (uint32_t base = 0; base < pn; base += (uint32_t)(kProbeU * kThreads)) {
-            uint2 e[kProbeU];
-#pragma unroll
-            for (int u = 0; u < kProbeU; ++u) {
-                const uint32_t i = base + u * kThreads + threadIdx.x;
-                e[u] = i < pn ? __ldcs(psrc + i) : make_uint2(0u, 0u);
-            }
-#pragma unroll
-            for (int u = 0; u < kProbeU; ++u) {
-                const uint32_t i = base + u * kThreads + threadIdx.x;
-                bool cand = false;
-                if (i < pn) {
-                    const uint32_t pb = presence_bit(e[u].x);
-                    cand = (bitmap[pb >> 5] >> (pb & 31u)) & 1u;
-                }
-                const uint32_t cm = __ballot_sync(0xffffffffu, cand);
-                if (cm) {
-                    if (cand) q[qn + __popc(cm & lanemask_lt())] = e[u];
-                    qn += __popc(cm);
-                    __syncwarp();
-                    if (qn >= 32) {
-                        probe_candidates(d, q, 32, table, off, mask, bs, emit_key, lane, o);
-                        // move the overflow (fewer than 32) to the front of the queue
-                        const uint2 rest = lane < qn - 32 ? q[32 + lane] : make_uint2(0u, 0u);
-                        __syncwarp();
-                        if (lane < qn - 32) q[lane] = rest;
-                        qn -= 32;
-                        __syncwarp();
-                    }
-                }
-            }
-        }
+        probe_stream<true, 2>(d, pbuf + PackedTiles{psrc}.mis(0), first, bitmap, q, qn, table, off, mask, bs,
+                           emit_key, lane, o);
+        if (pn > first)
+            probe_stream<false, kProbeU>(d, psrc + first, pn - first, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
         if (qn > 0) probe_candidates(d, q, qn, table, off, mask, bs, emit_key, lane, o);
         __syncwarp();
         __syncthreads();
@@ -1305,7 +1338,8 @@ cudaError_t enqueue_scan(const uint32_t* in, int64_t* out, int64_t n, int64_t* t
 }
 
 size_t probe_smem_bytes(int table_cap, int emit_key) {
-    return (size_t)table_cap * 8 + (size_t)(kThreads / 32) * kQueue * 8 + (size_t)kBitmapWords * 4 +
+    return (size_t)table_cap * 8 + (size_t)(kProbeFirst + 2) * 8 + (size_t)(kThreads / 32) * kQueue * 8 +
+           (size_t)kBitmapWords * 4 +
            ((size_t)table_cap + 4) * 4 +
            (size_t)(kThreads / 32) * kWarpBuf * (emit_key ? 3 : 2) * 4;
 }
@@ -1398,8 +1432,13 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 return err;
             uint32_t* h2 = a.hist2 + a.h2_begin[rel];
             if ((err = cudaMemsetAsync(h2, 0, (size_t)a.h2_len[rel] * 4, st)) != cudaSuccess) return err;
-            k_l2_hist<<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4, st>>>(
+            k_l2_hist<false><<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4, st>>>(
                 a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2, a.gwords);
+            if (rel == 1 && a.any_bloom_l2) {
+                k_l2_hist<true><<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4, st>>>(
+                a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2, a.gwords);
+                ++launches;
+            }
             ++launches;
             if ((err = enqueue_scan(h2, a.hist2_scan + a.h2_begin[rel], a.h2_len[rel], a.scan_tmp, nullptr, st)) !=
                 cudaSuccess)

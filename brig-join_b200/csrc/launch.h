@@ -39,6 +39,7 @@ struct PipelineArgs {
     int emit_key;
     int any_bloom;
     int any_bloom_l1;                 // some join probes its filter in S's first pass
+    int any_bloom_l2;                 // some join probes its filter in S's second pass
     int num_sms;
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
     int stages;                       // kRunPartR | kRunBloom | kRunPartS | kRunProbe
