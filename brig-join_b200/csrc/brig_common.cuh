@@ -90,33 +90,49 @@ struct PartFn {
     uint64_t M1, M2;    // fastmod magics (modulo mode)
 };
 
-BRIG_HD uint32_t part1(const PartFn& f, uint32_t key) {
-    if (f.mode == 0) return f.b1 == 0 ? 0u : (mix32(key) >> (32 - f.b1));
-    return fastmod(key, f.M1, f.P1);
+// Mode-specialised forms, M = 0 (hash) or 1 (modulo). The partition kernels are instantiated per
+// mode and skip the joins of the other mode, so their per-key code carries no mode test. In hash
+// mode p is the top b1 bits of mix32(key) and q the next b2 bits (both 0 when the bit count is 0).
+template <int M>
+BRIG_HD uint32_t part1_m(const PartFn& f, uint32_t key) {
+    if constexpr (M == 0) return (uint32_t)(((uint64_t)mix32(key) << f.b1) >> 32);
+    else return fastmod(key, f.M1, f.P1);
 }
-BRIG_HD uint32_t part2(const PartFn& f, uint32_t key) {
-    if (f.mode == 0) return f.b2 == 0 ? 0u : ((mix32(key) << f.b1) >> (32 - f.b2));
-    return fastmod(key, f.M2, f.P2);
+template <int M>
+BRIG_HD uint32_t part2_m(const PartFn& f, uint32_t key) {
+    if constexpr (M == 0) return (uint32_t)(((uint64_t)(mix32(key) << f.b1) << f.b2) >> 32);
+    else return fastmod(key, f.M2, f.P2);
 }
 // Finest partition id p * P2 + q: the probe-task unit and the Bloom segment index.
+template <int M>
+BRIG_HD uint32_t part_fine_m(const PartFn& f, uint32_t key) {
+    return part1_m<M>(f, key) * f.P2 + part2_m<M>(f, key);
+}
+BRIG_HD uint32_t part1(const PartFn& f, uint32_t key) { return f.mode == 0 ? part1_m<0>(f, key) : part1_m<1>(f, key); }
+BRIG_HD uint32_t part2(const PartFn& f, uint32_t key) { return f.mode == 0 ? part2_m<0>(f, key) : part2_m<1>(f, key); }
 BRIG_HD uint32_t part_fine(const PartFn& f, uint32_t key) {
-    return part1(f, key) * f.P2 + part2(f, key);
+    return f.mode == 0 ? part_fine_m<0>(f, key) : part_fine_m<1>(f, key);
 }
 // Shared-memory bucket of a key in a table of nb (power of two) buckets: the low bits of the mix.
 BRIG_HD uint32_t bucket_of(uint32_t key, uint32_t nb_mask) { return mix32(key) & nb_mask; }
 
 // ---- Bloom filter -------------------------------------------------------------------------------
-// Cache-line blocked and sectorised: the filter is one segment per finest partition, a segment is
-// seg_blocks blocks of 256 bits (one 32-byte DRAM sector, eight 32-bit words), and a key sets one
-// bit in each of its first k words (words 0..7, then again from word 0 for k > 8). So a probe is one
-// sector load and the masks are shifts, with no search or dynamic indexing ("sectorized" blocked
-// filters, Lang et al., "Performance-Optimal Filtering: Bloom overtakes Cuckoo at High
-// Throughput", VLDB 2019). The reference uses 256-bit blocks with k bit positions anywhere in the
-// block and one segment per first-level partition (src/bloom.cu:698-722,
+// Cache-sectorized blocked Bloom filter (Lang, Neumann, Kemper, Boncz, "Performance-Optimal
+// Filtering: Bloom overtakes Cuckoo at High Throughput", VLDB 2019). The filter is one segment per
+// finest partition; a segment is seg_blocks blocks of 256 bits, one 32-byte DRAM sector of eight
+// 32-bit words in two groups of four. A key picks one word in each group and sets its k bit
+// positions in those two words: the first ceil(k/2) in the word of group 0, the rest in the word of
+// group 1. So a build is two 32-bit atomicOr per key and a probe two word loads from one sector,
+// with no search or dynamic indexing. The reference uses 256-bit blocks with k bit positions
+// anywhere in the block and one segment per first-level partition (src/bloom.cu:698-722,
 // src/hash_kernel.cu:555-582).
+//
+// Hash bits (g = bloom_hash(key)): bits 40..63 pick the block, bits 35..36 and 37..38 the two words,
+// bits 5i..5i+4 the position of bit i for i < 7; positions of bits 7.. come from mix64(g).
 struct BloomKey {
-    uint32_t block;     // block index inside the segment
-    uint32_t mask[8];   // bits to set/test in the block's 8 words
+    uint32_t block;   // block index inside the segment
+    uint32_t wa, wb;  // word of group 0 (0..3) and of group 1 (4..7)
+    uint32_t ma, mb;  // bits to set/test in them
 };
 
 // The Bloom hash is mix32(key) (which the partition functions compute anyway) times an odd 64-bit
@@ -128,21 +144,61 @@ BRIG_HD uint64_t bloom_hash(uint32_t key) { return (uint64_t)mix32(key) * 0x9e37
 BRIG_HD uint32_t bloom_block_of(uint64_t g, uint32_t seg_blocks) {
     return (uint32_t)(((g >> 40) * (uint64_t)seg_blocks) >> 24);
 }
-// Bits to set/test in word w (0..7) of the block: hash i < k sets one bit of word i % 8, at the
-// bit position given by 5 hash bits (bits 5w.. of g for i < 8, of g2 = mix64(g) for i >= 8).
-BRIG_HD uint32_t bloom_word_mask(uint64_t g, uint64_t g2, int k, int w) {
-    uint32_t m = (w < k) ? (1u << ((uint32_t)(g >> (5 * w)) & 31u)) : 0u;
-    if (w + 8 < k) m |= 1u << ((uint32_t)(g2 >> (5 * w)) & 31u);
-    return m;
+
+// Bit masks of a key with hash g. K > 0: k == K known at compile time (a handful of shifts and ORs);
+// K == 0: any k in [1, 16].
+template <int K>
+BRIG_HD void bloom_masks(uint64_t g, int k, uint32_t& ma, uint32_t& mb) {
+    const uint32_t lo = (uint32_t)g, hi = (uint32_t)(g >> 32);
+    auto bit = [&](int i) -> uint32_t {  // i < 7: bits 5i..5i+4 of g
+        const uint32_t p = i < 6 ? (lo >> (5 * i)) : ((lo >> 30) | (hi << 2));
+        return 1u << (p & 31u);
+    };
+    if constexpr (K > 0 && K <= 7) {
+        constexpr int ka = (K + 1) / 2;
+        uint32_t a = 0, b = 0;
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            if (i < ka) a |= bit(i); else b |= bit(i);
+        }
+        ma = a;
+        mb = b;
+    } else {
+        const int ka = (k + 1) >> 1;
+        uint32_t a = 0, b = 0;
+#pragma unroll
+        for (int i = 0; i < 7; ++i) {
+            const uint32_t v = bit(i);
+            a |= i < ka ? v : 0u;
+            b |= (i >= ka && i < k) ? v : 0u;
+        }
+        if (k > 7) {
+            const uint64_t g2 = mix64(g);
+            for (int i = 7; i < k; ++i) {
+                const uint32_t v = 1u << ((uint32_t)(g2 >> (5 * (i - 7))) & 31u);
+                if (i < ka) a |= v; else b |= v;
+            }
+        }
+        ma = a;
+        mb = b;
+    }
 }
 
-BRIG_HD void bloom_key(uint32_t key, uint32_t seg_blocks, int k, BloomKey& bk) {
-    const uint64_t g = bloom_hash(key);
+template <int K = 0>
+BRIG_HD void bloom_key_of_hash(uint64_t g, uint32_t seg_blocks, int k, BloomKey& bk) {
     bk.block = bloom_block_of(g, seg_blocks);
-    const uint64_t g2 = k > 8 ? mix64(g) : 0ull;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) bk.mask[w] = bloom_word_mask(g, g2, k, w);
+    bk.wa = (uint32_t)(g >> 35) & 3u;
+    bk.wb = 4u + ((uint32_t)(g >> 37) & 3u);
+    bloom_masks<K>(g, k, bk.ma, bk.mb);
 }
+
+template <int K = 0>
+BRIG_HD void bloom_key(uint32_t key, uint32_t seg_blocks, int k, BloomKey& bk) {
+    bloom_key_of_hash<K>(bloom_hash(key), seg_blocks, k, bk);
+}
+// Compile-time k class of a join's filter: the Bloom kernels are instantiated for k = 7 (the usual
+// 10 bits/key setting) and for any k, and each instantiation skips the other's joins.
+constexpr int kBloomFastK = 7;
 
 // ---- per-join descriptor (device resident) ------------------------------------------------------
 struct RelPlan {

@@ -468,6 +468,10 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     a.any_bloom = sh.any_bloom ? 1 : 0;
     a.any_bloom_l1 = sh.any_bloom_l1 ? 1 : 0;
     a.any_bloom_l2 = sh.any_bloom_l2 ? 1 : 0;
+    a.modes = 0;
+    for (int j = 0; j < nj; ++j) a.modes |= plans[j].pf.mode == 0 ? 1 : 2;
+    a.kclasses = 0;
+    for (int j = 0; j < nj; ++j) a.kclasses |= (plans[j].bloom && plans[j].k == kBloomFastK) ? 2 : 1;
     a.num_sms = num_sms;
     a.stage_events = nullptr;
     a.stages = kRunAll;

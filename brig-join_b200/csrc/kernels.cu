@@ -34,6 +34,7 @@
 //     word the host reads instead of writing out of bounds.
 #include <cstdio>
 #include <algorithm>
+#include <type_traits>
 #include "launch.h"
 
 namespace brig {
@@ -235,13 +236,15 @@ struct KvTiles {
     }
 };
 
+template <int M>
 struct Bin1 {
     PartFn f;
-    __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return part1(f, key); }
+    __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return part1_m<M>(f, key); }
 };
+template <int M>
 struct Bin2 {
     PartFn f;
-    __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return part2(f, key); }
+    __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return part2_m<M>(f, key); }
 };
 
 // Scatters tuples [begin, end) of `in` into `out`. cursor[b] is the next output position of bin
@@ -346,38 +349,25 @@ __device__ __forceinline__ void init_bars(uint64_t* bars) {
 
 // Bloom probe, split in two so a thread can have several block loads in flight: the address of a
 // key's 32-byte block in the segment of its finest partition f, then the test of the loaded words.
-__device__ __forceinline__ bool bloom_words_pass(uint32_t key, uint32_t seg_blocks, int k, uint4 w0, uint4 w1) {
-    BloomKey bk;
-    bloom_key(key, seg_blocks, k, bk);
-    return ((w0.x & bk.mask[0]) == bk.mask[0]) && ((w0.y & bk.mask[1]) == bk.mask[1]) &&
-           ((w0.z & bk.mask[2]) == bk.mask[2]) && ((w0.w & bk.mask[3]) == bk.mask[3]) &&
-           ((w1.x & bk.mask[4]) == bk.mask[4]) && ((w1.y & bk.mask[5]) == bk.mask[5]) &&
-           ((w1.z & bk.mask[6]) == bk.mask[6]) && ((w1.w & bk.mask[7]) == bk.mask[7]);
+// The Bloom k class of a join (the K of the kernel instantiation that handles it).
+__device__ __forceinline__ int bloom_kclass(const JoinDesc& d) {
+    return (d.bloom != nullptr && d.bloom_k == kBloomFastK) ? kBloomFastK : 0;
 }
-// The 32-byte block of a key with hash g in the segment of finest partition f.
-__device__ __forceinline__ const uint4* bloom_block(const uint32_t* __restrict__ bloom, uint32_t seg_blocks, uint32_t f,
-                                                    uint64_t g) {
-    return reinterpret_cast<const uint4*>(bloom + ((int64_t)f * seg_blocks + bloom_block_of(g, seg_blocks)) * 8);
+
+// Address of the first word of a key's block in the segment of finest partition f.
+__device__ __forceinline__ const uint32_t* bloom_words(const uint32_t* __restrict__ bloom, uint32_t seg_blocks,
+                                                       uint32_t f, uint32_t block) {
+    return bloom + ((int64_t)f * seg_blocks + block) * 8;
 }
-// Tests the key with hash g (key itself for k > 8) against its loaded block words w0, w1: for
-// k <= 8 word w must have bit (g >> 5w) & 31 set for every w < k.
-__device__ __forceinline__ bool bloom_pass(uint64_t g, uint32_t key, uint32_t seg_blocks, int k, uint4 w0, uint4 w1) {
-    if (k > 8) return bloom_words_pass(key, seg_blocks, k, w0, w1);
-    const uint32_t wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-    uint32_t ok = 1u;
-#pragma unroll
-    for (int w = 0; w < 8; ++w)
-        if (w < k) ok &= wv[w] >> ((uint32_t)(g >> (5 * w)) & 31u);
-    return (ok & 1u) != 0;
-}
-constexpr int kProbeILP = 4;  // keys per thread with their filter blocks in flight together
-constexpr int kL2ProbeILP = 3;  // the level-2 probe reads L2-resident blocks: shorter latency, fewer registers
+constexpr int kProbeILP = 6;  // keys per thread with their filter words in flight together
+constexpr int kL2ProbeILP = 6;  // keys per thread with their filter words in flight in the level-2 probe
 
 // ---------------------------------------------------------------------------------------------
 // Level 1, pass 1: per-slice histogram over P1 partitions (R, or S without Bloom), or the fused
 // Bloom probe + survivor compaction + histogram (S with Bloom).
 // hist layout per relation: [p * nslices + s], plus one trailing zero (sentinel) so that the
 // exclusive scan of entry P1*nslices is the relation's total.
+template <int M, int K>
 __global__ void __launch_bounds__(kThreads, 2)
 k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
           uint32_t* __restrict__ hist, unsigned long long* gwords) {
@@ -393,6 +383,7 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         const int64_t b = (int64_t)s * R.slice_len;
         const int64_t e = min(b + R.slice_len, R.n);
         const PartFn pf = d.pf;
+        if (pf.mode != M || bloom_kclass(d) != K) continue;  // another instantiation's join (block-uniform)
         const uint32_t P1 = pf.P1;
         for (uint32_t i = threadIdx.x; i < P1; i += kThreads) sh_cnt[i] = 0;
         if (threadIdx.x == 0) s_cursor = 0;
@@ -410,26 +401,26 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                         k4[u] = __ldcs(reinterpret_cast<const uint4*>(key + i + 4 * u * kThreads));
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        atomicAdd(&sh_cnt[part1(pf, k4[u].x)], 1u);
-                        atomicAdd(&sh_cnt[part1(pf, k4[u].y)], 1u);
-                        atomicAdd(&sh_cnt[part1(pf, k4[u].z)], 1u);
-                        atomicAdd(&sh_cnt[part1(pf, k4[u].w)], 1u);
+                        atomicAdd(&sh_cnt[part1_m<M>(pf, k4[u].x)], 1u);
+                        atomicAdd(&sh_cnt[part1_m<M>(pf, k4[u].y)], 1u);
+                        atomicAdd(&sh_cnt[part1_m<M>(pf, k4[u].z)], 1u);
+                        atomicAdd(&sh_cnt[part1_m<M>(pf, k4[u].w)], 1u);
                     }
                 }
                 for (; i + 3 < e; i += 4 * kThreads) {
                     const uint4 k4 = __ldcs(reinterpret_cast<const uint4*>(key + i));
-                    atomicAdd(&sh_cnt[part1(pf, k4.x)], 1u);
-                    atomicAdd(&sh_cnt[part1(pf, k4.y)], 1u);
-                    atomicAdd(&sh_cnt[part1(pf, k4.z)], 1u);
-                    atomicAdd(&sh_cnt[part1(pf, k4.w)], 1u);
+                    atomicAdd(&sh_cnt[part1_m<M>(pf, k4.x)], 1u);
+                    atomicAdd(&sh_cnt[part1_m<M>(pf, k4.y)], 1u);
+                    atomicAdd(&sh_cnt[part1_m<M>(pf, k4.z)], 1u);
+                    atomicAdd(&sh_cnt[part1_m<M>(pf, k4.w)], 1u);
                 }
                 // tail: at most 3 tuples past the last full vector
                 const int64_t tail0 = b + ((e - b) & ~(int64_t)3);
                 for (int64_t t = tail0 + threadIdx.x; t < e; t += kThreads)
-                    atomicAdd(&sh_cnt[part1(pf, __ldcs(key + t))], 1u);
+                    atomicAdd(&sh_cnt[part1_m<M>(pf, __ldcs(key + t))], 1u);
             } else {
                 for (int64_t t = b + threadIdx.x; t < e; t += kThreads)
-                    atomicAdd(&sh_cnt[part1(pf, __ldcs(key + t))], 1u);
+                    atomicAdd(&sh_cnt[part1_m<M>(pf, __ldcs(key + t))], 1u);
             }
         } else {
             // Bloom probe of every S key against the segment of its finest partition; survivors are
@@ -442,38 +433,60 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t seg_blocks = d.seg_blocks;
             const uint32_t* __restrict__ bloom = d.bloom;
             uint2* __restrict__ cmp = R.cmp;
-            for (int64_t i0 = b; i0 < e; i0 += kProbeILP * kThreads) {
+            const int32_t len = (int32_t)(e - b);  // a slice is far below 2^31 tuples
+            const uint32_t* __restrict__ skey = key + b;
+            for (int32_t r0 = 0; r0 < len; r0 += kProbeILP * kThreads) {
                 uint32_t kk[kProbeILP];
-                uint4 w0[kProbeILP], w1[kProbeILP];
+                uint32_t va[kProbeILP], vb[kProbeILP];
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
-                    const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    kk[u] = i < e ? __ldcs(key + i) : 0u;
+                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+                    kk[u] = r < len ? __ldcs(skey + r) : 0u;
                 }
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
-                    const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    if (i < e) {
-                        const uint4* blk = bloom_block(bloom, seg_blocks, part_fine(pf, kk[u]), bloom_hash(kk[u]));
-                        w0[u] = __ldg(blk);
-                        w1[u] = __ldg(blk + 1);
+                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+                    if (r < len) {
+                        BloomKey bkey;
+                        bloom_key<K>(kk[u], seg_blocks, bk, bkey);
+                        const uint32_t* w =
+                            bloom_words(bloom, seg_blocks, part_fine_m<M>(pf, kk[u]), bkey.block);
+                        va[u] = __ldg(w + bkey.wa);
+                        vb[u] = __ldg(w + bkey.wb);
                     }
                 }
+                uint32_t pm = 0;  // bit u: tuple u passed the filter
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
-                    const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    const bool pass = i < e && bloom_pass(bloom_hash(kk[u]), kk[u], seg_blocks, bk, w0[u], w1[u]);
-                    const uint32_t m = __ballot_sync(0xffffffffu, pass);
-                    if (m) {
-                        uint32_t base = 0;
-                        if (lane == 0) base = atomicAdd(&s_cursor, (uint32_t)__popc(m));
-                        base = __shfl_sync(0xffffffffu, base, 0);
-                        if (pass) {
-                            atomicAdd(&sh_cnt[part1(pf, kk[u])], 1u);  // survivors only
-                            const int64_t dst = b + base + __popc(m & lanemask_lt());
-                            if (dst < e) cmp[dst] = make_uint2(kk[u], __ldg(val + i));
+                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+                    if (r < len) {
+                        uint32_t ma, mb;
+                        bloom_masks<K>(bloom_hash(kk[u]), bk, ma, mb);
+                        if ((va[u] & ma) == ma && (vb[u] & mb) == mb) pm |= 1u << u;
+                    }
+                }
+                // survivors: one shared-memory atomic per warp for the whole group
+                uint32_t bal[kProbeILP];
+                uint32_t tot = 0;
+#pragma unroll
+                for (int u = 0; u < kProbeILP; ++u) {
+                    bal[u] = __ballot_sync(0xffffffffu, (pm >> u) & 1u);
+                    tot += __popc(bal[u]);
+                }
+                if (tot) {
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(&s_cursor, tot);
+                    base = __shfl_sync(0xffffffffu, base, 0);
+#pragma unroll
+                    for (int u = 0; u < kProbeILP; ++u) {
+                        if ((pm >> u) & 1u) {
+                            const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+                            atomicAdd(&sh_cnt[part1_m<M>(pf, kk[u])], 1u);
+                            const int64_t dst = b + base + __popc(bal[u] & lanemask_lt());
+                            if (dst < e) cmp[dst] = make_uint2(kk[u], __ldg(val + b + r));
                             else atomicAdd(&gwords[kGErrors], 1ull);
                         }
+                        base += __popc(bal[u]);
                     }
                 }
             }
@@ -501,7 +514,7 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 // kPacked selects the slices this launch handles: false = tuples from the caller's key/value arrays,
 // true = S survivors of a level-1 Bloom probe, packed in cmp. One instantiation per input form keeps
 // each kernel within the 64 registers that two CTAs per SM allow.
-template <bool kPacked>
+template <bool kPacked, int M>
 __global__ void __launch_bounds__(kThreads, 2)
 k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
              const int64_t* __restrict__ scan, unsigned long long* gwords, int max_bins) {
@@ -523,7 +536,7 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const int s = (int)(g - slice_prefix[j]);
         const int64_t b = (int64_t)s * R.slice_len;
         const bool bloom = (rel == 1) && d.bloom != nullptr && d.bloom_level == 1;
-        if (bloom != kPacked) continue;  // the other instantiation's slice (block-uniform)
+        if (bloom != kPacked || d.pf.mode != M) continue;  // another instantiation's slice (block-uniform)
         const int64_t e = bloom ? b + R.slice_cnt[s] : min(b + R.slice_len, R.n);
         const uint32_t P1 = d.pf.P1;
         const int64_t* S = scan + R.hist_base;
@@ -531,7 +544,7 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         for (uint32_t p = threadIdx.x; p < P1; p += kThreads)
             cursor[p] = S[(int64_t)p * R.nslices + s] - s0;
         __syncthreads();
-        const Bin1 bin{d.pf};
+        const Bin1<M> bin{d.pf};
         if constexpr (kPacked) {
             scatter_tiles(PackedTiles{R.cmp}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf,
                           bars, ph, &gwords[kGErrors]);
@@ -613,7 +626,7 @@ __global__ void k_l2_plan(const JoinDesc* __restrict__ J, int nj, int rel, const
 // every key and compacts the survivors into cmp[slice begin, + survivors).
 // kBloom selects the slices this launch handles (S slices of joins probing their filter at level 2,
 // or all others); one instantiation per form keeps each within 64 registers.
-template <bool kBloom>
+template <bool kBloom, int M, int K>
 __global__ void __launch_bounds__(kThreads, 2)
 k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
           const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
@@ -629,9 +642,10 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         const uint32_t P2 = d.pf.P2;
         const int64_t begin = R.b1[x.p] + x.sl * kL2Slice;
         const int64_t end = min_i64(R.b1[x.p + 1], begin + kL2Slice);
-        const Bin2 bin{d.pf};
+        const Bin2<M> bin{d.pf};
         const bool bloom = rel == 1 && d.bloom != nullptr && d.bloom_level == 2;
-        if (bloom != kBloom) continue;  // the other instantiation's slice (block-uniform)
+        if (bloom != kBloom || d.pf.mode != M || (kBloom && bloom_kclass(d) != K))
+            continue;  // another instantiation's slice (block-uniform)
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cnt[q] = 0;
         if (threadIdx.x == 0) s_surv = 0;
         __syncthreads();
@@ -655,41 +669,58 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t* __restrict__ bloom = d.bloom;
             uint2* __restrict__ cmp = R.cmp;
             const uint32_t fbase = x.p * P2;
-            for (int64_t i0 = begin; i0 < end; i0 += kL2ProbeILP * kThreads) {
-                // only the tuples and their filter blocks are held per key (the hashes are cheap
-                // to recompute, registers are not)
+            const int32_t len = (int32_t)(end - begin);  // at most kL2Slice
+            const uint2* __restrict__ src = l1 + begin;
+            for (int32_t r0 = 0; r0 < len; r0 += kL2ProbeILP * kThreads) {
                 uint2 e[kL2ProbeILP];
-                uint4 w0[kL2ProbeILP], w1[kL2ProbeILP];
+                uint32_t va[kL2ProbeILP], vb[kL2ProbeILP];
 #pragma unroll
                 for (int u = 0; u < kL2ProbeILP; ++u) {
-                    const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    e[u] = i < end ? __ldcs(&l1[i]) : make_uint2(0u, 0u);
+                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+                    e[u] = r < len ? __ldcs(src + r) : make_uint2(0u, 0u);
                 }
 #pragma unroll
                 for (int u = 0; u < kL2ProbeILP; ++u) {
-                    const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    if (i < end) {
-                        const uint4* blk = bloom_block(bloom, seg_blocks, fbase + bin(e[u].x), bloom_hash(e[u].x));
-                        w0[u] = __ldg(blk);
-                        w1[u] = __ldg(blk + 1);
+                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+                    if (r < len) {
+                        BloomKey bkey;
+                        bloom_key<K>(e[u].x, seg_blocks, bk, bkey);
+                        const uint32_t* w = bloom_words(bloom, seg_blocks, fbase + bin(e[u].x), bkey.block);
+                        va[u] = __ldg(w + bkey.wa);
+                        vb[u] = __ldg(w + bkey.wb);
                     }
                 }
+                uint32_t pm = 0;  // bit u: tuple u passed the filter
 #pragma unroll
                 for (int u = 0; u < kL2ProbeILP; ++u) {
-                    const int64_t i = i0 + u * kThreads + threadIdx.x;
-                    const bool pass =
-                        i < end && bloom_pass(bloom_hash(e[u].x), e[u].x, seg_blocks, bk, w0[u], w1[u]);
-                    const uint32_t m = __ballot_sync(0xffffffffu, pass);
-                    if (m) {
-                        uint32_t base = 0;
-                        if (lane == 0) base = atomicAdd(&s_surv, (uint32_t)__popc(m));
-                        base = __shfl_sync(0xffffffffu, base, 0);
-                        if (pass) {
+                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+                    if (r < len) {
+                        uint32_t ma, mb;
+                        bloom_masks<K>(bloom_hash(e[u].x), bk, ma, mb);
+                        if ((va[u] & ma) == ma && (vb[u] & mb) == mb) pm |= 1u << u;
+                    }
+                }
+                // survivors: one shared-memory atomic per warp for the whole group
+                uint32_t bal[kL2ProbeILP];
+                uint32_t tot = 0;
+#pragma unroll
+                for (int u = 0; u < kL2ProbeILP; ++u) {
+                    bal[u] = __ballot_sync(0xffffffffu, (pm >> u) & 1u);
+                    tot += __popc(bal[u]);
+                }
+                if (tot) {
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd(&s_surv, tot);
+                    base = __shfl_sync(0xffffffffu, base, 0);
+#pragma unroll
+                    for (int u = 0; u < kL2ProbeILP; ++u) {
+                        if ((pm >> u) & 1u) {
                             atomicAdd(&cnt[bin(e[u].x)], 1u);
-                            const int64_t dst = begin + base + __popc(m & lanemask_lt());
+                            const int64_t dst = begin + base + __popc(bal[u] & lanemask_lt());
                             if (dst < end) cmp[dst] = e[u];
                             else atomicAdd(&gwords[kGErrors], 1ull);
                         }
+                        base += __popc(bal[u]);
                     }
                 }
             }
@@ -706,6 +737,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 }
 
 // Level-2 scatter of one slice into its private runs of the level-2 buffer.
+template <int M>
 __global__ void __launch_bounds__(kThreads, 2)
 k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
              const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
@@ -725,6 +757,7 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
     for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
         const L2Slice x = l2_decode(seg_prefix, nj, seg_off, seg_ns, total_segs, t);
         const JoinDesc& d = J[x.j];
+        if (d.pf.mode != M) continue;  // the other instantiation's join (block-uniform)
         const RelPlan& R = d.rel[rel];
         const uint32_t P2 = d.pf.P2;
         const int64_t begin = R.b1[x.p] + x.sl * kL2Slice;
@@ -735,7 +768,7 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const int64_t* Sx = S2 + x.local_off * P2;
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
         __syncthreads();
-        scatter_tiles(PackedTiles{bloom ? R.cmp : R.l1}, begin, end, Bin2{d.pf}, (int)P2, R.l2,
+        scatter_tiles(PackedTiles{bloom ? R.cmp : R.l1}, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2,
                       R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph, &gwords[kGErrors]);
     }
 }
@@ -765,18 +798,12 @@ __global__ void k_l2_bounds(const JoinDesc* __restrict__ J, int nj, int rel, con
     }
 }
 
-// The low 40 bits of g rotated right by s (0 <= s < 40).
-__device__ __forceinline__ uint64_t rot40(uint64_t g, uint32_t s) {
-    constexpr uint64_t kM = (1ull << 40) - 1;
-    const uint64_t x = g & kM;
-    return s ? (((x >> s) | (x << (40 - s))) & kM) : x;
-}
-
 // Bloom build: one CTA per group of G consecutive finest partitions of a Bloom-enabled join
 // (G = JoinDesc::bloom_group, chosen so the group's segments fit in shared memory). The group's R
-// tuples are contiguous in the final R buffer; every key sets its bits with 32-bit atomicOr in the
-// shared-memory copy of its segment, and the segments are written out whole, so the filter needs
+// tuples are contiguous in the final R buffer; every key sets its bits in its two words with two
+// 32-bit atomicOr in the shared-memory copy of its segment, and the segments are written out whole, so the filter needs
 // no clearing. A segment too large for shared memory (G = 1 then) is built with global atomicOr.
+template <int M, int K>
 __global__ void __launch_bounds__(kThreads)
 k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ bloom_prefix,
               int smem_words, unsigned long long* gwords) {
@@ -785,6 +812,7 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(bloom_prefix, nj, g);
         const JoinDesc& d = J[j];
+        if (d.pf.mode != M || bloom_kclass(d) != K) continue;  // another instantiation's join (block-uniform)
         const RelPlan& R = d.rel[0];
         const int64_t nfine = (int64_t)d.pf.P1 * d.pf.P2;
         const int64_t f0 = (g - bloom_prefix[j]) * d.bloom_group;
@@ -799,7 +827,6 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
         const int k = d.bloom_k;
         const PartFn pf = d.pf;
         const uint32_t seg_blocks = d.seg_blocks;
-        const uint32_t l8 = threadIdx.x & 7u, rs = 5u * l8;
         const bool in_smem = words <= smem_words;
         uint32_t* dst = in_smem ? seg : gseg;
         for (int64_t w = threadIdx.x; w < words; w += kThreads) dst[w] = 0;
@@ -815,34 +842,16 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
             for (int u = 0; u < kProbeILP; ++u) {
                 const int64_t i = i0 + u * kThreads + threadIdx.x;
                 if (i >= end) continue;
-                const int64_t local = (int64_t)part_fine(pf, kk[u]) - f0;
+                const int64_t local = (int64_t)part_fine_m<M>(pf, kk[u]) - f0;
                 if (local < 0 || local >= f1 - f0) {
                     atomicAdd(&gwords[kGErrors], 1ull);
                     continue;
                 }
-                const uint64_t g = bloom_hash(kk[u]);
-                uint32_t* blk = dst + local * nw + (int64_t)bloom_block_of(g, seg_blocks) * 8;
-                // Lane l starts at word l % 8 of its block, so the lanes of one atomic instruction
-                // touch different words and mostly different shared-memory banks (all lanes on
-                // the same word would be an 8-way bank conflict, since blocks are 8 words). For
-                // k <= 8 the 40 bits of word positions are rotated once by 5 * (l % 8) bits so
-                // that step t reads its position with a constant shift.
-                if (k <= 8) {
-                    const uint64_t r = rot40(g, rs);
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const uint32_t w = ((uint32_t)t + l8) & 7u;
-                        if (w < (uint32_t)k) atomicOr(blk + w, 1u << ((uint32_t)(r >> (5 * t)) & 31u));
-                    }
-                } else {
-                    const uint64_t g2 = mix64(g);
-#pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const int w = (int)(((uint32_t)t + l8) & 7u);
-                        const uint32_t m = bloom_word_mask(g, g2, k, w);
-                        if (m) atomicOr(blk + w, m);
-                    }
-                }
+                BloomKey bkey;
+                bloom_key<K>(kk[u], seg_blocks, k, bkey);
+                uint32_t* blk = dst + local * nw + (int64_t)bkey.block * 8;
+                atomicOr(blk + bkey.wa, bkey.ma);
+                if (bkey.mb) atomicOr(blk + bkey.wb, bkey.mb);
             }
         }
         __syncthreads();
@@ -1354,6 +1363,23 @@ static cudaError_t set_smem_attr(const void* fn, size_t bytes) {
     return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
+// Calls f(std::integral_constant<int, M>, std::integral_constant<int, K>) for every partition mode
+// M and Bloom k class K present in the batch.
+template <class F>
+static void for_mode_k(int modes, int kclasses, F&& f) {
+    if ((modes & 1) && (kclasses & 1)) f(std::integral_constant<int, 0>{}, std::integral_constant<int, 0>{});
+    if ((modes & 1) && (kclasses & 2)) f(std::integral_constant<int, 0>{}, std::integral_constant<int, kBloomFastK>{});
+    if ((modes & 2) && (kclasses & 1)) f(std::integral_constant<int, 1>{}, std::integral_constant<int, 0>{});
+    if ((modes & 2) && (kclasses & 2)) f(std::integral_constant<int, 1>{}, std::integral_constant<int, kBloomFastK>{});
+}
+
+// Calls f(std::integral_constant<int, M>) for every partition mode M present in the batch.
+template <class F>
+static void for_modes(int modes, F&& f) {
+    if (modes & 1) f(std::integral_constant<int, 0>{});
+    if (modes & 2) f(std::integral_constant<int, 1>{});
+}
+
 static int grid_for(int64_t work, int num_sms, int per_sm) {
     int64_t g = std::min<int64_t>(work, (int64_t)num_sms * per_sm);
     return (int)std::max<int64_t>(g, 1);
@@ -1363,10 +1389,17 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     static thread_local bool attrs_done = false;
     cudaError_t err;
     if (!attrs_done) {
-        if ((err = set_smem_attr((const void*)k_l1_scatter<false>, scatter_smem(kMaxP1))) != cudaSuccess) return err;
-        if ((err = set_smem_attr((const void*)k_l1_scatter<true>, scatter_smem(kMaxP1))) != cudaSuccess) return err;
-        if ((err = set_smem_attr((const void*)k_l2_scatter, scatter_smem(kMaxP2))) != cudaSuccess) return err;
-        if ((err = set_smem_attr((const void*)k_bloom_build, kBloomSmemWords * 4)) != cudaSuccess) return err;
+        const void* l1s[] = {(const void*)k_l1_scatter<false, 0>, (const void*)k_l1_scatter<false, 1>,
+                             (const void*)k_l1_scatter<true, 0>, (const void*)k_l1_scatter<true, 1>};
+        for (const void* f : l1s)
+            if ((err = set_smem_attr(f, scatter_smem(kMaxP1))) != cudaSuccess) return err;
+        const void* l2s[] = {(const void*)k_l2_scatter<0>, (const void*)k_l2_scatter<1>};
+        for (const void* f : l2s)
+            if ((err = set_smem_attr(f, scatter_smem(kMaxP2))) != cudaSuccess) return err;
+        const void* bbs[] = {(const void*)k_bloom_build<0, 0>, (const void*)k_bloom_build<1, 0>,
+                             (const void*)k_bloom_build<0, kBloomFastK>, (const void*)k_bloom_build<1, kBloomFastK>};
+        for (const void* f : bbs)
+            if ((err = set_smem_attr(f, kBloomSmemWords * 4)) != cudaSuccess) return err;
         if ((err = set_smem_attr((const void*)k_probe, probe_smem_bytes(kMaxTable, 1))) != cudaSuccess)
             return err;
         attrs_done = true;
@@ -1386,10 +1419,13 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
         const bool part = (a.stages & (rel == 0 ? kRunPartR : kRunPartS)) != 0;
         if (rel == 1 && (a.stages & kRunBloom) && a.any_bloom && a.total_bloom_groups > 0) {
             // Bloom filter over the final R partitions, before S's first pass probes it.
-            k_bloom_build<<<grid_for(a.total_bloom_groups, sms, 4), kThreads,
-                            (size_t)a.bloom_smem_words * 4, st>>>(a.J, a.nj, a.bloom_prefix,
-                                                                  a.bloom_smem_words, a.gwords);
-            ++launches;
+            for_mode_k(a.modes, a.kclasses, [&](auto mt, auto kt) {
+                constexpr int M = decltype(mt)::value, K = decltype(kt)::value;
+                k_bloom_build<M, K><<<grid_for(a.total_bloom_groups, sms, 4), kThreads,
+                                   (size_t)a.bloom_smem_words * 4, st>>>(a.J, a.nj, a.bloom_prefix,
+                                                                         a.bloom_smem_words, a.gwords);
+                ++launches;
+            });
         }
         if (rel == 1) mark(5);
         const int m0 = rel == 0 ? 1 : 6;  // first stage mark of this relation
@@ -1398,9 +1434,12 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             continue;
         }
         if (a.total_slices[rel] > 0) {
-            k_l1_hist<<<grid_for(a.total_slices[rel], sms, 4), kThreads, (size_t)a.max_p1 * 4, st>>>(
-                a.J, a.nj, rel, a.slice_prefix[rel], a.hist, a.gwords);
-            ++launches;
+            for_mode_k(a.modes, a.kclasses, [&](auto mt, auto kt) {
+                constexpr int M = decltype(mt)::value, K = decltype(kt)::value;
+                k_l1_hist<M, K><<<grid_for(a.total_slices[rel], sms, 4), kThreads, (size_t)a.max_p1 * 4, st>>>(
+                    a.J, a.nj, rel, a.slice_prefix[rel], a.hist, a.gwords);
+                ++launches;
+            });
         }
         mark(m0);
         if ((err = enqueue_scan(a.hist + a.hist_begin[rel], a.hist_scan + a.hist_begin[rel],
@@ -1408,14 +1447,18 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             return err;
         mark(m0 + 1);
         if (a.total_slices[rel] > 0) {
-            k_l1_scatter<false><<<grid_for(a.total_slices[rel], sms, 2), kThreads, scatter_smem(a.max_p1), st>>>(
-                a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
-            ++launches;
-            if (rel == 1 && a.any_bloom_l1) {
-                k_l1_scatter<true><<<grid_for(a.total_slices[rel], sms, 2), kThreads, scatter_smem(a.max_p1), st>>>(
+            for_modes(a.modes, [&](auto mt) {
+                constexpr int M = decltype(mt)::value;
+                const dim3 grid(grid_for(a.total_slices[rel], sms, 2));
+                k_l1_scatter<false, M><<<grid, kThreads, scatter_smem(a.max_p1), st>>>(
                     a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
                 ++launches;
-            }
+                if (rel == 1 && a.any_bloom_l1) {
+                    k_l1_scatter<true, M><<<grid, kThreads, scatter_smem(a.max_p1), st>>>(
+                        a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
+                    ++launches;
+                }
+            });
         }
         mark(m0 + 2);
         {
@@ -1432,24 +1475,37 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 return err;
             uint32_t* h2 = a.hist2 + a.h2_begin[rel];
             if ((err = cudaMemsetAsync(h2, 0, (size_t)a.h2_len[rel] * 4, st)) != cudaSuccess) return err;
-            k_l2_hist<false><<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4, st>>>(
-                a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2, a.gwords);
-            if (rel == 1 && a.any_bloom_l2) {
-                k_l2_hist<true><<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4, st>>>(
-                a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2, a.gwords);
+            for_modes(a.modes, [&](auto mt) {
+                constexpr int M = decltype(mt)::value;
+                const dim3 grid(grid_for(a.l2_slice_cap[rel], sms, 4));
+                k_l2_hist<false, M, 0><<<grid, kThreads, (size_t)a.max_p2 * 4, st>>>(
+                    a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2,
+                    a.gwords);
                 ++launches;
+            });
+            if (rel == 1 && a.any_bloom_l2) {
+                for_mode_k(a.modes, a.kclasses, [&](auto mt, auto kt) {
+                    constexpr int M = decltype(mt)::value, K = decltype(kt)::value;
+                    k_l2_hist<true, M, K><<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4,
+                                            st>>>(a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs,
+                                                  a.hist2, a.slice_cnt2, a.gwords);
+                    ++launches;
+                });
             }
-            ++launches;
             if ((err = enqueue_scan(h2, a.hist2_scan + a.h2_begin[rel], a.h2_len[rel], a.scan_tmp, nullptr, st)) !=
                 cudaSuccess)
                 return err;
-            k_l2_scatter<<<grid_for(a.l2_slice_cap[rel], sms, 2), kThreads, scatter_smem(a.max_p2), st>>>(
-                a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2_scan, a.slice_cnt2, a.gwords,
-                a.max_p2);
+            for_modes(a.modes, [&](auto mt) {
+                constexpr int M = decltype(mt)::value;
+                k_l2_scatter<M><<<grid_for(a.l2_slice_cap[rel], sms, 2), kThreads, scatter_smem(a.max_p2), st>>>(
+                    a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2_scan, a.slice_cnt2,
+                    a.gwords, a.max_p2);
+                ++launches;
+            });
             dim3 grid((unsigned)std::min<int64_t>(((int64_t)a.max_p1 * a.max_p2 + 1 + 255) / 256, 4096),
                       (unsigned)std::min(a.nj, 65535));
             k_l2_bounds<<<grid, 256, 0, st>>>(a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.hist2_scan);
-            launches += 2;
+            ++launches;
         }
         mark(m0 + 3);
     }

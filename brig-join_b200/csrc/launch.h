@@ -40,6 +40,8 @@ struct PipelineArgs {
     int any_bloom;
     int any_bloom_l1;                 // some join probes its filter in S's first pass
     int any_bloom_l2;                 // some join probes its filter in S's second pass
+    int modes;                        // partition modes present: bit 0 hash, bit 1 modulo
+    int kclasses;                     // Bloom k classes present: bit 0 any k (or no filter), bit 1 k = 7
     int num_sms;
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
     int stages;                       // kRunPartR | kRunBloom | kRunPartS | kRunProbe
