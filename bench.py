@@ -180,18 +180,26 @@ def whole_job_value(world: int, steps: int, nr: int, ns: int, ms_total: float) -
 
 
 # ---- per-stage algorithmic bytes ------------------------------------------------------------------
-def stage_bytes(nr, ns, surv, matches, bloom_bits):
-    """Minimum bytes each stage must move (read inputs once, write outputs once)."""
+def stage_bytes(nr, ns, surv, matches, bloom_bits, bloom_level):
+    """Minimum bytes each stage must move in this layout: inputs read once, outputs written once.
+
+    Partitioned buffers hold packed 8-byte (key, value) tuples, so a pass that only needs the keys
+    still reads 8 bytes per tuple. bloom_level is the S pass that probes the filter (0: no filter).
+    Level-1 probes read one random 32-byte sector per S tuple from HBM; level-2 probes read the
+    filter from L2 (a partition's segments), which is not HBM traffic."""
+    s_l1 = bloom_level == 1
     return {
         "r_hist": 4 * nr,
         "r_scan": 0,
         "r_scatter": 16 * nr,
-        "r_level2": 16 * nr,
-        "bloom_build": 4 * nr + bloom_bits // 8,
-        "s_hist_probe": 4 * ns + 32 * ns + 12 * surv,
+        "r_l2_hist": 8 * nr,
+        "r_l2_scatter": 16 * nr,
+        "bloom_build": 8 * nr + bloom_bits // 8,
+        "s_hist_probe": (4 * ns + 32 * ns + 12 * surv) if s_l1 else 4 * ns,
         "s_scan": 0,
-        "s_scatter": 16 * surv,
-        "s_level2": 16 * surv,
+        "s_scatter": 16 * (surv if s_l1 else ns),
+        "s_l2_hist": 8 * surv if s_l1 else (8 * ns + 8 * surv if bloom_level == 2 else 8 * ns),
+        "s_l2_scatter": 16 * surv,
         "tasks": 0,
         "probe": 8 * nr + 8 * surv + 8 * matches,
     }
@@ -469,7 +477,11 @@ def main():
 
     peak, peak_kind = peaks()
     avg = stages
-    sb = stage_bytes(nr, ns, st.s_survivors, st.count, st.bloom_num_bits)
+    blvl = 0
+    if wl["bloom"]:
+        blvl = args.bloom_level or (1 if st.bloom_num_bits // 8 <= (64 << 20) or st.second_partition_size <= 1
+                                    else 2)
+    sb = stage_bytes(nr, ns, st.s_survivors, st.count, st.bloom_num_bits, blvl)
     dom = max(avg, key=avg.get)
     achieved = sb[dom] / (avg[dom] / 1e3) / 1e9
     join_bytes = 8 * (nr + ns) + 8 * st.count

@@ -42,7 +42,7 @@ STATUS_NAMES = {
 PART_HASH = 0
 PART_MODULO = 1
 ABI_VERSION = 1
-NUM_STAGES = 11
+NUM_STAGES = 13
 NOALLOC_MAX_TUPLES = 262144
 
 _u32p = C.POINTER(C.c_uint32)

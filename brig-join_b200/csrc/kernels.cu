@@ -1327,8 +1327,9 @@ void set_capturing(bool on) {
 int64_t take_capture_tally() { return g_capture_tally; }
 
 const char* stage_name(int i) {
-    static const char* names[kNumStages] = {"r_hist", "r_scan", "r_scatter", "r_level2", "bloom_build",
-                                            "s_hist_probe", "s_scan", "s_scatter", "s_level2", "tasks",
+    static const char* names[kNumStages] = {"r_hist", "r_scan", "r_scatter", "r_l2_hist", "r_l2_scatter",
+                                            "bloom_build", "s_hist_probe", "s_scan", "s_scatter", "s_l2_hist",
+                                            "s_l2_scatter", "tasks",
                                             "probe"};
     return (i >= 0 && i < kNumStages) ? names[i] : nullptr;
 }
@@ -1427,10 +1428,10 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 ++launches;
             });
         }
-        if (rel == 1) mark(5);
-        const int m0 = rel == 0 ? 1 : 6;  // first stage mark of this relation
+        if (rel == 1) mark(6);
+        const int m0 = rel == 0 ? 1 : 7;  // first stage mark of this relation
         if (!part) {
-            for (int m = m0; m < m0 + 4; ++m) mark(m);
+            for (int m = m0; m < m0 + 5; ++m) mark(m);
             continue;
         }
         if (a.total_slices[rel] > 0) {
@@ -1492,6 +1493,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                     ++launches;
                 });
             }
+            mark(m0 + 3);
             if ((err = enqueue_scan(h2, a.hist2_scan + a.h2_begin[rel], a.h2_len[rel], a.scan_tmp, nullptr, st)) !=
                 cudaSuccess)
                 return err;
@@ -1506,13 +1508,15 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                       (unsigned)std::min(a.nj, 65535));
             k_l2_bounds<<<grid, 256, 0, st>>>(a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.hist2_scan);
             ++launches;
+        } else {
+            mark(m0 + 3);
         }
-        mark(m0 + 3);
+        mark(m0 + 4);
     }
     // ---- tasks --------------------------------------------------------------------------------
     if (!(a.stages & kRunProbe)) {
-        mark(10);
-        mark(11);
+        mark(12);
+        mark(13);
         note_launches(launches);
         return cudaGetLastError();
     }
@@ -1528,7 +1532,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                                                           a.gwords);
         ++launches;
     }
-    mark(10);
+    mark(12);
     // ---- probe --------------------------------------------------------------------------------
     {
         const size_t smem = probe_smem_bytes(a.table_cap, a.emit_key);
@@ -1538,7 +1542,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             return err;
         occ = std::max(occ, 1);
         k_probe<<<sms * occ, kThreads, smem, st>>>(a.J, a.tasks, a.gwords, a.table_cap, a.emit_key);
-        mark(11);
+        mark(13);
         k_publish_counts<<<1, 256, 0, st>>>(a.J, a.nj);
         launches += 2;
     }

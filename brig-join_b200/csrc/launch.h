@@ -58,7 +58,7 @@ struct PipelineArgs {
 // Pipeline parts (a full join runs all four; the reference-named entry points run subsets).
 enum RunPart : int { kRunPartR = 1, kRunBloom = 2, kRunPartS = 4, kRunProbe = 8, kRunAll = 15 };
 
-constexpr int kNumStages = 11;
+constexpr int kNumStages = 13;
 constexpr int kBloomSmemWords = 12288;  // 48 KB of Bloom segments per build CTA
 const char* stage_name(int i);
 

@@ -156,9 +156,9 @@ int brig_join_run_host(brig_join_t* h,
 int brig_join_get_stats(brig_join_t* h, brig_join_stats* st);
 
 /* Pipeline stages timed when profile_stages is set, in execution order. */
-#define BRIG_NUM_STAGES 11
-/* Name of stage i ("r_hist", "r_scan", "r_scatter", "r_level2", "bloom_build", "s_hist_probe",
- * "s_scan", "s_scatter", "s_level2", "tasks", "probe"), or NULL. */
+#define BRIG_NUM_STAGES 13
+/* Name of stage i ("r_hist", "r_scan", "r_scatter", "r_l2_hist", "r_l2_scatter", "bloom_build",
+ * "s_hist_probe", "s_scan", "s_scatter", "s_l2_hist", "s_l2_scatter", "tasks", "probe"), or NULL. */
 const char* brig_join_stage_name(int32_t i);
 /* Waits for the last run and writes the mean device time of each stage in milliseconds, over
  * the runs since the previous call (at most the last 64), into ms[BRIG_NUM_STAGES] (the

@@ -77,8 +77,9 @@ def test_null_arguments_rejected(bj):
     assert bj.lib().brig_join_get_stats(None, None) == bj.BRIG_E_INVALID
     assert bj.lib().brig_join_destroy(None) == bj.BRIG_OK
     assert bj.lib().brig_join_stage_name(0) == b"r_hist"
-    assert bj.lib().brig_join_stage_name(10) == b"probe"
-    assert bj.lib().brig_join_stage_name(11) is None
+    assert bj.lib().brig_join_stage_name(3) == b"r_l2_hist"
+    assert bj.lib().brig_join_stage_name(12) == b"probe"
+    assert bj.lib().brig_join_stage_name(13) is None
 
 
 def test_generator_properties(bj):
