@@ -298,18 +298,20 @@ Engine::~Engine() {
     if (done_) cudaEventDestroy(done_);
 }
 
-void Engine::ensure_workspace(size_t bytes) {
+// Growing the workspace is stream-ordered (cudaFreeAsync / cudaMallocAsync on the run's stream,
+// after the handle's previous run), so it never synchronises the device: other handles' work on
+// other streams, e.g. the other slots of a server, keeps running.
+void Engine::ensure_workspace(size_t bytes, cudaStream_t stream) {
     if (bytes <= ws_bytes_) return;
-    if (have_run_) cuda_check(cudaEventSynchronize(done_), "cudaEventSynchronize");
     if (graph_exec_) {
         cudaGraphExecDestroy(graph_exec_);
         graph_exec_ = nullptr;
         graph_key_.clear();
     }
-    if (ws_) cudaFree(ws_);
+    if (ws_) cuda_check(cudaFreeAsync(ws_, stream), "workspace cudaFreeAsync");
     ws_ = nullptr;
     ws_bytes_ = 0;
-    cuda_check(cudaMalloc(&ws_, bytes), "workspace cudaMalloc");
+    cuda_check(cudaMallocAsync(&ws_, bytes, stream), "workspace cudaMallocAsync");
     ws_bytes_ = bytes;
 }
 
@@ -496,7 +498,10 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
     std::vector<JoinOffs> jo(nj);
     Shape sh;
     layout_for(cfg_, plans.data(), nj, num_sms_, jo.data(), sh);
-    ensure_workspace(sh.total);
+    // A handle's runs are ordered even across streams: this run's work (and a workspace growth)
+    // starts after the previous run's last operation.
+    if (have_run_) cuda_check(cudaStreamWaitEvent(stream, done_, 0), "cudaStreamWaitEvent");
+    ensure_workspace(sh.total, stream);
     ensure_staging(sh.meta_bytes);
     // The staging buffer may still be read by the previous run's copy.
     if (have_run_) cuda_check(cudaEventSynchronize(stage_free_), "cudaEventSynchronize");

@@ -122,7 +122,7 @@ public:
     void ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key);
 
 private:
-    void ensure_workspace(size_t bytes);
+    void ensure_workspace(size_t bytes, cudaStream_t stream);
     void ensure_staging(size_t bytes);
 
     brig_join_config cfg_;
