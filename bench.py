@@ -205,6 +205,28 @@ def stage_bytes(nr, ns, surv, matches, bloom_bits, bloom_level):
     }
 
 
+# DRAM bytes (read + write) per tuple of each stage's main kernel, from one ncu capture of the same
+# kernels on 2^26 x 2^26 (inputs 4x the L2, level-1 fan-out 512 as at 640M; level-2 fan-out 64) in the
+# profiles directory: (bytes per tuple, which count the stage's launch processes). Used to scale the
+# measured traffic to the benchmarked launch; the per-tuple traffic of these streaming kernels does
+# not depend on the relation size once the inputs exceed the L2.
+NCU_TRAFFIC_PER_TUPLE = {
+    "r_hist": (4.06, "nr"), "r_scatter": (18.2, "nr"), "r_l2_hist": (8.05, "nr"), "r_l2_scatter": (15.4, "nr"),
+    "bloom_build": (8.44, "nr"), "s_hist_probe": (4.06, "ns"), "s_scatter": (18.2, "ns"),
+    "s_l2_hist": (10.5, "ns"), "probe": (10.0, "nr"),
+}
+
+
+def stage_traffic(stage, nr, ns, bloom_level):
+    """ncu-measured DRAM bytes of the stage's main kernel scaled to this launch, or None."""
+    if stage not in NCU_TRAFFIC_PER_TUPLE:
+        return None
+    if stage in ("s_hist_probe", "s_scatter") and bloom_level == 1:
+        return None  # captured with the filter probed in the second pass
+    per, unit = NCU_TRAFFIC_PER_TUPLE[stage]
+    return per * (nr if unit == "nr" else ns)
+
+
 # ---- batched uneven joins -------------------------------------------------------------------------
 def batch_shapes(n_joins, seed, lo=4096, hi=1 << 24):
     """|R_j| log-uniform in [lo, hi], |S_j| = 4 |R_j| (the 256-join uneven batch)."""
@@ -315,7 +337,10 @@ def run_serve_workload(args):
 
     def serve(rate, streams, max_wave):
         lat, queue, results = [], [], []
-        outs = {i: (np.empty(pool[i][3] + 16, np.uint32), np.empty(pool[i][3] + 16, np.uint32)) for i in set(seq)}
+        # pinned host outputs: the pairs come back by asynchronous copies, as a client that hands
+        # the server page-locked buffers would receive them
+        outs = {i: tuple(torch.empty(pool[i][3] + 16, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+                         for _ in range(2)) for i in set(seq)}
         gaps = np.random.default_rng(3).exponential(1.0 / rate, len(seq)) if rate > 0 else np.zeros(len(seq))
         with bj.Server(hbm_budget_bytes=120 * 10**9, max_wave=max_wave, streams=streams) as srv:
             tickets = []
@@ -537,7 +562,10 @@ def main():
                              + (", far above the 126 MB L2" if 8 * (nr + ns) > 4 * 126e6 else ""),
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind},
+                         "frac": achieved / peak, "traffic": stage_traffic(dom, nr, ns, blvl),
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per tuple on "
+                                           "2^26 x 2^26, scaled to this launch",
+                         "peak_kind": peak_kind},
             "join_roofline": {"algorithmic_bytes": join_bytes, "achieved": join_gbs, "peak": peak,
                               "frac": join_gbs / peak, "unit": "GB/s"},
             "stage_ms": {k: round(v, 4) for k, v in avg.items()},

@@ -27,7 +27,9 @@ constexpr int kDefaultChunk = 65536;  // default streamed tuples per probe task
 constexpr int kMinTable = 256;
 constexpr int kMaxBloomK = 16;
 constexpr int kThreads = 512;         // threads per CTA of every partition and probe kernel
-constexpr int kTile = 4096;           // tuples per scatter tile staged in shared memory
+constexpr int kTile = 4096;           // unit of the level-2 slice length
+constexpr int kSThreads = 1024;       // threads per CTA of the scatter kernels (one CTA per SM)
+constexpr int kSTile = 8192;          // tuples per scatter tile staged in shared memory
 constexpr int kWarpBuf = 128;         // output pairs staged per warp before a global flush
 constexpr int64_t kL2Slice = 32 * kTile;  // tuples per level-2 slice (131072)
 

@@ -135,11 +135,11 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
     for (int j = 0; j < nj; ++j) jo[j] = JoinOffs{};
     int64_t total_tuples = 0;
     for (int j = 0; j < nj; ++j) total_tuples += plans[j].nr + plans[j].ns;
-    // Slices of about total/(8 * SMs) tuples, a multiple of the scatter tile, at least 4 tiles.
+    // Slices of about total/(8 * SMs) tuples, a multiple of the scatter tile, at least 2 tiles.
     const int64_t target = (int64_t)num_sms * 8;
     int64_t sl = (total_tuples + target - 1) / std::max<int64_t>(target, 1);
-    sl = ((sl + kTile - 1) / kTile) * kTile;
-    sl = std::max<int64_t>(sl, 4 * kTile);
+    sl = ((sl + kSTile - 1) / kSTile) * kSTile;
+    sl = std::max<int64_t>(sl, 2 * kSTile);
     sh.slice_len = sl;
     const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
     const int C = cfg.s_chunk > 0 ? cfg.s_chunk : kDefaultChunk;

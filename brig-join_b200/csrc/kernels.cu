@@ -61,11 +61,12 @@ __device__ __forceinline__ int find_owner(const int64_t* __restrict__ prefix, in
 }
 
 // Block-wide exclusive scan of n uint32 values in shared memory, in place. Returns the total.
-// blockDim.x must be kThreads; tmp holds kThreads/32 words.
-__device__ uint32_t block_scan_excl(uint32_t* a, int n, uint32_t* tmp) {
+// blockDim.x must be NT; tmp holds NT/32 words.
+template <int NT>
+__device__ uint32_t block_scan_excl_n(uint32_t* a, int n, uint32_t* tmp) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    constexpr int kWarps = kThreads / 32;
-    const int per = (n + kThreads - 1) / kThreads;
+    constexpr int kWarps = NT / 32;
+    const int per = (n + NT - 1) / NT;
     const int beg = min(n, (int)threadIdx.x * per);
     const int end = min(n, beg + per);
     uint32_t sum = 0;
@@ -97,6 +98,9 @@ __device__ uint32_t block_scan_excl(uint32_t* a, int n, uint32_t* tmp) {
     }
     __syncthreads();
     return total;
+}
+__device__ __forceinline__ uint32_t block_scan_excl(uint32_t* a, int n, uint32_t* tmp) {
+    return block_scan_excl_n<kThreads>(a, n, tmp);
 }
 
 // Same for int64 values (one value per thread), returns the exclusive prefix of this thread.
@@ -189,7 +193,7 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, unsign
 // (tn mod 4) tuples of a tile, or every tuple of unaligned arrays, are read with ordinary loads, so
 // nothing outside the caller's arrays is read. issue() is called by one thread and arms `bar`
 // (with no bytes when nothing is copied); item() reads tuple i of the tile.
-constexpr size_t kTileBuf = (size_t)(kTile + 2) * 8;  // one input buffer
+constexpr size_t kTileBuf = (size_t)(kSTile + 2) * 8;  // one scatter input buffer
 
 struct PackedTiles {
     const uint2* p;
@@ -223,7 +227,7 @@ struct KvTiles {
             const uint32_t bytes = (uint32_t)(tn & ~3) * 4u;
             mbar_arrive_tx(bar, 2 * bytes);
             bulk_g2s(buf, k + t0, bytes, bar);
-            bulk_g2s(buf + (size_t)kTile * 4, v + t0, bytes, bar);
+            bulk_g2s(buf + (size_t)kSTile * 4, v + t0, bytes, bar);
         } else {
             mbar_arrive(bar);
         }
@@ -231,7 +235,7 @@ struct KvTiles {
     __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t t0, int i, int tn, uint32_t) const {
         if (bulk && i < (tn & ~3))
             return make_uint2(reinterpret_cast<const uint32_t*>(buf)[i],
-                              reinterpret_cast<const uint32_t*>(buf + (size_t)kTile * 4)[i]);
+                              reinterpret_cast<const uint32_t*>(buf + (size_t)kSTile * 4)[i]);
         return make_uint2(__ldcs(k + t0 + i), __ldcs(v + t0 + i));
     }
 };
@@ -248,9 +252,9 @@ struct Bin2 {
 };
 
 // Scatters tuples [begin, end) of `in` into `out`. cursor[b] is the next output position of bin
-// b; it advances as tiles are written. Each tile of kTile tuples arrives by bulk copy into one of
+// b; it advances as tiles are written. Each tile of kSTile tuples arrives by bulk copy into one of
 // the two input buffers while the previous tile is processed. Per tile every thread holds its
-// kTile / kThreads tuples in registers, takes a rank inside its tuple's bin with one shared-memory
+// kSTile / kSThreads tuples in registers, takes a rank inside its tuple's bin with one shared-memory
 // atomic, and after a scan of the bin counts writes the tuple to its bin-ordered position in
 // `stage` (the tile's own input buffer, free once the tuples are in registers) with its bin in
 // `sbin`. The write pass then stores consecutive staged positions from consecutive threads, i.e.
@@ -262,14 +266,14 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
                               uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, int64_t* delta,
                               uint32_t* cnt, uint16_t* sbin, uint32_t* tmp, unsigned char* inbuf, uint64_t* bars,
                               uint32_t& ph, unsigned long long* errors) {
-    constexpr int kItems = kTile / kThreads;
-    const int64_t ntiles = (end - begin + kTile - 1) / kTile;
+    constexpr int kItems = kSTile / kSThreads;
+    const int64_t ntiles = (end - begin + kSTile - 1) / kSTile;
     if (ntiles <= 0) return;
-    for (int x = threadIdx.x; x < nbins; x += kThreads) cnt[x] = 0;
-    if (threadIdx.x == 0) in.issue(begin, (int)min_i64(kTile, end - begin), inbuf, &bars[0]);
+    for (int x = threadIdx.x; x < nbins; x += kSThreads) cnt[x] = 0;
+    if (threadIdx.x == 0) in.issue(begin, (int)min_i64(kSTile, end - begin), inbuf, &bars[0]);
     for (int64_t t = 0; t < ntiles; ++t) {
-        const int64_t t0 = begin + t * kTile;
-        const int tn = (int)min_i64(kTile, end - t0);
+        const int64_t t0 = begin + t * kSTile;
+        const int tn = (int)min_i64(kSTile, end - t0);
         const int b = (int)(t & 1);
         mbar_wait(&bars[b], (ph >> b) & 1u, errors);
         ph ^= 1u << b;
@@ -277,14 +281,14 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
         // (and cnt is zero again): the next tile may now be copied into b ^ 1.
         __syncthreads();
         if (threadIdx.x == 0 && t + 1 < ntiles)
-            in.issue(t0 + kTile, (int)min_i64(kTile, end - t0 - kTile), inbuf + (b ^ 1) * kTileBuf, &bars[b ^ 1]);
+            in.issue(t0 + kSTile, (int)min_i64(kSTile, end - t0 - kSTile), inbuf + (b ^ 1) * kTileBuf, &bars[b ^ 1]);
         unsigned char* buf = inbuf + b * kTileBuf;
         const uint32_t mis = in.mis(t0);
         uint2 it[kItems];
         uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
-            const int i = k * kThreads + threadIdx.x;
+            const int i = k * kSThreads + threadIdx.x;
             if (i < tn) {
                 it[k] = in.item(buf, t0, i, tn, mis);
                 const uint32_t bb = bin(it[k].x);
@@ -292,8 +296,8 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
             }
         }
         __syncthreads();
-        block_scan_excl(cnt, nbins, tmp);  // cnt[b] = first staged position of bin b
-        for (int x = threadIdx.x; x < nbins; x += kThreads) {
+        block_scan_excl_n<kSThreads>(cnt, nbins, tmp);  // cnt[b] = first staged position of bin b
+        for (int x = threadIdx.x; x < nbins; x += kSThreads) {
             const uint32_t e0 = cnt[x];
             const uint32_t e1 = (x + 1 < nbins) ? cnt[x + 1] : (uint32_t)tn;
             const int64_t c = cursor[x];
@@ -303,7 +307,7 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
         uint2* stage = reinterpret_cast<uint2*>(buf);
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
-            const int i = k * kThreads + threadIdx.x;
+            const int i = k * kSThreads + threadIdx.x;
             if (i < tn) {
                 const uint32_t bb = br[k] >> 16;
                 const uint32_t pos = cnt[bb] + (br[k] & 0xffffu);
@@ -312,10 +316,10 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
             }
         }
         __syncthreads();
-        for (int x = threadIdx.x; x < nbins; x += kThreads) cnt[x] = 0;  // for the next tile
+        for (int x = threadIdx.x; x < nbins; x += kSThreads) cnt[x] = 0;  // for the next tile
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
-            const int i = k * kThreads + threadIdx.x;
+            const int i = k * kSThreads + threadIdx.x;
             if (i < tn) {
                 const int64_t dst = delta[sbin[i]] + i;
                 if ((uint64_t)dst < (uint64_t)out_limit) out[dst] = stage[i];
@@ -515,7 +519,7 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 // true = S survivors of a level-1 Bloom probe, packed in cmp. One instantiation per input form keeps
 // each kernel within the 64 registers that two CTAs per SM allow.
 template <bool kPacked, int M>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kSThreads, 1)
 k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
              const int64_t* __restrict__ scan, unsigned long long* gwords, int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -524,7 +528,7 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
     uint32_t* cnt;
     uint16_t* sbin;
     scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
-    __shared__ uint32_t tmp[kThreads / 32];
+    __shared__ uint32_t tmp[kSThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
     uint32_t ph = 0;
@@ -541,7 +545,7 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const uint32_t P1 = d.pf.P1;
         const int64_t* S = scan + R.hist_base;
         const int64_t s0 = S[0];
-        for (uint32_t p = threadIdx.x; p < P1; p += kThreads)
+        for (uint32_t p = threadIdx.x; p < P1; p += kSThreads)
             cursor[p] = S[(int64_t)p * R.nslices + s] - s0;
         __syncthreads();
         const Bin1<M> bin{d.pf};
@@ -738,7 +742,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 
 // Level-2 scatter of one slice into its private runs of the level-2 buffer.
 template <int M>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kSThreads, 1)
 k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
              const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
              const int64_t* __restrict__ scan2, const uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords,
@@ -749,7 +753,7 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
     uint32_t* cnt;
     uint16_t* sbin;
     scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
-    __shared__ uint32_t tmp[kThreads / 32];
+    __shared__ uint32_t tmp[kSThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
     uint32_t ph = 0;
@@ -766,7 +770,7 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const int64_t* S2 = scan2 + R.h2_base;
         const int64_t s0 = S2[0];
         const int64_t* Sx = S2 + x.local_off * P2;
-        for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
+        for (uint32_t q = threadIdx.x; q < P2; q += kSThreads) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
         __syncthreads();
         scatter_tiles(PackedTiles{bloom ? R.cmp : R.l1}, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2,
                       R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph, &gwords[kGErrors]);
@@ -1357,7 +1361,7 @@ size_t probe_smem_bytes(int table_cap, int emit_key) {
 // Shared memory of the scatter kernels: two bulk-copy tile buffers, the reordered tile, and a
 // cursor and a count per bin.
 static size_t scatter_smem(int max_bins) {
-    return 2 * kTileBuf + (size_t)max_bins * (8 + 8 + 4) + (size_t)kTile * 2;
+    return 2 * kTileBuf + (size_t)max_bins * (8 + 8 + 4) + (size_t)kSTile * 2;
 }
 
 static cudaError_t set_smem_attr(const void* fn, size_t bytes) {
@@ -1450,12 +1454,12 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
         if (a.total_slices[rel] > 0) {
             for_modes(a.modes, [&](auto mt) {
                 constexpr int M = decltype(mt)::value;
-                const dim3 grid(grid_for(a.total_slices[rel], sms, 2));
-                k_l1_scatter<false, M><<<grid, kThreads, scatter_smem(a.max_p1), st>>>(
+                const dim3 grid(grid_for(a.total_slices[rel], sms, 1));
+                k_l1_scatter<false, M><<<grid, kSThreads, scatter_smem(a.max_p1), st>>>(
                     a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
                 ++launches;
                 if (rel == 1 && a.any_bloom_l1) {
-                    k_l1_scatter<true, M><<<grid, kThreads, scatter_smem(a.max_p1), st>>>(
+                    k_l1_scatter<true, M><<<grid, kSThreads, scatter_smem(a.max_p1), st>>>(
                         a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
                     ++launches;
                 }
@@ -1499,7 +1503,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 return err;
             for_modes(a.modes, [&](auto mt) {
                 constexpr int M = decltype(mt)::value;
-                k_l2_scatter<M><<<grid_for(a.l2_slice_cap[rel], sms, 2), kThreads, scatter_smem(a.max_p2), st>>>(
+                k_l2_scatter<M><<<grid_for(a.l2_slice_cap[rel], sms, 1), kSThreads, scatter_smem(a.max_p2), st>>>(
                     a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2_scan, a.slice_cnt2,
                     a.gwords, a.max_p2);
                 ++launches;
