@@ -335,47 +335,59 @@ def run_serve_workload(args):
     torch.cuda.synchronize()
     seq = [int(x) for x in rng.integers(0, len(pool), args.requests)]
 
-    def serve(rate, streams, max_wave):
-        lat, queue, results = [], [], []
-        # pinned host outputs: the pairs come back by asynchronous copies, as a client that hands
-        # the server page-locked buffers would receive them
-        outs = {i: tuple(torch.empty(pool[i][3] + 16, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
-                         for _ in range(2)) for i in set(seq)}
+    # pinned host outputs: the pairs come back by asynchronous copies, as a client that hands the
+    # server page-locked buffers would receive them
+    outs = {i: tuple(torch.empty(pool[i][3] + 16, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+                     for _ in range(2)) for i in range(len(pool))}
+
+    def one_load(srv, rate):
+        lat, queue = [], []
         gaps = np.random.default_rng(3).exponential(1.0 / rate, len(seq)) if rate > 0 else np.zeros(len(seq))
-        with bj.Server(hbm_budget_bytes=120 * 10**9, max_wave=max_wave, streams=streams) as srv:
-            tickets = []
-            t0 = time.perf_counter()
-            def submitter():
-                nxt = t0
-                for k, i in enumerate(seq):
-                    nxt += gaps[k]
-                    d = nxt - time.perf_counter()
-                    if d > 0:
-                        time.sleep(d)
-                    t, nr, ns, m = pool[i]
-                    tickets.append((srv.submit(t[0], t[1], t[2], t[3], capacity=m + 16, out=outs[i],
-                                               on_device=True), i))
-            th = threading.Thread(target=submitter)
-            th.start()
-            done = 0
-            while done < len(seq):
-                while len(tickets) <= done:
-                    time.sleep(0.0005)
-                tk, i = tickets[done]
-                res, a, b = srv.poll(tk)
-                assert res.status == bj.BRIG_OK and res.count == pool[i][3]
-                lat.append(res.submit_to_done_ms)
-                queue.append(res.queue_ms)
-                done += 1
-            th.join()
-            wall = time.perf_counter() - t0
+        tickets = []
+        t0 = time.perf_counter()
+
+        def submitter():
+            nxt = t0
+            for k, i in enumerate(seq):
+                nxt += gaps[k]
+                d = nxt - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                t, nr, ns, m = pool[i]
+                tickets.append((srv.submit(t[0], t[1], t[2], t[3], capacity=m + 16, out=outs[i], on_device=True), i))
+        th = threading.Thread(target=submitter)
+        th.start()
+        done = 0
+        while done < len(seq):
+            while len(tickets) <= done:
+                time.sleep(0.0005)
+            tk, i = tickets[done]
+            res, a, b = srv.poll(tk)
+            assert res.status == bj.BRIG_OK and res.count == pool[i][3]
+            lat.append(res.submit_to_done_ms)
+            queue.append(res.queue_ms)
+            done += 1
+        th.join()
+        wall = time.perf_counter() - t0
         tuples = sum(pool[i][1] + pool[i][2] for i in seq)
         return {"offered_req_per_s": rate, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "mean_queue_ms": float(np.mean(queue)), "tuples_per_s": tuples / wall, "wall_s": wall}
 
+    def run_mode(streams, max_wave):
+        # One long-running server per mode. A warm-up pass over the whole pool sizes every slot's
+        # workspace (growing it maps fresh device memory, which a running server pays once), then
+        # each offered load replays the same Poisson request sequence.
+        with bj.Server(hbm_budget_bytes=120 * 10**9, max_wave=max_wave, streams=streams) as srv:
+            for _ in range(2):
+                tk = [srv.submit(t[0], t[1], t[2], t[3], capacity=m + 16, out=outs[i], on_device=True)
+                      for i, (t, nr, ns, m) in enumerate(pool)]
+                for x in tk:
+                    srv.poll(x)
+            return [one_load(srv, r) for r in rates]
+
     rates = [float(x) for x in args.rates.split(",")]
-    sweep = [serve(r, args.streams, 16) for r in rates]
-    base = [serve(r, 1, 1) for r in rates]
+    sweep = run_mode(args.streams, 16)
+    base = run_mode(1, 1)
     line = {
         "metric": "served join tuples/s and p50/p99 latency", "value": max(x["tuples_per_s"] for x in sweep),
         "unit": UNIT, "n_gpus": 1, "dtype": "u32", "data": "synthetic", "higher_is_better": True,
@@ -398,7 +410,7 @@ def main():
     ap.add_argument("--joins", type=int, default=256, help="batch workload: number of joins")
     ap.add_argument("--pool", type=int, default=24, help="serve workload: distinct requests")
     ap.add_argument("--requests", type=int, default=64, help="serve workload: requests per load point")
-    ap.add_argument("--rates", default="5,20,80", help="serve workload: offered loads (requests/s)")
+    ap.add_argument("--rates", default="20,80,320,1280", help="serve workload: offered loads (requests/s)")
     ap.add_argument("--streams", type=int, default=3, help="serve workload: concurrent waves")
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -111,7 +111,8 @@ class ServeConfig(C.Structure):
         ("max_wave", C.c_int32),
         ("streams", C.c_int32),
         ("max_queue", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("max_wave_mtuples", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -338,9 +339,9 @@ class Join:
 class Server:
     """Served joins (brig_serve_*): submit host-array requests, poll tickets."""
 
-    def __init__(self, hbm_budget_bytes=0, max_wave=0, streams=0, max_queue=0, **join_cfg):
+    def __init__(self, hbm_budget_bytes=0, max_wave=0, streams=0, max_queue=0, max_wave_mtuples=0, **join_cfg):
         self.cfg = make_config(**join_cfg)
-        self.scfg = ServeConfig(hbm_budget_bytes, max_wave, streams, max_queue)
+        self.scfg = ServeConfig(hbm_budget_bytes, max_wave, streams, max_queue, max_wave_mtuples)
         h = C.c_void_p()
         check(lib().brig_serve_create(C.byref(self.cfg), C.byref(self.scfg), C.byref(h)), "brig_serve_create")
         self.h = h

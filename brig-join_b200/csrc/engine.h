@@ -101,6 +101,11 @@ public:
     void sync_counters(std::vector<int64_t>& counters, int64_t& errors);
     const std::vector<JoinPlan>& last_plans() const { return plans_; }
     int64_t workspace_bytes() const { return (int64_t)ws_bytes_; }
+    // Grows the workspace to at least `bytes`, stream-ordered on `stream` (after the last run).
+    void reserve_workspace(size_t bytes, cudaStream_t stream) {
+        if (have_run_ && bytes > ws_bytes_) cuda_check(cudaStreamWaitEvent(stream, done_, 0), "cudaStreamWaitEvent");
+        ensure_workspace(bytes, stream);
+    }
     const brig_join_config& config() const { return cfg_; }
     int device() const { return device_; }
     const std::vector<int64_t>& last_caps() const { return caps_; }

@@ -40,6 +40,7 @@ struct Req {
 struct Slot {
     cudaStream_t stream = nullptr;
     Engine* eng = nullptr;
+    int64_t ws_target = 0;  // workspace the admitted wave runs in (accounted in the budget)
     std::vector<Req*> wave;
     int phase = 0;  // 0 idle, 1 joining, 2 copying results
     cudaEvent_t ev = nullptr;
@@ -120,6 +121,7 @@ struct Server {
             brig_join_output o{q->outr, q->outs, nullptr, q->cap, nullptr};
             io.push_back(JoinIO{rk, rv, sk, sv, r.n_r, r.n_s, o});
         }
+        s.eng->reserve_workspace((size_t)s.ws_target, s.stream);
         s.eng->run(io, s.stream, false);
         cuda_check(cudaEventRecord(s.ev, s.stream), "cudaEventRecord");
         s.phase = 1;
@@ -186,11 +188,16 @@ struct Server {
                     // Grow the wave while the budget holds: bytes in use (live request buffers and
                     // every slot's workspace) + this wave's request buffers + the growth of this
                     // slot's workspace.
+                    // A wave also stops at max_wave_mtuples million tuples, so small requests
+                    // batch together while a large one runs alone and does not hold them back.
                     std::lock_guard<std::mutex> lk(mu);
                     const int64_t ws_have = s.eng->workspace_bytes();
-                    int64_t io = 0, ws_new = ws_have;
+                    const int64_t max_tuples = (int64_t)scfg.max_wave_mtuples * 1000000;
+                    int64_t io = 0, ws_new = ws_have, tuples = 0;
                     while (!pending.empty() && (int)wave.size() < scfg.max_wave) {
                         Req* q = pending.front();
+                        const int64_t t2 = tuples + q->in.n_r + q->in.n_s;
+                        if (!wave.empty() && t2 > max_tuples) break;
                         wave.push_back(q);
                         const int64_t io2 = io + io_bytes(q->in, q->cap);
                         const int64_t ws2 = std::max(ws_have, wave_workspace(wave));
@@ -200,12 +207,23 @@ struct Server {
                         }
                         io = io2;
                         ws_new = ws2;
+                        tuples = t2;
                         pending.pop_front();
                         q->state = 1;
                         q->t_start = Clock::now();
                         q->res.wave = next_wave;
                     }
+                    // A slot that must grow grows to at least the largest workspace of any slot
+                    // (when the budget allows), so after a warm-up no slot grows again: growing
+                    // maps fresh device memory and blocks the scheduler for that long.
+                    if (!wave.empty() && ws_new > ws_have) {
+                        int64_t widest = 0;
+                        for (const auto& o : slots) widest = std::max(widest, o.ws_target);
+                        const int64_t room = scfg.hbm_budget_bytes - (used + io + (ws_new - ws_have));
+                        if (widest > ws_new) ws_new += std::min(widest - ws_new, std::max<int64_t>(room, 0));
+                    }
                     used += io + (ws_new - ws_have);
+                    if (!wave.empty()) s.ws_target = ws_new;
                 }
                 if (wave.empty()) break;
                 s.wave = wave;
@@ -285,6 +303,7 @@ int brig_serve_create(const brig_join_config* jcfg, const brig_serve_config* scf
         if (s->scfg.max_wave <= 0) s->scfg.max_wave = 64;
         if (s->scfg.streams <= 0) s->scfg.streams = 2;
         if (s->scfg.max_queue <= 0) s->scfg.max_queue = 4096;
+        if (s->scfg.max_wave_mtuples <= 0) s->scfg.max_wave_mtuples = 256;
         try {
             if (jcfg->device >= 0) brig::cuda_check(cudaSetDevice(jcfg->device), "cudaSetDevice");
             brig::cuda_check(cudaGetDevice(&s->device), "cudaGetDevice");

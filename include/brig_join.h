@@ -210,7 +210,9 @@ typedef struct brig_serve_config {
     int32_t max_wave;          /* max joins per wave; 0 = 64 */
     int32_t streams;           /* concurrent waves; 0 = 2 */
     int32_t max_queue;         /* pending requests before submit rejects; 0 = 4096 */
-    int32_t reserved[5];
+    int32_t max_wave_mtuples;  /* a wave stops growing at this many million tuples (|R|+|S| summed);
+                                  a larger request runs as a wave of its own; 0 = 256 */
+    int32_t reserved[4];
 } brig_serve_config;
 
 /* One request. Inputs are HOST arrays (copied in by the server) or device arrays when
