@@ -1029,15 +1029,16 @@ __device__ __forceinline__ void warp_flush(const JoinDesc& d, const uint32_t* wr
 
 // Persistent probe kernel, two CTAs per SM. Each CTA takes tasks from the global queue (the next
 // task index is fetched while the current task runs). Per task the CTA
-//   * loads the build chunk (at most table_cap tuples) once, into registers, kBuildPer per thread,
-//     counts it per bucket with shared-memory reductions, scans the counts into bucket starts and
-//     places every tuple with an atomic on its bucket's cursor: a bucketised table in which off[b]
-//     ends as the end of bucket b, so bucket b = [off[b-1], off[b]). Every build key also sets one
-//     bit of a 65536-bit presence bitmap;
+//   * loads the build chunk (at most table_cap tuples) into registers, kBuildPer per thread, counts
+//     it per bucket with one shared-memory atomic per tuple (the atomic's result is the tuple's rank
+//     in its bucket), scans the counts into bucket starts (off[nb] = the chunk size) and places
+//     every tuple at off[bucket] + rank: a bucketised table, bucket b = [off[b], off[b+1]). Every
+//     build key also sets one bit of a 65536-bit presence bitmap;
 //   * streams the other side: its first kProbeFirst tuples from shared memory, where a bulk copy
 //     issued at the start of the task has put them while the table was built, the rest straight
-//     from global memory with kProbeU coalesced tuples per thread in flight. A streamed tuple whose
-//     bitmap bit is clear cannot match (at most 4096 keys set at most 6% of the bits); the others are compacted with ballot/popc into the warp's candidate
+//     from global memory with kProbeU coalesced tuples per thread in flight. (The build side is
+//     loaded once, into registers.) A streamed tuple whose bitmap bit is clear cannot match (at most 4096 keys set at
+//     most 6% of the bits); the others are compacted with ballot/popc into the warp's candidate
 //     queue in shared memory. Every 32 queued candidates the warp scans their buckets in lock step,
 //     one candidate per lane, and compacts matches into the warp's output staging buffer, which is
 //     written out with one global atomic per flush. So the bucket scans, whose cost is the longest
@@ -1069,8 +1070,8 @@ __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2*
     if (lane < n) {
         e = q[lane];
         const uint32_t bk = bucket_of(e.x, mask);
-        lo = bk ? off[bk - 1] : 0u;  // off[b] is the end of bucket b
-        hi = off[bk];
+        lo = off[bk];
+        hi = off[bk + 1];
     }
     while (__any_sync(0xffffffffu, lo < hi)) {
         bool m = false;
@@ -1202,11 +1203,9 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         while (nb < (uint32_t)nr) nb <<= 1;
         const uint32_t mask = nb - 1;
         // the previous task's probe is done with table, off, bitmap and pbuf
-        for (uint32_t i = threadIdx.x; i < nb; i += kThreads) off[i] = 0;
+        for (uint32_t i = threadIdx.x; i <= nb; i += kThreads) off[i] = 0;
         for (int i = threadIdx.x; i < kBitmapWords; i += kThreads) bitmap[i] = 0;
-        // ---- build: count per bucket and set the bitmap bits (reductions), scan the counts into
-        // bucket starts, then place every tuple with an atomic on its bucket's cursor, which leaves
-        // off[b] = end of bucket b (bucket b = [off[b-1], off[b]))
+        // ---- build: count per bucket (the atomic's result is the rank), set the bitmap bits
         uint2 bt[kBuildPer];
 #pragma unroll
         for (int k = 0; k < kBuildPer; ++k) {
@@ -1214,21 +1213,23 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
             if (i < nr) bt[k] = __ldg(bsrc + i);
         }
         __syncthreads();
+        uint32_t br[kBuildPer];  // bucket << 16 | rank in bucket
 #pragma unroll
         for (int k = 0; k < kBuildPer; ++k) {
             const int i = k * kThreads + threadIdx.x;
             if (i < nr) {
-                atomicAdd(&off[bucket_of(bt[k].x, mask)], 1u);
+                const uint32_t bk = bucket_of(bt[k].x, mask);
+                br[k] = (bk << 16) | atomicAdd(&off[bk], 1u);
                 const uint32_t pb = presence_bit(bt[k].x);
                 atomicOr(&bitmap[pb >> 5], 1u << (pb & 31u));
             }
         }
         __syncthreads();
-        block_scan_excl(off, (int)nb, tmp);  // off[b] = start of bucket b
+        block_scan_excl(off, (int)nb + 1, tmp);  // off[b] = start of bucket b, off[nb] = nr
 #pragma unroll
         for (int k = 0; k < kBuildPer; ++k) {
             const int i = k * kThreads + threadIdx.x;
-            if (i < nr) table[atomicAdd(&off[bucket_of(bt[k].x, mask)], 1u)] = bt[k];
+            if (i < nr) table[off[br[k] >> 16] + (br[k] & 0xffffu)] = bt[k];
         }
         mbar_wait(&bar, ph, errors);
         ph ^= 1u;

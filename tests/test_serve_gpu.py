@@ -63,6 +63,26 @@ def test_same_result_alone_and_in_mix(bj, oracle, torch_cuda):
             assert_same_pairs(oracle, ak, bk, ork, osk)
 
 
+def test_wave_tuple_cap_runs_large_requests_alone(bj, oracle, torch_cuda):
+    # With a 1M-tuple cap per wave, requests above 1M tuples each run as a wave of their own, while
+    # the small ones may share waves; every result is still exact.
+    small = [_req(bj, 300 + i, 20_000, 4, 0.1) for i in range(8)]
+    large = [_req(bj, 400 + i, 400_000, 4, 0.1) for i in range(3)]
+    reqs = small[:4] + large + small[4:]
+    with bj.Server(hbm_budget_bytes=4 << 30, max_wave=16, streams=1, max_wave_mtuples=1) as srv:
+        tickets = [srv.submit(*r) for r in reqs]
+        results = [srv.poll(t) for t in tickets]
+    waves = {}
+    for (res, a, b), r in zip(results, reqs):
+        assert res.status == bj.BRIG_OK
+        er, es = oracle.pairs(*r)
+        assert res.count == len(er)
+        assert_same_pairs(oracle, a, b, er, es)
+        waves.setdefault(res.wave, []).append(len(r[0]) + len(r[2]))
+    for sizes in waves.values():
+        assert sum(sizes) <= 1_000_000 or len(sizes) == 1, waves
+
+
 def test_admission_rejects_oversized_and_drains_under_tight_budget(bj, oracle, torch_cuda):
     big = _req(bj, 5, 2_000_000, 1, 0.1)
     small = [_req(bj, 50 + i, 100_000, 4, 0.1) for i in range(6)]
