@@ -189,15 +189,16 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, unsign
 // Where the tuples of a tile come from. PackedTiles: (key, value) pairs in an engine buffer; a tile
 // is copied from the 16-byte boundary at or below its first tuple (engine buffers are padded, so
 // reading up to 8 bytes past either end stays inside the workspace). KvTiles: the caller's separate
-// key and value arrays, bulk-copied when both are 16-byte aligned at tile starts; the last
-// (tn mod 4) tuples of a tile, or every tuple of unaligned arrays, are read with ordinary loads, so
-// nothing outside the caller's arrays is read. issue() is called by one thread and arms `bar`
-// (with no bytes when nothing is copied); item() reads tuple i of the tile.
+// key and value arrays; the 16-byte-aligned span of each array inside the tile is bulk-copied (the
+// two arrays may be misaligned differently) and the up to 3 + 3 tuples at its edges are read with
+// ordinary loads, so nothing outside the caller's arrays is read. mis(t0, tn) is the per-tile
+// layout word, issue() is called by one thread and arms `bar` (with no bytes when nothing is
+// copied), item() reads tuple i of the tile.
 constexpr size_t kTileBuf = (size_t)(kSTile + 2) * 8;  // one scatter input buffer
 
 struct PackedTiles {
     const uint2* p;
-    __device__ __forceinline__ uint32_t mis(int64_t t0) const {
+    __device__ __forceinline__ uint32_t mis(int64_t t0, int = 0) const {
         return (((uintptr_t)(p + t0)) & 15) ? 1u : 0u;
     }
     __device__ __forceinline__ void issue(int64_t t0, int tn, unsigned char* buf, uint64_t* bar) const {
@@ -219,24 +220,38 @@ struct PackedTiles {
 struct KvTiles {
     const uint32_t* k;
     const uint32_t* v;
-    bool bulk;
-    __device__ __forceinline__ uint32_t mis(int64_t) const { return 0u; }
+    bool bulk;  // both arrays are 4-byte aligned (uint32 arrays always are, unless misused)
+    // Per tile: the 16-byte-aligned span of each array inside [t0, t0 + tn), packed as
+    // hk | hv << 2 | nk << 4 | nv << 18 (h: first aligned offset from t0, n: aligned count).
+    __device__ __forceinline__ static uint32_t span(const uint32_t* p, int64_t t0, int tn, uint32_t& n) {
+        const uint32_t h = (4u - (uint32_t)(((uintptr_t)(p + t0) >> 2) & 3u)) & 3u;
+        n = (int)h < tn ? (uint32_t)(tn - (int)h) & ~3u : 0u;
+        return h;
+    }
+    __device__ __forceinline__ uint32_t mis(int64_t t0, int tn) const {
+        if (!bulk) return 0u;
+        uint32_t nk, nv;
+        const uint32_t hk = span(k, t0, tn, nk), hv = span(v, t0, tn, nv);
+        return hk | (hv << 2) | (nk << 4) | (nv << 18);
+    }
     __device__ __forceinline__ void issue(int64_t t0, int tn, unsigned char* buf, uint64_t* bar) const {
         fence_proxy_async();
-        if (bulk && (tn & ~3) > 0) {
-            const uint32_t bytes = (uint32_t)(tn & ~3) * 4u;
-            mbar_arrive_tx(bar, 2 * bytes);
-            bulk_g2s(buf, k + t0, bytes, bar);
-            bulk_g2s(buf + (size_t)kSTile * 4, v + t0, bytes, bar);
-        } else {
+        const uint32_t m = mis(t0, tn);
+        const uint32_t hk = m & 3u, hv = (m >> 2) & 3u, nk = (m >> 4) & 0x3fffu, nv = m >> 18;
+        if (nk + nv == 0) {
             mbar_arrive(bar);
+            return;
         }
+        mbar_arrive_tx(bar, 4u * (nk + nv));
+        if (nk) bulk_g2s(buf, k + t0 + hk, nk * 4u, bar);
+        if (nv) bulk_g2s(buf + (size_t)kSTile * 4, v + t0 + hv, nv * 4u, bar);
     }
-    __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t t0, int i, int tn, uint32_t) const {
-        if (bulk && i < (tn & ~3))
-            return make_uint2(reinterpret_cast<const uint32_t*>(buf)[i],
-                              reinterpret_cast<const uint32_t*>(buf + (size_t)kSTile * 4)[i]);
-        return make_uint2(__ldcs(k + t0 + i), __ldcs(v + t0 + i));
+    __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t t0, int i, int, uint32_t m) const {
+        const uint32_t ik = (uint32_t)i - (m & 3u), iv = (uint32_t)i - ((m >> 2) & 3u);  // wrap below the span
+        const uint32_t key = ik < ((m >> 4) & 0x3fffu) ? reinterpret_cast<const uint32_t*>(buf)[ik] : __ldcs(k + t0 + i);
+        const uint32_t val = iv < (m >> 18) ? reinterpret_cast<const uint32_t*>(buf + (size_t)kSTile * 4)[iv]
+                                            : __ldcs(v + t0 + i);
+        return make_uint2(key, val);
     }
 };
 
@@ -283,7 +298,7 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
         if (threadIdx.x == 0 && t + 1 < ntiles)
             in.issue(t0 + kSTile, (int)min_i64(kSTile, end - t0 - kSTile), inbuf + (b ^ 1) * kTileBuf, &bars[b ^ 1]);
         unsigned char* buf = inbuf + b * kTileBuf;
-        const uint32_t mis = in.mis(t0);
+        const uint32_t mis = in.mis(t0, tn);
         uint2 it[kItems];
         uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
 #pragma unroll
@@ -395,8 +410,13 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         const bool bloom = (rel == 1) && d.bloom != nullptr && d.bloom_level == 1;
         if (!bloom) {
             const uint32_t* __restrict__ key = R.key;
-            if ((((uintptr_t)(key + b)) & 15) == 0) {
-                int64_t i = b + 4 * (int64_t)threadIdx.x;
+            // the keys before the first 16-byte boundary (at most 3) one by one, then 16-byte loads
+            const int64_t head = (((uintptr_t)key) & 3) ? (e - b)
+                                 : min_i64(e - b, (4 - (int64_t)((((uintptr_t)(key + b)) >> 2) & 3)) & 3);
+            if (head < e - b) {
+                if ((int64_t)threadIdx.x < head) atomicAdd(&sh_cnt[part1_m<M>(pf, __ldcs(key + b + threadIdx.x))], 1u);
+                const int64_t b4 = b + head;  // 16-byte aligned
+                int64_t i = b4 + 4 * (int64_t)threadIdx.x;
                 // four 16-byte loads in flight per thread
                 for (; i + 12 * kThreads + 3 < e; i += 16 * kThreads) {
                     uint4 k4[4];
@@ -419,7 +439,7 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                     atomicAdd(&sh_cnt[part1_m<M>(pf, k4.w)], 1u);
                 }
                 // tail: at most 3 tuples past the last full vector
-                const int64_t tail0 = b + ((e - b) & ~(int64_t)3);
+                const int64_t tail0 = b4 + ((e - b4) & ~(int64_t)3);
                 for (int64_t t = tail0 + threadIdx.x; t < e; t += kThreads)
                     atomicAdd(&sh_cnt[part1_m<M>(pf, __ldcs(key + t))], 1u);
             } else {
@@ -553,7 +573,7 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
             scatter_tiles(PackedTiles{R.cmp}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf,
                           bars, ph, &gwords[kGErrors]);
         } else {
-            const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 15) == 0;
+            const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 3) == 0;
             scatter_tiles(KvTiles{R.key, R.val, al}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp,
                           inbuf, bars, ph, &gwords[kGErrors]);
         }

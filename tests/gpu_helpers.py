@@ -14,17 +14,19 @@ def run_device(bj, torch, rk, rv, sk, sv, cap=None, emit_key=False, handle=None,
     """Joins numpy inputs on the GPU; returns (stats, r_vals, s_vals, keys-or-None).
 
     `offset` > 0 places each input `offset` elements into its buffer, so the kernels see
-    addresses that are not 16-byte aligned."""
+    addresses that are not 16-byte aligned; a 4-tuple gives each of (r_key, r_val, s_key, s_val)
+    its own offset."""
     if cap is None:
         cap = max(len(sk), 1)
+    offs = tuple(offset) if isinstance(offset, (tuple, list)) else (offset,) * 4
     ins = []
-    for a in (rk, rv, sk, sv):
+    for a, off in zip((rk, rv, sk, sv), offs):
         a = np.ascontiguousarray(a, dtype=np.uint32)
-        buf = torch.zeros(len(a) + offset + 1, dtype=torch.int32, device="cuda")
+        buf = torch.zeros(len(a) + off + 1, dtype=torch.int32, device="cuda")
         if len(a):
-            buf[offset:offset + len(a)] = torch.from_numpy(a.view(np.int32)).to("cuda")
+            buf[off:off + len(a)] = torch.from_numpy(a.view(np.int32)).to("cuda")
         ins.append(buf)
-    ptr = [t.data_ptr() + 4 * offset for t in ins]
+    ptr = [t.data_ptr() + 4 * off for t, off in zip(ins, offs)]
     out_r = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
     out_s = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
     out_k = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda") if emit_key else None

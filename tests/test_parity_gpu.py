@@ -100,6 +100,18 @@ def test_ragged_unaligned_inputs(bj, oracle, torch_cuda):
     assert_same_pairs(oracle, r, s, exp_r, exp_s)
 
 
+@pytest.mark.parametrize("offsets", [(1, 3, 2, 0), (3, 1, 0, 2), (2, 2, 3, 1)])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_differently_misaligned_key_and_value_arrays(bj, oracle, torch_cuda, offsets, mode):
+    # keys and values misaligned by different amounts, over many scatter tiles per slice
+    rk, rv, sk, sv = bj.gen_host(31, 700_001, 900_003, 0.2)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    st, r, s, _ = run_device(bj, torch_cuda, rk, rv, sk, sv, cap=len(exp_r), offset=offsets,
+                             partition_mode=mode, use_bloom=mode)
+    assert st.count == len(exp_r)
+    assert_same_pairs(oracle, r, s, exp_r, exp_s)
+
+
 def test_capacity_overflow_counts_exactly(bj, oracle, torch_cuda):
     rk, rv, sk, sv = bj.gen_host(3, 50_000, 50_000, 0.4)
     exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
