@@ -327,7 +327,10 @@ class Join:
         chosen = Config()
         check(lib().brig_join_autotune(self.h, self._items(items), len(items), _ptr(stream), C.byref(chosen)),
               "brig_join_autotune")
-        return {"table_capacity": chosen.table_capacity, "max_level1_bits": chosen.max_level1_bits}
+        return {"table_capacity": chosen.table_capacity, "max_level1_bits": chosen.max_level1_bits,
+                "use_bloom": chosen.use_bloom,
+                "bloom_bits_per_key": chosen.bloom_bits_per_key if chosen.use_bloom else 0.0,
+                "bloom_num_hashes": chosen.bloom_num_hashes if chosen.use_bloom else 0}
 
     def batch_counts(self, n: int, allow_overflow=False) -> np.ndarray:
         c = np.zeros(n, np.int64)

@@ -594,9 +594,20 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
 
 brig_join_config Engine::autotune(const std::vector<JoinIO>& joins, cudaStream_t stream) {
     // Candidates: shared-memory table capacity (build-chunk size, which also sets the partition
-    // count through the planner's fill target) x largest level-1 fan-out.
+    // count through the planner's fill target) x largest level-1 fan-out x Bloom prefilter (off, or
+    // 10 bits/key with 7 hashes; the filter changes only the speed, never the result). A caller's
+    // own Bloom setting is kept as the "on" candidate.
     const int tables[] = {1024, 2048, 4096};
     const int l1bits[] = {8, 9, 10};
+    struct BloomChoice {
+        int use;
+        double bpk;
+        int k;
+    };
+    const BloomChoice blooms[] = {
+        {0, 0.0, 0},
+        {1, cfg_.use_bloom && cfg_.bloom_bits_per_key > 0 ? cfg_.bloom_bits_per_key : 10.0,
+         cfg_.use_bloom && cfg_.bloom_num_hashes > 0 ? cfg_.bloom_num_hashes : 7}};
     const brig_join_config base = cfg_;
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
@@ -604,12 +615,19 @@ brig_join_config Engine::autotune(const std::vector<JoinIO>& joins, cudaStream_t
     float best = -1.f;
     brig_join_config best_cfg = base;
     try {
+        for (const BloomChoice& bc : blooms)
         for (int t : tables) {
             for (int b : l1bits) {
                 cfg_ = base;
                 cfg_.table_capacity = t;
                 cfg_.max_level1_bits = b;
                 cfg_.profile_stages = 0;
+                cfg_.use_bloom = bc.use;
+                if (bc.use) {
+                    cfg_.bloom_bits_per_key = bc.bpk;
+                    cfg_.bloom_num_hashes = bc.k;
+                    cfg_.bloom_num_bits = 0;
+                }
                 run(joins, stream, false);  // warm-up (sizes the workspace)
                 cuda_check(cudaEventRecord(e0, stream), "cudaEventRecord");
                 run(joins, stream, false);

@@ -212,7 +212,9 @@ struct PackedTiles {
         mbar_arrive_tx(bar, bytes);
         bulk_g2s(buf, p + t0 - m, bytes, bar);
     }
-    __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t, int i, int, uint32_t m) const {
+    using Layout = uint32_t;  // tuples before the first one in the buffer (0 or 1)
+    __device__ __forceinline__ Layout layout(int64_t t0, int) const { return mis(t0); }
+    __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t, int i, int, Layout m) const {
         return reinterpret_cast<const uint2*>(buf)[i + m];
     }
 };
@@ -246,11 +248,25 @@ struct KvTiles {
         if (nk) bulk_g2s(buf, k + t0 + hk, nk * 4u, bar);
         if (nv) bulk_g2s(buf + (size_t)kSTile * 4, v + t0 + hv, nv * 4u, bar);
     }
-    __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t t0, int i, int, uint32_t m) const {
-        const uint32_t ik = (uint32_t)i - (m & 3u), iv = (uint32_t)i - ((m >> 2) & 3u);  // wrap below the span
-        const uint32_t key = ik < ((m >> 4) & 0x3fffu) ? reinterpret_cast<const uint32_t*>(buf)[ik] : __ldcs(k + t0 + i);
-        const uint32_t val = iv < (m >> 18) ? reinterpret_cast<const uint32_t*>(buf + (size_t)kSTile * 4)[iv]
-                                            : __ldcs(v + t0 + i);
+    // The tile layout word decoded once per tile.
+    struct Layout {
+        uint32_t hk, hv, nk, nv;
+        bool whole;  // both spans cover the whole tile: every tuple from shared memory
+    };
+    __device__ __forceinline__ Layout layout(int64_t t0, int tn) const {
+        const uint32_t m = mis(t0, tn);
+        Layout l{m & 3u, (m >> 2) & 3u, (m >> 4) & 0x3fffu, m >> 18, false};
+        l.whole = l.hk == 0 && l.hv == 0 && l.nk == (uint32_t)tn && l.nv == (uint32_t)tn;
+        return l;
+    }
+    __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t t0, int i, int, const Layout& l) const {
+        if (l.whole)  // tile-uniform
+            return make_uint2(reinterpret_cast<const uint32_t*>(buf)[i],
+                              reinterpret_cast<const uint32_t*>(buf + (size_t)kSTile * 4)[i]);
+        const uint32_t ik = (uint32_t)i - l.hk, iv = (uint32_t)i - l.hv;  // wrap below the span
+        const uint32_t key = ik < l.nk ? reinterpret_cast<const uint32_t*>(buf)[ik] : __ldcs(k + t0 + i);
+        const uint32_t val = iv < l.nv ? reinterpret_cast<const uint32_t*>(buf + (size_t)kSTile * 4)[iv]
+                                       : __ldcs(v + t0 + i);
         return make_uint2(key, val);
     }
 };
@@ -298,14 +314,14 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
         if (threadIdx.x == 0 && t + 1 < ntiles)
             in.issue(t0 + kSTile, (int)min_i64(kSTile, end - t0 - kSTile), inbuf + (b ^ 1) * kTileBuf, &bars[b ^ 1]);
         unsigned char* buf = inbuf + b * kTileBuf;
-        const uint32_t mis = in.mis(t0, tn);
+        const auto lay = in.layout(t0, tn);
         uint2 it[kItems];
         uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const int i = k * kSThreads + threadIdx.x;
             if (i < tn) {
-                it[k] = in.item(buf, t0, i, tn, mis);
+                it[k] = in.item(buf, t0, i, tn, lay);
                 const uint32_t bb = bin(it[k].x);
                 br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
             }

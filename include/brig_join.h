@@ -193,10 +193,10 @@ int brig_join_run_batch(brig_join_t* h, const brig_join_batch_item* items, int32
  * BRIG_E_OVERFLOW if any join exceeded its capacity. */
 int brig_join_batch_counts(brig_join_t* h, int64_t* counts, int32_t n_items);
 
-/* Times candidate configurations (shared-memory table capacity x level-1 fan-out) on the given
- * batch and keeps the fastest in the handle; the chosen configuration is copied to *chosen when
- * not NULL. Runs the batch 2 x 9 times; results of those runs are discarded (outputs are
- * overwritten). The reference has no autotuner; its sizing is fixed heuristics
+/* Times candidate configurations (shared-memory table capacity x level-1 fan-out x Bloom
+ * prefilter off or on) on the given batch and keeps the fastest in the handle; the chosen
+ * configuration is copied to *chosen when not NULL. Runs the batch 2 x 18 times; results of those
+ * runs are discarded (outputs are overwritten). The reference has no autotuner; its sizing is fixed heuristics
  * (src/hash_kernel.cu:198-284). */
 int brig_join_autotune(brig_join_t* h, const brig_join_batch_item* items, int32_t n_items, void* stream,
                        brig_join_config* chosen);
