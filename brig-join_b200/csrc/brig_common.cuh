@@ -186,21 +186,34 @@ BRIG_HD void bloom_masks(uint64_t g, int k, uint32_t& ma, uint32_t& mb) {
     }
 }
 
-template <int K = 0>
-BRIG_HD void bloom_key_of_hash(uint64_t g, uint32_t seg_blocks, int k, BloomKey& bk) {
+// Where a key with hash g lives: its block and the two words in it (masks are separate).
+BRIG_HD void bloom_place(uint64_t g, uint32_t seg_blocks, BloomKey& bk) {
     bk.block = bloom_block_of(g, seg_blocks);
     bk.wa = (uint32_t)(g >> 35) & 3u;
     bk.wb = 4u + ((uint32_t)(g >> 37) & 3u);
-    bloom_masks<K>(g, k, bk.ma, bk.mb);
 }
 
-template <int K = 0>
-BRIG_HD void bloom_key(uint32_t key, uint32_t seg_blocks, int k, BloomKey& bk) {
-    bloom_key_of_hash<K>(bloom_hash(key), seg_blocks, k, bk);
-}
 // Compile-time k class of a join's filter: the Bloom kernels are instantiated for k = 7 (the usual
 // 10 bits/key setting) and for any k, and each instantiation skips the other's joins.
 constexpr int kBloomFastK = 7;
+
+// For k = 7 the masks are pattern-blocked (Lang et al., as above): hash bits 0..9 pick one of 1024
+// 4-bit patterns for the group-0 word and bits 10..19 one of 1024 3-bit patterns for the group-1
+// word. Pattern i of word w is the OR of 1 << (5-bit fields of a SplitMix64 hash of (w, i)), so the
+// two table look-ups replace the shifts of seven bit positions. The kernels that build or probe a
+// k = 7 filter keep both tables (8 KB) in shared memory.
+constexpr int kPatterns = 1024;
+BRIG_HD uint32_t bloom_pattern(int word, uint32_t i) {
+    const uint64_t h = mix64(((uint64_t)(word + 1) << 32) ^ (uint64_t)i ^ 0x243f6a8885a308d3ull);
+    const int nb = word == 0 ? 4 : 3;
+    uint32_t m = 0;
+    for (int b = 0; b < nb; ++b) m |= 1u << ((uint32_t)(h >> (5 * b)) & 31u);
+    return m;
+}
+BRIG_HD void bloom_pattern_masks(const uint32_t* pat, uint64_t g, uint32_t& ma, uint32_t& mb) {
+    ma = pat[(uint32_t)g & (kPatterns - 1)];
+    mb = pat[kPatterns + ((uint32_t)(g >> 10) & (kPatterns - 1))];
+}
 
 // ---- per-join descriptor (device resident) ------------------------------------------------------
 struct RelPlan {

@@ -384,6 +384,18 @@ __device__ __forceinline__ void init_bars(uint64_t* bars) {
 
 // Bloom probe, split in two so a thread can have several block loads in flight: the address of a
 // key's 32-byte block in the segment of its finest partition f, then the test of the loaded words.
+// Bit masks of a key with hash g: the shared-memory pattern tables for k = 7 (pat), the bit
+// arithmetic for any other k.
+template <int K>
+__device__ __forceinline__ void key_masks(const uint32_t* pat, uint64_t g, int k, uint32_t& ma, uint32_t& mb) {
+    if constexpr (K == kBloomFastK) bloom_pattern_masks(pat, g, ma, mb);
+    else bloom_masks<0>(g, k, ma, mb);
+}
+// Fills the two pattern tables of a k = 7 kernel (block-wide; the caller synchronises).
+__device__ __forceinline__ void fill_patterns(uint32_t* pat) {
+    for (int i = threadIdx.x; i < 2 * kPatterns; i += blockDim.x) pat[i] = bloom_pattern(i / kPatterns, i % kPatterns);
+}
+
 // The Bloom k class of a join (the K of the kernel instantiation that handles it).
 __device__ __forceinline__ int bloom_kclass(const JoinDesc& d) {
     return (d.bloom != nullptr && d.bloom_k == kBloomFastK) ? kBloomFastK : 0;
@@ -408,6 +420,8 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
           uint32_t* __restrict__ hist, unsigned long long* gwords) {
     extern __shared__ uint32_t sh_cnt[];  // [max P1]
     __shared__ uint32_t s_cursor;
+    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // k = 7 pattern tables
+    if constexpr (K == kBloomFastK) fill_patterns(s_pat);  // synchronised by the slice loop's first barrier
     const int lane = threadIdx.x & 31;
     const int64_t total = slice_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
@@ -488,7 +502,7 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
                     if (r < len) {
                         BloomKey bkey;
-                        bloom_key<K>(kk[u], seg_blocks, bk, bkey);
+                        bloom_place(bloom_hash(kk[u]), seg_blocks, bkey);
                         const uint32_t* w =
                             bloom_words(bloom, seg_blocks, part_fine_m<M>(pf, kk[u]), bkey.block);
                         va[u] = __ldg(w + bkey.wa);
@@ -501,7 +515,7 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
                     if (r < len) {
                         uint32_t ma, mb;
-                        bloom_masks<K>(bloom_hash(kk[u]), bk, ma, mb);
+                        key_masks<K>(s_pat, bloom_hash(kk[u]), bk, ma, mb);
                         if ((va[u] & ma) == ma && (vb[u] & mb) == mb) pm |= 1u << u;
                     }
                 }
@@ -673,6 +687,8 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
           uint32_t* __restrict__ hist2, uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords) {
     extern __shared__ uint32_t cnt[];  // [max P2]
     __shared__ uint32_t s_surv;
+    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // k = 7 pattern tables
+    if constexpr (K == kBloomFastK && kBloom) fill_patterns(s_pat);  // synchronised by the slice loop's first barrier
     const int lane = threadIdx.x & 31;
     const int64_t total = (int64_t)gwords[kGL2Slices + rel];
     for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
@@ -724,7 +740,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
                     if (r < len) {
                         BloomKey bkey;
-                        bloom_key<K>(e[u].x, seg_blocks, bk, bkey);
+                        bloom_place(bloom_hash(e[u].x), seg_blocks, bkey);
                         const uint32_t* w = bloom_words(bloom, seg_blocks, fbase + bin(e[u].x), bkey.block);
                         va[u] = __ldg(w + bkey.wa);
                         vb[u] = __ldg(w + bkey.wb);
@@ -736,7 +752,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
                     if (r < len) {
                         uint32_t ma, mb;
-                        bloom_masks<K>(bloom_hash(e[u].x), bk, ma, mb);
+                        key_masks<K>(s_pat, bloom_hash(e[u].x), bk, ma, mb);
                         if ((va[u] & ma) == ma && (vb[u] & mb) == mb) pm |= 1u << u;
                     }
                 }
@@ -848,6 +864,8 @@ __global__ void __launch_bounds__(kThreads)
 k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ bloom_prefix,
               int smem_words, unsigned long long* gwords) {
     extern __shared__ __align__(16) uint32_t seg[];
+    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // k = 7 pattern tables
+    if constexpr (K == kBloomFastK) fill_patterns(s_pat);  // synchronised by the group loop's first barrier
     const int64_t total = bloom_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(bloom_prefix, nj, g);
@@ -887,11 +905,14 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
                     atomicAdd(&gwords[kGErrors], 1ull);
                     continue;
                 }
+                const uint64_t g = bloom_hash(kk[u]);
                 BloomKey bkey;
-                bloom_key<K>(kk[u], seg_blocks, k, bkey);
+                bloom_place(g, seg_blocks, bkey);
+                uint32_t ma, mb;
+                key_masks<K>(s_pat, g, k, ma, mb);
                 uint32_t* blk = dst + local * nw + (int64_t)bkey.block * 8;
-                atomicOr(blk + bkey.wa, bkey.ma);
-                if (bkey.mb) atomicOr(blk + bkey.wb, bkey.mb);
+                atomicOr(blk + bkey.wa, ma);
+                if (mb) atomicOr(blk + bkey.wb, mb);
             }
         }
         __syncthreads();
