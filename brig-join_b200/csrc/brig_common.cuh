@@ -122,18 +122,17 @@ BRIG_HD uint32_t bucket_of(uint32_t key, uint32_t nb_mask) { return mix32(key) &
 // Cache-sectorized blocked Bloom filter (Lang, Neumann, Kemper, Boncz, "Performance-Optimal
 // Filtering: Bloom overtakes Cuckoo at High Throughput", VLDB 2019). The filter is one segment per
 // finest partition; a segment is seg_blocks blocks of 256 bits, one 32-byte DRAM sector of eight
-// 32-bit words in two groups of four. A key picks one word in each group and sets its k bit
-// positions in those two words: the first ceil(k/2) in the word of group 0, the rest in the word of
-// group 1. So a build is two 32-bit atomicOr per key and a probe two word loads from one sector,
-// with no search or dynamic indexing. The reference uses 256-bit blocks with k bit positions
-// anywhere in the block and one segment per first-level partition (src/bloom.cu:698-722,
-// src/hash_kernel.cu:555-582).
+// 32-bit words, i.e. four 8-byte word pairs. A key picks one word pair and sets its k bit positions
+// in those two words: the first ceil(k/2) in the even word, the rest in the odd word. So a build
+// is two 32-bit atomicOr per key and a probe one 8-byte load, with no search or dynamic indexing.
+// The reference uses 256-bit blocks with k bit positions anywhere in the block and one segment
+// per first-level partition (src/bloom.cu:698-722, src/hash_kernel.cu:555-582).
 //
-// Hash bits (g = bloom_hash(key)): bits 40..63 pick the block, bits 35..36 and 37..38 the two words,
-// bits 5i..5i+4 the position of bit i for i < 7; positions of bits 7.. come from mix64(g).
+// Hash bits (g = bloom_hash(key)): bits 40..63 pick the block, bits 35..36 the word pair, bits
+// 5i..5i+4 the position of bit i for i < 7 (k != 7); positions of bits 7.. come from mix64(g).
 struct BloomKey {
     uint32_t block;   // block index inside the segment
-    uint32_t wa, wb;  // word of group 0 (0..3) and of group 1 (4..7)
+    uint32_t wa, wb;  // the pair's even and odd word (wb = wa + 1)
     uint32_t ma, mb;  // bits to set/test in them
 };
 
@@ -186,11 +185,13 @@ BRIG_HD void bloom_masks(uint64_t g, int k, uint32_t& ma, uint32_t& mb) {
     }
 }
 
-// Where a key with hash g lives: its block and the two words in it (masks are separate).
+// Where a key with hash g lives: its block and the two words in it (masks are separate). The
+// kernels use the word pair layout: hash bits 35..36 pick one of the block's four 8-byte word
+// pairs, so a probe reads both words with one 8-byte load.
 BRIG_HD void bloom_place(uint64_t g, uint32_t seg_blocks, BloomKey& bk) {
     bk.block = bloom_block_of(g, seg_blocks);
-    bk.wa = (uint32_t)(g >> 35) & 3u;
-    bk.wb = 4u + ((uint32_t)(g >> 37) & 3u);
+    bk.wa = 2u * ((uint32_t)(g >> 35) & 3u);
+    bk.wb = bk.wa + 1u;
 }
 
 // Compile-time k class of a join's filter: the Bloom kernels are instantiated for k = 7 (the usual
@@ -198,7 +199,7 @@ BRIG_HD void bloom_place(uint64_t g, uint32_t seg_blocks, BloomKey& bk) {
 constexpr int kBloomFastK = 7;
 
 // For k = 7 the masks are pattern-blocked (Lang et al., as above): hash bits 0..9 pick one of 1024
-// 4-bit patterns for the group-0 word and bits 10..19 one of 1024 3-bit patterns for the group-1
+// 4-bit patterns for the even word and bits 10..19 one of 1024 3-bit patterns for the odd
 // word. Pattern i of word w is the OR of 1 << (5-bit fields of a SplitMix64 hash of (w, i)), so the
 // two table look-ups replace the shifts of seven bit positions. The kernels that build or probe a
 // k = 7 filter keep both tables (8 KB) in shared memory.

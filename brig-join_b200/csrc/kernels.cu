@@ -505,8 +505,9 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                         bloom_place(bloom_hash(kk[u]), seg_blocks, bkey);
                         const uint32_t* w =
                             bloom_words(bloom, seg_blocks, part_fine_m<M>(pf, kk[u]), bkey.block);
-                        va[u] = __ldg(w + bkey.wa);
-                        vb[u] = __ldg(w + bkey.wb);
+                        const uint2 pair = __ldg(reinterpret_cast<const uint2*>(w + bkey.wa));
+                        va[u] = pair.x;
+                        vb[u] = pair.y;
                     }
                 }
                 uint32_t pm = 0;  // bit u: tuple u passed the filter
@@ -742,8 +743,9 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                         BloomKey bkey;
                         bloom_place(bloom_hash(e[u].x), seg_blocks, bkey);
                         const uint32_t* w = bloom_words(bloom, seg_blocks, fbase + bin(e[u].x), bkey.block);
-                        va[u] = __ldg(w + bkey.wa);
-                        vb[u] = __ldg(w + bkey.wb);
+                        const uint2 pair = __ldg(reinterpret_cast<const uint2*>(w + bkey.wa));
+                        va[u] = pair.x;
+                        vb[u] = pair.y;
                     }
                 }
                 uint32_t pm = 0;  // bit u: tuple u passed the filter
