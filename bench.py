@@ -211,9 +211,9 @@ def stage_bytes(nr, ns, surv, matches, bloom_bits, bloom_level):
 # measured traffic to the benchmarked launch; the per-tuple traffic of these streaming kernels does
 # not depend on the relation size once the inputs exceed the L2.
 NCU_TRAFFIC_PER_TUPLE = {
-    "r_hist": (4.06, "nr"), "r_scatter": (18.2, "nr"), "r_l2_hist": (8.05, "nr"), "r_l2_scatter": (15.4, "nr"),
-    "bloom_build": (8.44, "nr"), "s_hist_probe": (4.06, "ns"), "s_scatter": (18.2, "ns"),
-    "s_l2_hist": (10.5, "ns"), "probe": (10.0, "nr"),
+    "r_hist": (4.07, "nr"), "r_scatter": (16.3, "nr"), "r_l2_hist": (8.06, "nr"), "r_l2_scatter": (15.4, "nr"),
+    "bloom_build": (8.44, "nr"), "s_hist_probe": (4.06, "ns"), "s_scatter": (16.3, "ns"),
+    "s_l2_hist": (10.06, "ns"), "probe": (9.61, "nr"),
 }
 
 
