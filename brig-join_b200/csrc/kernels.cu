@@ -282,124 +282,95 @@ struct Bin2 {
     __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return part2_m<M>(f, key); }
 };
 
-// Scatters tuples [begin, end) of `in` into `out` with software write-combining buffers: every bin
-// has a buffer of `wcap` tuples in shared memory (wc[bin * wcap ..]); cursor[b] is the output
-// position of bin b's next flush. Tiles of kSTile tuples arrive by bulk copy into one of two input
-// buffers while the previous tile is processed, and each tile is consumed in kSTile / kSThreads
-// rounds. In a round every thread takes one tuple and one slot of its bin (a shared-memory atomic
-// on the bin's fill count): a slot inside the buffer stores the tuple there; a slot past it (the
-// bin received more than its free space this round) writes the tuple straight to
-// cursor + slot, since the flush below reserves those positions. Then every full buffer is written
-// out as one run of wcap consecutive tuples (a 128-byte line for wcap = 16), the bin's cursor
-// advances by its whole fill count and the buffer empties. After the last tile the partly filled
-// buffers are written out. Per tuple that is one atomic, one shared-memory store and one load (no
-// per-tile scan or full-tile reorder), and the global stores are whole runs except for overflows.
+// Scatters tuples [begin, end) of `in` into `out`. cursor[b] is the next output position of bin
+// b; it advances as tiles are written. Each tile of kSTile tuples arrives by bulk copy into one of
+// the two input buffers while the previous tile is processed. Per tile every thread holds its
+// kSTile / kSThreads tuples in registers, takes a rank inside its tuple's bin with one shared-memory
+// atomic, and after a scan of the bin counts writes the tuple to its bin-ordered position in
+// `stage` (the tile's own input buffer, free once the tuples are in registers) with its bin in
+// `sbin`. The write pass then stores consecutive staged positions from consecutive threads, i.e.
+// runs of one bin to consecutive addresses; delta[b] = cursor[b] - (first staged position of b)
+// turns a staged position into its output position with one add.
+// `inbuf` holds two tile buffers, `bars` their mbarriers, `ph` the parity of each barrier.
 template <class In, class Bin>
 __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
-                              uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, uint2* wc,
-                              uint32_t* fill, uint32_t wcap, unsigned char* inbuf, uint64_t* bars,
+                              uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, int64_t* delta,
+                              uint32_t* cnt, uint16_t* sbin, uint32_t* tmp, unsigned char* inbuf, uint64_t* bars,
                               uint32_t& ph, unsigned long long* errors) {
     constexpr int kItems = kSTile / kSThreads;
-    constexpr int kWarps = kSThreads / 32;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int64_t ntiles = (end - begin + kSTile - 1) / kSTile;
     if (ntiles <= 0) return;
-    for (int x = threadIdx.x; x < nbins; x += kSThreads) fill[x] = 0;
+    for (int x = threadIdx.x; x < nbins; x += kSThreads) cnt[x] = 0;
     if (threadIdx.x == 0) in.issue(begin, (int)min_i64(kSTile, end - begin), inbuf, &bars[0]);
-    // Writes out bin x's buffered tuples (the first min(count, wcap) of `count` this round) with the
-    // lanes of the calling warp and advances its cursor past all `count`.
-    auto flush_bin = [&](uint32_t x, uint32_t count) {
-        const int64_t c = cursor[x];
-        const uint32_t n = count < wcap ? count : wcap;
-        for (uint32_t l = (uint32_t)lane; l < n; l += 32) {
-            const int64_t dst = c + l;
-            if ((uint64_t)dst < (uint64_t)out_limit) out[dst] = wc[(size_t)x * wcap + l];
-            else atomicAdd(errors, 1ull);
-        }
-        __syncwarp();
-        if (lane == 0) {
-            cursor[x] = c + count;
-            fill[x] = 0;
-        }
-    };
     for (int64_t t = 0; t < ntiles; ++t) {
         const int64_t t0 = begin + t * kSTile;
         const int tn = (int)min_i64(kSTile, end - t0);
         const int b = (int)(t & 1);
         mbar_wait(&bars[b], (ph >> b) & 1u, errors);
         ph ^= 1u << b;
-        // Every thread has taken all tuples of the previous tile out of buffer b ^ 1.
+        // Every thread is past the previous tile's write pass, which read buffer b ^ 1 as `stage`
+        // (and cnt is zero again): the next tile may now be copied into b ^ 1.
         __syncthreads();
         if (threadIdx.x == 0 && t + 1 < ntiles)
             in.issue(t0 + kSTile, (int)min_i64(kSTile, end - t0 - kSTile), inbuf + (b ^ 1) * kTileBuf, &bars[b ^ 1]);
-        const unsigned char* buf = inbuf + b * kTileBuf;
+        unsigned char* buf = inbuf + b * kTileBuf;
         const auto lay = in.layout(t0, tn);
-        for (int r = 0; r < kItems; ++r) {
-            if (r * kSThreads >= tn) break;  // block-uniform
-            const int i = r * kSThreads + (int)threadIdx.x;
+        uint2 it[kItems];
+        uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const int i = k * kSThreads + threadIdx.x;
             if (i < tn) {
-                const uint2 e = in.item(buf, t0, i, tn, lay);
-                const uint32_t x = bin(e.x);
-                const uint32_t slot = atomicAdd(&fill[x], 1u);
-                if (slot < wcap) {
-                    wc[(size_t)x * wcap + slot] = e;
-                } else {
-                    const int64_t dst = cursor[x] + slot;  // reserved by this round's flush of bin x
-                    if ((uint64_t)dst < (uint64_t)out_limit) out[dst] = e;
-                    else atomicAdd(errors, 1ull);
-                }
+                it[k] = in.item(buf, t0, i, tn, lay);
+                const uint32_t bb = bin(it[k].x);
+                br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
             }
-            __syncthreads();
-            // every warp flushes the full buffers among its bins
-            for (int x0 = wid * 32; x0 < nbins; x0 += kWarps * 32) {
-                const int x = x0 + lane;
-                const uint32_t f = x < nbins ? fill[x] : 0u;
-                uint32_t m = __ballot_sync(0xffffffffu, f >= wcap);
-                while (m) {
-                    const int l = __ffs(m) - 1;
-                    m &= m - 1;
-                    flush_bin((uint32_t)(x0 + l), __shfl_sync(0xffffffffu, f, l));
-                }
+        }
+        __syncthreads();
+        block_scan_excl_n<kSThreads>(cnt, nbins, tmp);  // cnt[b] = first staged position of bin b
+        for (int x = threadIdx.x; x < nbins; x += kSThreads) {
+            const uint32_t e0 = cnt[x];
+            const uint32_t e1 = (x + 1 < nbins) ? cnt[x + 1] : (uint32_t)tn;
+            const int64_t c = cursor[x];
+            delta[x] = c - (int64_t)e0;
+            cursor[x] = c + (int64_t)(e1 - e0);
+        }
+        uint2* stage = reinterpret_cast<uint2*>(buf);
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const int i = k * kSThreads + threadIdx.x;
+            if (i < tn) {
+                const uint32_t bb = br[k] >> 16;
+                const uint32_t pos = cnt[bb] + (br[k] & 0xffffu);
+                stage[pos] = it[k];
+                sbin[pos] = (uint16_t)bb;
             }
-            __syncthreads();
+        }
+        __syncthreads();
+        for (int x = threadIdx.x; x < nbins; x += kSThreads) cnt[x] = 0;  // for the next tile
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const int i = k * kSThreads + threadIdx.x;
+            if (i < tn) {
+                const int64_t dst = delta[sbin[i]] + i;
+                if ((uint64_t)dst < (uint64_t)out_limit) out[dst] = stage[i];
+                else atomicAdd(errors, 1ull);
+            }
         }
     }
-    // the partly filled buffers
-    for (int x0 = wid * 32; x0 < nbins; x0 += kWarps * 32) {
-        const int x = x0 + lane;
-        const uint32_t f = x < nbins ? fill[x] : 0u;
-        uint32_t m = __ballot_sync(0xffffffffu, f > 0);
-        while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            flush_bin((uint32_t)(x0 + l), __shfl_sync(0xffffffffu, f, l));
-        }
-    }
-    __syncthreads();  // the buffers, cursor and fill are free for the next slice
+    __syncthreads();  // the last write pass is done with the buffers, cursor and cnt
 }
 
-// Shared-memory layout of the scatter kernels: two tile buffers, the write-combining buffers
-// (wc_tuples tuples: wcap per bin), then cursor (int64 per bin) and fill (uint32 per bin). wcap is the
-// largest power of two up to 16 whose buffers fit (16 for up to 512 bins; fewer for the rare larger
-// fan-outs, down to 1 at 4096 bins).
-constexpr int kWcTuples = 8192;
-constexpr size_t kScatterSmemMax = 232448 - 1024;  // 227 KB per CTA, less room for static shared memory
-__host__ __device__ __forceinline__ uint32_t wc_tuples(int max_bins) {
-    const int64_t room = ((int64_t)kScatterSmemMax - 2 * (int64_t)kTileBuf - (int64_t)max_bins * 12) / 8;
-    return (uint32_t)(room < kWcTuples ? (room > 0 ? room : 0) : kWcTuples);
-}
-__host__ __device__ __forceinline__ uint32_t wc_cap(int max_bins) {
-    const uint32_t room = wc_tuples(max_bins);
-    uint32_t w = 16;
-    while (w > 1 && (uint64_t)max_bins * w > room) w >>= 1;
-    return w;
-}
-__device__ __forceinline__ void scatter_carve(unsigned char* smem, int max_bins, unsigned char*& inbuf, uint2*& wc,
-                                              int64_t*& cursor, uint32_t*& fill) {
+// Shared-memory layout of the scatter kernels: two tile buffers, then cursor and delta (int64 per
+// bin), the bin counts (uint32 per bin) and the staged bins (uint16 per tile position).
+__device__ __forceinline__ void scatter_carve(unsigned char* smem, int max_bins, unsigned char*& inbuf,
+                                              int64_t*& cursor, int64_t*& delta, uint32_t*& cnt,
+                                              uint16_t*& sbin) {
     inbuf = smem;
-    wc = reinterpret_cast<uint2*>(smem + 2 * kTileBuf);
-    cursor = reinterpret_cast<int64_t*>(wc + wc_tuples(max_bins));
-    fill = reinterpret_cast<uint32_t*>(cursor + max_bins);
+    cursor = reinterpret_cast<int64_t*>(smem + 2 * kTileBuf);
+    delta = cursor + max_bins;
+    cnt = reinterpret_cast<uint32_t*>(delta + max_bins);
+    sbin = reinterpret_cast<uint16_t*>(cnt + max_bins);
 }
 
 __device__ __forceinline__ void init_bars(uint64_t* bars) {
@@ -604,11 +575,11 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
              const int64_t* __restrict__ scan, unsigned long long* gwords, int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* inbuf;
-    uint2* wc;
-    int64_t* cursor;
-    uint32_t* fill;
-    scatter_carve(smem, max_bins, inbuf, wc, cursor, fill);
-    const uint32_t wcap = wc_cap(max_bins);
+    int64_t *cursor, *delta;
+    uint32_t* cnt;
+    uint16_t* sbin;
+    scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
+    __shared__ uint32_t tmp[kSThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
     uint32_t ph = 0;
@@ -630,12 +601,12 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         __syncthreads();
         const Bin1<M> bin{d.pf};
         if constexpr (kPacked) {
-            scatter_tiles(PackedTiles{R.cmp}, b, e, bin, (int)P1, R.l1, R.n, cursor, wc, fill, wcap, inbuf, bars, ph,
-                          &gwords[kGErrors]);
+            scatter_tiles(PackedTiles{R.cmp}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf,
+                          bars, ph, &gwords[kGErrors]);
         } else {
             const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 3) == 0;
-            scatter_tiles(KvTiles{R.key, R.val, al}, b, e, bin, (int)P1, R.l1, R.n, cursor, wc, fill, wcap, inbuf,
-                          bars, ph, &gwords[kGErrors]);
+            scatter_tiles(KvTiles{R.key, R.val, al}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp,
+                          inbuf, bars, ph, &gwords[kGErrors]);
         }
     }
 }
@@ -832,11 +803,11 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
              int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* inbuf;
-    uint2* wc;
-    int64_t* cursor;
-    uint32_t* fill;
-    scatter_carve(smem, max_bins, inbuf, wc, cursor, fill);
-    const uint32_t wcap = wc_cap(max_bins);
+    int64_t *cursor, *delta;
+    uint32_t* cnt;
+    uint16_t* sbin;
+    scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
+    __shared__ uint32_t tmp[kSThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
     uint32_t ph = 0;
@@ -855,8 +826,8 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const int64_t* Sx = S2 + x.local_off * P2;
         for (uint32_t q = threadIdx.x; q < P2; q += kSThreads) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
         __syncthreads();
-        scatter_tiles(PackedTiles{bloom ? R.cmp : R.l1}, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2, R.n, cursor, wc,
-                      fill, wcap, inbuf, bars, ph, &gwords[kGErrors]);
+        scatter_tiles(PackedTiles{bloom ? R.cmp : R.l1}, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2,
+                      R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph, &gwords[kGErrors]);
     }
 }
 
@@ -1449,7 +1420,7 @@ size_t probe_smem_bytes(int table_cap, int emit_key) {
 // Shared memory of the scatter kernels: two bulk-copy tile buffers, the reordered tile, and a
 // cursor and a count per bin.
 static size_t scatter_smem(int max_bins) {
-    return 2 * kTileBuf + (size_t)wc_tuples(max_bins) * 8 + (size_t)max_bins * (8 + 4);
+    return 2 * kTileBuf + (size_t)max_bins * (8 + 8 + 4) + (size_t)kSTile * 2;
 }
 
 static cudaError_t set_smem_attr(const void* fn, size_t bytes) {
