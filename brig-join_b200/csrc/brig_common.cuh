@@ -105,12 +105,6 @@ BRIG_HD uint32_t part2_m(const PartFn& f, uint32_t key) {
     if constexpr (M == 0) return (uint32_t)(((uint64_t)(mix32(key) << f.b1) << f.b2) >> 32);
     else return fastmod(key, f.M2, f.P2);
 }
-// The level-2 id from an already computed m = mix32(key) (hash mode) or from the key (modulo).
-template <int M>
-BRIG_HD uint32_t part2_m_mixed(const PartFn& f, uint32_t key, uint32_t m) {
-    if constexpr (M == 0) return (uint32_t)(((uint64_t)(m << f.b1) << f.b2) >> 32);
-    else return fastmod(key, f.M2, f.P2);
-}
 // Finest partition id p * P2 + q: the probe-task unit and the Bloom segment index.
 template <int M>
 BRIG_HD uint32_t part_fine_m(const PartFn& f, uint32_t key) {
@@ -145,8 +139,7 @@ struct BloomKey {
 // The Bloom hash is mix32(key) (which the partition functions compute anyway) times an odd 64-bit
 // constant: multiplication by an odd constant is a bijection modulo every power of two, so each
 // field of the product is uniform when mix32(key) is, and the top bits depend on every input bit.
-constexpr uint64_t kBloomMul = 0x9e3779b97f4a7c15ull;
-BRIG_HD uint64_t bloom_hash(uint32_t key) { return (uint64_t)mix32(key) * kBloomMul; }
+BRIG_HD uint64_t bloom_hash(uint32_t key) { return (uint64_t)mix32(key) * 0x9e3779b97f4a7c15ull; }
 
 // Bits 40..63 of the hash pick the block (24-bit multiply-shift range reduction).
 BRIG_HD uint32_t bloom_block_of(uint64_t g, uint32_t seg_blocks) {

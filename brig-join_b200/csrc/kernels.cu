@@ -726,12 +726,10 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t* __restrict__ bloom = d.bloom;
             uint2* __restrict__ cmp = R.cmp;
             const uint32_t fbase = x.p * P2;
-            const PartFn pf = d.pf;
             const int32_t len = (int32_t)(end - begin);  // at most kL2Slice
             const uint2* __restrict__ src = l1 + begin;
             for (int32_t r0 = 0; r0 < len; r0 += kL2ProbeILP * kThreads) {
                 uint2 e[kL2ProbeILP];
-                uint32_t mx[kL2ProbeILP];  // mix32 of the key: the level-2 id and the Bloom hash
                 uint32_t va[kL2ProbeILP], vb[kL2ProbeILP];
 #pragma unroll
                 for (int u = 0; u < kL2ProbeILP; ++u) {
@@ -741,12 +739,10 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kL2ProbeILP; ++u) {
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
-                    mx[u] = mix32(e[u].x);
                     if (r < len) {
                         BloomKey bkey;
-                        bloom_place((uint64_t)mx[u] * kBloomMul, seg_blocks, bkey);
-                        const uint32_t* w =
-                            bloom_words(bloom, seg_blocks, fbase + part2_m_mixed<M>(pf, e[u].x, mx[u]), bkey.block);
+                        bloom_place(bloom_hash(e[u].x), seg_blocks, bkey);
+                        const uint32_t* w = bloom_words(bloom, seg_blocks, fbase + bin(e[u].x), bkey.block);
                         const uint2 pair = __ldg(reinterpret_cast<const uint2*>(w + bkey.wa));
                         va[u] = pair.x;
                         vb[u] = pair.y;
@@ -758,7 +754,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
                     if (r < len) {
                         uint32_t ma, mb;
-                        key_masks<K>(s_pat, (uint64_t)mx[u] * kBloomMul, bk, ma, mb);
+                        key_masks<K>(s_pat, bloom_hash(e[u].x), bk, ma, mb);
                         if ((va[u] & ma) == ma && (vb[u] & mb) == mb) pm |= 1u << u;
                     }
                 }
@@ -777,7 +773,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                     for (int u = 0; u < kL2ProbeILP; ++u) {
                         if ((pm >> u) & 1u) {
-                            atomicAdd(&cnt[part2_m_mixed<M>(pf, e[u].x, mx[u])], 1u);
+                            atomicAdd(&cnt[bin(e[u].x)], 1u);
                             const int64_t dst = begin + base + __popc(bal[u] & lanemask_lt());
                             if (dst < end) cmp[dst] = e[u];
                             else atomicAdd(&gwords[kGErrors], 1ull);
