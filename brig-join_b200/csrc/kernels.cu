@@ -163,6 +163,15 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
+// Asks the TMA unit to bring [p, p + bytes) into L2 (a hint; no data is returned). The range is
+// shrunk to whole 16-byte units inside [lo, hi), so nothing outside the buffer is touched.
+__device__ __forceinline__ void prefetch_l2_range(const void* lo, const void* hi) {
+    const uintptr_t a = ((uintptr_t)lo + 15) & ~(uintptr_t)15, b = (uintptr_t)hi & ~(uintptr_t)15;
+    if (b > a) {
+        const uint32_t bytes = (uint32_t)min_i64((int64_t)(b - a), 1 << 20);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(bytes) : "memory");
+    }
+}
 // Orders this thread's earlier shared-memory accesses before later async-proxy (bulk copy) writes.
 __device__ __forceinline__ void fence_proxy_async() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1167,7 +1176,11 @@ __device__ __forceinline__ void probe_stream(const JoinDesc& d, const uint2* __r
                                              const uint32_t* bitmap, uint2* q, int& qn, const uint2* table,
                                              const uint32_t* off, uint32_t mask, bool bs, int emit_key, int lane,
                                              WarpOut& o) {
-    for (uint32_t base = 0; base < n; base += (uint32_t)(U * kThreads)) {
+    constexpr uint32_t kStep = (uint32_t)(U * kThreads);
+    for (uint32_t base = 0; base < n; base += kStep) {
+        // streamed from global memory: keep the range two iterations ahead on its way into L2
+        if (!kShared && threadIdx.x == 0 && base + 2 * kStep < n)
+            prefetch_l2_range(src + base + 2 * kStep, src + min_i64((int64_t)n, (int64_t)base + 3 * kStep));
         uint2 e[U];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
@@ -1247,6 +1260,9 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         if (threadIdx.x == 0) {
             s_task[slot ^ 1] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
             PackedTiles{psrc}.issue(0, (int)first, reinterpret_cast<unsigned char*>(pbuf), &bar);
+            // the first two global iterations of the probe side go to L2 while the table is built
+            if (pn > first)
+                prefetch_l2_range(psrc + first, psrc + min_i64((int64_t)pn, (int64_t)first + 2 * kProbeU * kThreads));
         }
         if (tk.join != cur) {
             if (cur >= 0 && o.count > 0) warp_flush(J[cur], o.wr, o.ws, o.wk, o.count, lane);
