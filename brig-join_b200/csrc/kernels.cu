@@ -456,12 +456,8 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                 if ((int64_t)threadIdx.x < head) atomicAdd(&sh_cnt[part1_m<M>(pf, __ldcs(key + b + threadIdx.x))], 1u);
                 const int64_t b4 = b + head;  // 16-byte aligned
                 int64_t i = b4 + 4 * (int64_t)threadIdx.x;
-                constexpr int64_t kStep = 16 * kThreads;  // keys per iteration of the CTA
-                if (threadIdx.x == 0) prefetch_l2_range(key + b4, key + min_i64(e, b4 + 2 * kStep));
-                // four 16-byte loads in flight per thread, the slice two iterations ahead into L2
-                for (; i + 12 * kThreads + 3 < e; i += kStep) {
-                    if (threadIdx.x == 0 && i + 2 * kStep < e)
-                        prefetch_l2_range(key + i + 2 * kStep, key + min_i64(e, i + 3 * kStep));
+                // four 16-byte loads in flight per thread
+                for (; i + 12 * kThreads + 3 < e; i += 16 * kThreads) {
                     uint4 k4[4];
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
@@ -721,12 +717,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         __syncthreads();
         const uint2* __restrict__ l1 = R.l1;
         if constexpr (!kBloom) {
-            constexpr int64_t kStep = 8 * kThreads;
-            if (threadIdx.x == 0) prefetch_l2_range(l1 + begin, l1 + min_i64(end, begin + 2 * kStep));
-            for (int64_t i0 = begin + threadIdx.x; i0 < end; i0 += kStep) {
-                // keep the slice two iterations ahead on its way into L2
-                if (threadIdx.x == 0 && i0 + 2 * kStep < end)
-                    prefetch_l2_range(l1 + i0 + 2 * kStep, l1 + min_i64(end, i0 + 3 * kStep));
+            for (int64_t i0 = begin + threadIdx.x; i0 < end; i0 += 8 * kThreads) {
                 uint32_t kk[8];
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
@@ -746,11 +737,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t fbase = x.p * P2;
             const int32_t len = (int32_t)(end - begin);  // at most kL2Slice
             const uint2* __restrict__ src = l1 + begin;
-            constexpr int32_t kStep = kL2ProbeILP * kThreads;
-            if (threadIdx.x == 0) prefetch_l2_range(src, src + min(len, 2 * kStep));
-            for (int32_t r0 = 0; r0 < len; r0 += kStep) {
-                if (threadIdx.x == 0 && r0 + 2 * kStep < len)
-                    prefetch_l2_range(src + r0 + 2 * kStep, src + min(len, r0 + 3 * kStep));
+            for (int32_t r0 = 0; r0 < len; r0 += kL2ProbeILP * kThreads) {
                 uint2 e[kL2ProbeILP];
                 uint32_t va[kL2ProbeILP], vb[kL2ProbeILP];
 #pragma unroll
