@@ -1101,30 +1101,30 @@ __device__ __forceinline__ void warp_flush(const JoinDesc& d, const uint32_t* wr
 
 // Persistent probe kernel, two CTAs per SM. Each CTA takes tasks from the global queue (the next
 // task index is fetched while the current task runs). Per task the CTA
-//   * loads the build chunk (at most table_cap tuples) into registers, kBuildPer per thread, counts
-//     it per bucket with one shared-memory atomic per tuple (the atomic's result is the tuple's rank
-//     in its bucket), scans the counts into bucket starts (off[nb] = the chunk size) and places
-//     every tuple at off[bucket] + rank: a bucketised table, bucket b = [off[b], off[b+1]). Every
-//     build key also sets one bit of a presence bitmap of 16 bits per build tuple (1024 to 65536 bits);
+//   * loads the build chunk (at most table_cap tuples) once, into registers, kBuildPer per thread,
+//     counts it per bucket with one shared-memory atomic per tuple (the atomic's result is the
+//     tuple's rank in its bucket), scans the counts into bucket starts (off[nb] = the chunk size)
+//     and places every tuple at off[bucket] + rank: a bucketised table with at least as many
+//     buckets as tuples, bucket b = [off[b], off[b+1]). Every build key also sets one bit of a
+//     65536-bit presence bitmap;
 //   * streams the other side: its first kProbeFirst tuples from shared memory, where a bulk copy
 //     issued at the start of the task has put them while the table was built, the rest straight
-//     from global memory with kProbeU coalesced tuples per thread in flight. (The build side is
-//     loaded once, into registers.) A streamed tuple whose bitmap bit is clear cannot match (16 bits per key set at
-//     most 6% of the bits); the others are compacted with ballot/popc into the warp's candidate
-//     queue in shared memory. Every 32 queued candidates the warp scans their buckets in lock step,
-//     one candidate per lane, and compacts matches into the warp's output staging buffer, which is
-//     written out with one global atomic per flush. So the bucket scans, whose cost is the longest
-//     bucket among the lanes, run only on full warps of likely matches.
+//     from global memory with kProbeU coalesced tuples per thread in flight (and the range two
+//     iterations ahead prefetched into L2). A streamed tuple whose bitmap bit is clear cannot match
+//     (at most 4096 keys set at most 6% of the bits); the others are compacted with ballot/popc into
+//     the warp's candidate queue in shared memory. Every 32 queued candidates the warp scans their
+//     buckets in lock step, one candidate per lane, and compacts matches into the warp's output
+//     staging buffer, which is written out with one global atomic per flush. So the bucket scans,
+//     whose cost is the longest bucket among the lanes, run only on full warps of likely matches.
 // The bitmap index is a multiplicative hash of the key, independent of the partition bits (the
 // keys of one task share the top bits of mix32) and of the bucket bits.
 constexpr int kProbeU = 4;                        // streamed tuples per thread in flight
 constexpr int kBuildPer = kMaxTable / kThreads;   // build tuples per thread
-constexpr int kBitmapWords = 2048;                // presence bitmap capacity: 65536 bits
+constexpr int kBitmapWords = 2048;                // 65536-bit presence bitmap
 constexpr int kQueue = 64;                        // candidates queued per warp
 constexpr int kProbeFirst = 2048;                 // first probe-side tuples of a task, bulk-copied
 
-// Bit of a key in a presence bitmap of 2^(32 - shift) bits.
-__device__ __forceinline__ uint32_t presence_bit(uint32_t key, uint32_t shift) { return (key * 0x9E3779B1u) >> shift; }
+__device__ __forceinline__ uint32_t presence_bit(uint32_t key) { return (key * 0x9E3779B1u) >> 16; }
 
 // Output staging of one warp: the pairs found so far for join `d`.
 struct WarpOut {
@@ -1178,8 +1178,7 @@ __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2*
 // the warp's candidate queue; full warps of candidates are probed as they form.
 template <bool kShared, int U>
 __device__ __forceinline__ void probe_stream(const JoinDesc& d, const uint2* __restrict__ src, uint32_t n,
-                                             const uint32_t* bitmap, uint32_t pshift, uint2* q, int& qn,
-                                             const uint2* table,
+                                             const uint32_t* bitmap, uint2* q, int& qn, const uint2* table,
                                              const uint32_t* off, uint32_t mask, bool bs, int emit_key, int lane,
                                              WarpOut& o) {
     constexpr uint32_t kStep = (uint32_t)(U * kThreads);
@@ -1199,7 +1198,7 @@ __device__ __forceinline__ void probe_stream(const JoinDesc& d, const uint2* __r
             const uint32_t i = base + u * kThreads + threadIdx.x;
             bool cand = false;
             if (i < n) {
-                const uint32_t pb = presence_bit(e[u].x, pshift);
+                const uint32_t pb = presence_bit(e[u].x);
                 cand = (bitmap[pb >> 5] >> (pb & 31u)) & 1u;
             }
             const uint32_t cm = __ballot_sync(0xffffffffu, cand);
@@ -1280,19 +1279,12 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
             if (threadIdx.x == 0) atomicAdd(errors, 1ull);
             nr = table_cap;
         }
-        // About two tuples per bucket and 16 bitmap bits per tuple (1024 to 65536 bits): the
-        // per-task clearing and scanning scale with the build chunk.
-        uint32_t np2 = 32;
-        while (np2 < (uint32_t)nr) np2 <<= 1;
-        const uint32_t nb = np2 >> 1 > 32 ? np2 >> 1 : 32;
+        uint32_t nb = 32;
+        while (nb < (uint32_t)nr) nb <<= 1;
         const uint32_t mask = nb - 1;
-        uint32_t lbits = 10;
-        while (lbits < 16 && (1u << lbits) < 16u * np2) ++lbits;
-        const uint32_t pshift = 32 - lbits;
-        const int bwords = (int)((1u << lbits) >> 5);
         // the previous task's probe is done with table, off, bitmap and pbuf
         for (uint32_t i = threadIdx.x; i <= nb; i += kThreads) off[i] = 0;
-        for (int i = threadIdx.x; i < bwords; i += kThreads) bitmap[i] = 0;
+        for (int i = threadIdx.x; i < kBitmapWords; i += kThreads) bitmap[i] = 0;
         // ---- build: count per bucket (the atomic's result is the rank), set the bitmap bits
         uint2 bt[kBuildPer];
 #pragma unroll
@@ -1308,7 +1300,7 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
             if (i < nr) {
                 const uint32_t bk = bucket_of(bt[k].x, mask);
                 br[k] = (bk << 16) | atomicAdd(&off[bk], 1u);
-                const uint32_t pb = presence_bit(bt[k].x, pshift);
+                const uint32_t pb = presence_bit(bt[k].x);
                 atomicOr(&bitmap[pb >> 5], 1u << (pb & 31u));
             }
         }
@@ -1324,11 +1316,10 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         __syncthreads();
         // ---- probe: the first chunk from shared memory, the rest straight from global memory
         int qn = 0;  // candidates in this warp's queue (warp-uniform)
-        probe_stream<true, 2>(d, pbuf + PackedTiles{psrc}.mis(0), first, bitmap, pshift, q, qn, table, off, mask, bs,
-                              emit_key, lane, o);
+        probe_stream<true, 2>(d, pbuf + PackedTiles{psrc}.mis(0), first, bitmap, q, qn, table, off, mask, bs,
+                           emit_key, lane, o);
         if (pn > first)
-            probe_stream<false, kProbeU>(d, psrc + first, pn - first, bitmap, pshift, q, qn, table, off, mask, bs,
-                                         emit_key, lane, o);
+            probe_stream<false, kProbeU>(d, psrc + first, pn - first, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
         if (qn > 0) probe_candidates(d, q, qn, table, off, mask, bs, emit_key, lane, o);
         __syncwarp();
         __syncthreads();
