@@ -1099,6 +1099,51 @@ __device__ __forceinline__ void warp_flush(const JoinDesc& d, const uint32_t* wr
     __syncwarp();
 }
 
+// Exclusive scan of the bucket directory off[0, nb) for nb = PER * kThreads (PER a multiple of 4):
+// each thread scans PER consecutive entries with 16-byte
+// shared-memory accesses. off[nb] is set to the total.
+template <int PER>
+__device__ __forceinline__ void scan_dir(uint32_t* off, uint32_t nb, uint32_t* tmp) {
+    static_assert(PER % 4 == 0, "16-byte accesses");
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    constexpr int kWarps = kThreads / 32;
+    uint4 v[PER / 4];
+    uint4* p = reinterpret_cast<uint4*>(off + threadIdx.x * PER);
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < PER / 4; ++k) {
+        v[k] = p[k];
+        sum += v[k].x + v[k].y + v[k].z + v[k].w;
+    }
+    uint32_t x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) tmp[wid] = x;
+    __syncthreads();
+    uint32_t w = lane < kWarps ? tmp[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, w, kWarps - 1);
+    uint32_t run = x - sum + (wid > 0 ? __shfl_sync(0xffffffffu, w, wid - 1) : 0u);
+#pragma unroll
+    for (int k = 0; k < PER / 4; ++k) {
+        uint4 o4;
+        o4.x = run; run += v[k].x;
+        o4.y = run; run += v[k].y;
+        o4.z = run; run += v[k].z;
+        o4.w = run; run += v[k].w;
+        p[k] = o4;
+    }
+    if (threadIdx.x == 0) off[nb] = total;
+    __syncthreads();
+}
+
 // Persistent probe kernel, two CTAs per SM. Each CTA takes tasks from the global queue (the next
 // task index is fetched while the current task runs). Per task the CTA
 //   * loads the build chunk (at most table_cap tuples) once, into registers, kBuildPer per thread,
@@ -1305,7 +1350,10 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
             }
         }
         __syncthreads();
-        block_scan_excl(off, (int)nb + 1, tmp);  // off[b] = start of bucket b, off[nb] = nr
+        // off[b] = start of bucket b, off[nb] = nr
+        if (nb == 8 * kThreads) scan_dir<8>(off, nb, tmp);
+        else if (nb == 4 * kThreads) scan_dir<4>(off, nb, tmp);
+        else block_scan_excl(off, (int)nb + 1, tmp);
 #pragma unroll
         for (int k = 0; k < kBuildPer; ++k) {
             const int i = k * kThreads + threadIdx.x;
