@@ -28,6 +28,9 @@ static int ceil_log2(int64_t x) {
 }
 static bool is_pow2(int64_t x) { return x > 0 && (x & (x - 1)) == 0; }
 
+// Filter bytes that a first-pass Bloom probe may touch and still find in L2.
+constexpr int64_t kL2FilterBytes = 64ll << 20;
+
 JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
     JoinPlan p;
     p.nr = nr;
@@ -103,7 +106,6 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
         // Probing in S's first pass reads one random 32-byte block per S tuple; that is cheap only
         // while the filter stays in the 126 MB L2. A larger filter is probed in S's second pass,
         // one level-1 partition (a contiguous run of segments) at a time.
-        const int64_t kL2FilterBytes = 64ll << 20;
         int lvl = cfg.bloom_probe_level;
         if (lvl == 0) lvl = (p.bloom_bits / 8 <= kL2FilterBytes) ? 1 : 2;
         if (lvl != 1 && lvl != 2) fail(BRIG_E_INVALID, "bloom_probe_level must be 0, 1 or 2");
@@ -111,6 +113,30 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
         p.bloom_level = lvl;
     }
     return p;
+}
+
+std::vector<JoinPlan> plan_batch(const brig_join_config& cfg, const int64_t* nr, const int64_t* ns, int nj) {
+    std::vector<JoinPlan> plans(nj);
+    for (int j = 0; j < nj; ++j) plans[j] = plan_join(cfg, nr[j], ns[j]);
+    if (cfg.bloom_probe_level != 0) return plans;
+    // One first-pass probe launch covers every join of the batch, so their filters share L2.
+    // While they do not fit, the largest joins that have a second pass probe there instead.
+    int64_t l1 = 0;
+    std::vector<int> movable;
+    for (int j = 0; j < nj; ++j) {
+        const JoinPlan& p = plans[j];
+        if (!p.bloom || p.bloom_level != 1) continue;
+        l1 += p.bloom_bits / 8;
+        if (p.pf.P2 > 1) movable.push_back(j);
+    }
+    std::stable_sort(movable.begin(), movable.end(),
+                     [&](int a, int b) { return plans[a].bloom_bits > plans[b].bloom_bits; });
+    for (int j : movable) {
+        if (l1 <= kL2FilterBytes) break;
+        plans[j].bloom_level = 2;
+        l1 -= plans[j].bloom_bits / 8;
+    }
+    return plans;
 }
 
 // ---- workspace layout ---------------------------------------------------------------------------
@@ -133,14 +159,23 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
     sh = Shape{};
     sh.jo = jo;
     for (int j = 0; j < nj; ++j) jo[j] = JoinOffs{};
-    int64_t total_tuples = 0;
-    for (int j = 0; j < nj; ++j) total_tuples += plans[j].nr + plans[j].ns;
-    // Slices of about total/(8 * SMs) tuples, a multiple of the scatter tile, at least 2 tiles.
-    const int64_t target = (int64_t)num_sms * 8;
-    int64_t sl = (total_tuples + target - 1) / std::max<int64_t>(target, 1);
-    sl = ((sl + kSTile - 1) / kSTile) * kSTile;
-    sl = std::max<int64_t>(sl, 2 * kSTile);
-    sh.slice_len = sl;
+    // Level-1 slice length per launch class: R; S probed by the Bloom filter in its first pass;
+    // the other S. Each class is one launch over all joins of the run that deals slices to CTAs
+    // round-robin, so a class of n tuples is cut into about W x SMs slices (a multiple of the
+    // scatter tile, at least 2 tiles): W = 4 for one join, whose slices are then equal, and 16 for
+    // a batch, where every join ends in a partial slice and finer slices keep the CTAs' shares even.
+    int64_t class_tuples[3] = {0, 0, 0};
+    auto slice_class = [](const JoinPlan& p, int r) { return r == 0 ? 0 : (p.bloom && p.bloom_level == 1 ? 1 : 2); };
+    for (int j = 0; j < nj; ++j)
+        for (int r = 0; r < 2; ++r) class_tuples[slice_class(plans[j], r)] += r == 0 ? plans[j].nr : plans[j].ns;
+    const int64_t target = (int64_t)std::max(num_sms, 1) * (nj > 1 ? 16 : 4);
+    int64_t class_sl[3];
+    for (int c = 0; c < 3; ++c) {
+        int64_t sl = (class_tuples[c] + target - 1) / target;
+        sl = ((sl + kSTile - 1) / kSTile) * kSTile;
+        class_sl[c] = std::max<int64_t>(sl, 2 * kSTile);
+    }
+    sh.slice_len = class_sl[0];
     const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
     const int C = cfg.s_chunk > 0 ? cfg.s_chunk : kDefaultChunk;
     Layout L;
@@ -153,6 +188,7 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
         sh.max_p2 = std::max<int>(sh.max_p2, (int)p.pf.P2);
         for (int r = 0; r < 2; ++r) {
             RelOffs& ro = o.rel[r];
+            const int64_t sl = class_sl[slice_class(p, r)];
             ro.slice_len = sl;
             ro.nslices = (int32_t)std::max<int64_t>(1, (n[r] + sl - 1) / sl);
             ro.l1 = L.take((size_t)std::max<int64_t>(n[r], 1) * 8);
@@ -493,8 +529,12 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
 void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph) {
     const int nj = (int)joins.size();
     if (nj <= 0) fail(BRIG_E_INVALID, "no joins");
-    std::vector<JoinPlan> plans(nj);
-    for (int j = 0; j < nj; ++j) plans[j] = plan_join(cfg_, joins[j].nr, joins[j].ns);
+    std::vector<int64_t> nr(nj), ns(nj);
+    for (int j = 0; j < nj; ++j) {
+        nr[j] = joins[j].nr;
+        ns[j] = joins[j].ns;
+    }
+    std::vector<JoinPlan> plans = plan_batch(cfg_, nr.data(), ns.data(), nj);
     std::vector<JoinOffs> jo(nj);
     Shape sh;
     layout_for(cfg_, plans.data(), nj, num_sms_, jo.data(), sh);

@@ -1179,7 +1179,36 @@ struct WarpOut {
     int count;
 };
 
+// Stages one match per lane with m set (warp-wide; flushes first when the staging buffer is full).
+__device__ __forceinline__ void stage_matches(const JoinDesc& d, bool m, uint32_t r_val, uint32_t s_val,
+                                              uint32_t key, int emit_key, int lane, WarpOut& o) {
+    const uint32_t mm = __ballot_sync(0xffffffffu, m);
+    if (!mm) return;
+    const int c = __popc(mm);
+    if (o.count + c > kWarpBuf) {
+        warp_flush(d, o.wr, o.ws, o.wk, o.count, lane);
+        o.count = 0;
+    }
+    if (m) {
+        const int pos = o.count + __popc(mm & lanemask_lt());
+        o.wr[pos] = r_val;
+        o.ws[pos] = s_val;
+        if (emit_key) o.wk[pos] = key;
+    }
+    o.count += c;
+    __syncwarp();
+}
+
+// Longest bucket the lanes scan in lock step; a warp with a longer one spreads the entries of all
+// its buckets over the lanes instead (duplicate-heavy build keys, e.g. Zipf-skewed matches).
+constexpr uint32_t kLockstepMax = 8;
+
 // The warp scans the buckets of candidates q[0, n) (n <= 32), one per lane, and stages every match.
+// Short buckets are scanned in lock step, one entry per lane per step, so the warp takes as many
+// steps as its longest bucket. When that exceeds kLockstepMax the warp instead walks the
+// concatenation of all its buckets 32 entries at a time: a warp prefix sum of the bucket lengths,
+// and per entry a five-step shuffle binary search for the candidate that owns it. A key repeated k
+// times on the build side then costs about k/32 steps instead of k.
 __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2* q, int n, const uint2* table,
                                                  const uint32_t* off, uint32_t mask, bool bs, int emit_key,
                                                  int lane, WarpOut& o) {
@@ -1191,6 +1220,39 @@ __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2*
         lo = off[bk];
         hi = off[bk + 1];
     }
+    const uint32_t len = hi - lo;
+    if (__reduce_max_sync(0xffffffffu, len) > kLockstepMax) {
+        uint32_t inc = len;  // inclusive prefix of the bucket lengths over the lanes
+#pragma unroll
+        for (int s = 1; s < 32; s <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, s);
+            if (lane >= s) inc += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+        for (uint32_t base = 0; base < total; base += 32) {
+            const uint32_t g = base + (uint32_t)lane;
+            // owner: the first lane c with inc[c] > g (lanes with empty buckets are skipped over)
+            int c = 0;
+#pragma unroll
+            for (int s = 16; s > 0; s >>= 1) {
+                const uint32_t v = __shfl_sync(0xffffffffu, inc, c + s - 1);
+                if (v <= g) c += s;
+            }
+            const uint32_t c_lo = __shfl_sync(0xffffffffu, lo, c);
+            const uint32_t c_start = __shfl_sync(0xffffffffu, inc - len, c);
+            const uint32_t c_key = __shfl_sync(0xffffffffu, e.x, c);
+            const uint32_t c_val = __shfl_sync(0xffffffffu, e.y, c);
+            bool m = false;
+            uint32_t rv = 0;
+            if (g < total) {
+                const uint2 cc = table[c_lo + (g - c_start)];
+                m = (cc.x == c_key);
+                rv = cc.y;
+            }
+            stage_matches(d, m, bs ? c_val : rv, bs ? rv : c_val, c_key, emit_key, lane, o);
+        }
+        return;
+    }
     while (__any_sync(0xffffffffu, lo < hi)) {
         bool m = false;
         uint32_t rv = 0;
@@ -1200,22 +1262,7 @@ __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2*
             rv = cc.y;
             ++lo;
         }
-        const uint32_t mm = __ballot_sync(0xffffffffu, m);
-        if (mm) {
-            const int c = __popc(mm);
-            if (o.count + c > kWarpBuf) {
-                warp_flush(d, o.wr, o.ws, o.wk, o.count, lane);
-                o.count = 0;
-            }
-            if (m) {
-                const int pos = o.count + __popc(mm & lanemask_lt());
-                o.wr[pos] = bs ? e.y : rv;
-                o.ws[pos] = bs ? rv : e.y;
-                if (emit_key) o.wk[pos] = e.x;
-            }
-            o.count += c;
-            __syncwarp();
-        }
+        stage_matches(d, m, bs ? e.y : rv, bs ? rv : e.y, e.x, emit_key, lane, o);
     }
 }
 

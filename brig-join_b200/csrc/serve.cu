@@ -76,10 +76,12 @@ struct Server {
         return Engine::workspace_needed(jcfg, {p}, num_sms) + io_bytes(r, cap);
     }
     int64_t wave_workspace(const std::vector<Req*>& w) const {
-        std::vector<JoinPlan> plans;
-        plans.reserve(w.size());
-        for (Req* q : w) plans.push_back(plan_join(jcfg, q->in.n_r, q->in.n_s));
-        return Engine::workspace_needed(jcfg, plans, num_sms);
+        std::vector<int64_t> nr, ns;
+        for (Req* q : w) {
+            nr.push_back(q->in.n_r);
+            ns.push_back(q->in.n_s);
+        }
+        return Engine::workspace_needed(jcfg, plan_batch(jcfg, nr.data(), ns.data(), (int)w.size()), num_sms);
     }
 
     // Request buffers are stream-ordered allocations on the slot's stream, so allocating and

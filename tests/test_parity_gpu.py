@@ -135,6 +135,24 @@ def test_zipf_skewed_probe_side(bj, oracle, torch_cuda):
     assert st.count == 80_000
 
 
+@pytest.mark.parametrize("build_side", ["r", "s"])
+def test_long_and_short_buckets_in_one_warp(bj, oracle, torch_cuda, build_side):
+    """Build chunks holding a few keys repeated hundreds of times among unique keys: warps whose
+    candidates mix long and short buckets take the load-balanced bucket walk."""
+    rng = np.random.default_rng(5)
+    uniq = rng.permutation(np.arange(1, 200_001, dtype=np.uint32))
+    hot = np.repeat(np.array([7, 1_000_003, 0x80000000, 0xFFFFFFFF], np.uint32), [900, 300, 40, 9])
+    small = np.concatenate([uniq[:30_000], hot])
+    big = np.concatenate([uniq[10_000:150_000], np.array([7, 0x80000000, 0xFFFFFFFF, 5], np.uint32)])
+    small = small[rng.permutation(len(small))]
+    big = big[rng.permutation(len(big))]
+    rk, sk = (small, big) if build_side == "r" else (big, small)
+    rv = np.arange(len(rk), dtype=np.uint32)
+    sv = np.arange(len(sk), dtype=np.uint32) + 3
+    for bloom in (0, 1):
+        _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=bloom, table_capacity=1024, emit_key=True)
+
+
 def test_handle_reuse_and_graph_replay(bj, oracle, torch_cuda):
     with bj.Join(use_bloom=1, use_cuda_graph=1) as j:
         for seed in (1, 2, 3):
