@@ -176,6 +176,18 @@ __device__ __forceinline__ void prefetch_l2_range(const void* lo, const void* hi
 __device__ __forceinline__ void fence_proxy_async() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+// Shared -> global bulk copy of `bytes` (a multiple of 16; both addresses 16-byte aligned), tracked
+// in this thread's bulk async-group.
+__device__ __forceinline__ void bulk_s2g(void* gdst, const void* ssrc, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(ssrc)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until this thread's committed bulk stores have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Waits until this thread's committed bulk stores have completed their global writes.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -370,6 +382,130 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
     __syncthreads();  // the last write pass is done with the buffers, cursor and cnt
 }
 
+// The same scatter for at most kBulkMaxBins bins, with each bin's run of a tile written by the
+// bulk-copy engine instead of a write pass over the tile. Thread x owns bin x. Per tile:
+//   1. every thread takes its tuples from the tile buffer into registers and ranks them within
+//      their bins (one shared-memory atomic each);
+//   2. a scan of the bin counts gives each bin its staged start: bin b gets count + 1 slots, and
+//      its run starts on the slot whose parity equals the parity of its output position, so the
+//      run's source and destination are 16-byte aligned together;
+//   3. every tuple is written to its staged slot (the tile's own buffer, free once the tuples are
+//      in registers);
+//   4. the owner of bin b stores the run [o, o + n) of b: a lone first tuple when o is odd and a
+//      lone last tuple when the rest is odd, with plain 8-byte stores, and the pairs between them
+//      with one shared -> global bulk copy.
+// There is no pass that reads the staged tile back through the registers, so shared memory sees
+// the staging stores and the bulk engine's reads only. The next tile's load goes into the other
+// buffer once the bulk copies of the tile that used it have finished reading it (checked after
+// step 1, by when they normally have).
+constexpr int kBulkMaxBins = 1024;
+static_assert(kBulkMaxBins <= kSThreads, "one bin per thread");
+// One tile buffer of the bulk scatter: the tile plus one slot per bin, a multiple of 16 bytes.
+__host__ __device__ constexpr size_t bulk_tile_buf(int max_bins) {
+    return (size_t)((kSTile + max_bins + 2 + 1) & ~1) * 8;
+}
+
+template <class In, class Bin>
+__device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
+                                   uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, uint32_t* cnt,
+                                   uint32_t* spos, uint32_t* tmp, unsigned char* inbuf, size_t buf_stride,
+                                   uint64_t* bars, uint32_t& ph, unsigned long long* errors) {
+    constexpr int kItems = kSTile / kSThreads;
+    constexpr int kWarps = kSThreads / 32;
+    const int64_t ntiles = (end - begin + kSTile - 1) / kSTile;
+    if (ntiles <= 0) return;
+    const int x = threadIdx.x, lane = x & 31, wid = x >> 5;
+    const bool owner = x < nbins;
+    if (owner) cnt[x] = 0;
+    if (x == 0) in.issue(begin, (int)min_i64(kSTile, end - begin), inbuf, &bars[0]);
+    __syncthreads();  // cnt is zero
+    for (int64_t t = 0; t < ntiles; ++t) {
+        const int64_t t0 = begin + t * kSTile;
+        const int tn = (int)min_i64(kSTile, end - t0);
+        const int b = (int)(t & 1);
+        mbar_wait(&bars[b], (ph >> b) & 1u, errors);
+        ph ^= 1u << b;
+        unsigned char* buf = inbuf + b * buf_stride;
+        const auto lay = in.layout(t0, tn);
+        uint2 it[kItems];
+        uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const int i = k * kSThreads + x;
+            if (i < tn) {
+                it[k] = in.item(buf, t0, i, tn, lay);
+                const uint32_t bb = bin(it[k].x);
+                br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
+            }
+        }
+        bulk_wait_read();  // this thread's bulk stores of the previous tile have read buffer b ^ 1
+        __syncthreads();
+        if (x == 0 && t + 1 < ntiles)
+            in.issue(t0 + kSTile, (int)min_i64(kSTile, end - t0 - kSTile), inbuf + (b ^ 1) * buf_stride, &bars[b ^ 1]);
+        // exclusive scan of the counts, one bin per thread (every warp scans the warp totals itself);
+        // cursor[x] (the next output position of bin x) and spos[x] (staged start | count << 16)
+        // stay in shared memory until the owner stores the run, which keeps registers free for the
+        // tuples held across the scan
+        const uint32_t n = owner ? cnt[x] : 0u;
+        if (owner) cnt[x] = 0;  // for the next tile (its ranks may start before this tile's stores)
+        uint32_t inc = n;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) tmp[wid] = inc;
+        __syncthreads();
+        uint32_t w = lane < kWarps ? tmp[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        const uint32_t wbase = __shfl_sync(0xffffffffu, w, (wid + 31) & 31);
+        const uint32_t e0 = inc - n + (wid > 0 ? wbase : 0u);
+        if (owner) {
+            const uint32_t base = e0 + (uint32_t)x;                              // bin x owns n + 1 slots
+            spos[x] = (base + ((base ^ (uint32_t)cursor[x]) & 1u)) | (n << 16);  // same parity as its output
+        }
+        __syncthreads();
+        uint2* stage = reinterpret_cast<uint2*>(buf);
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const int i = k * kSThreads + x;
+            if (i < tn) stage[(spos[br[k] >> 16] & 0xffffu) + (br[k] & 0xffffu)] = it[k];
+        }
+        fence_proxy_async();  // the staging stores before the bulk engine reads them
+        __syncthreads();
+        if (owner) {
+            const uint32_t sp = spos[x];
+            const uint32_t n = sp >> 16, s = sp & 0xffffu;
+            const int64_t o = cursor[x];
+            cursor[x] = o + n;
+            if (n == 0) {
+            } else if (o < 0 || o + (int64_t)n > out_limit) {
+                atomicAdd(errors, 1ull);
+            } else {
+                const uint32_t h = (uint32_t)(o & 1);  // a lone first tuple
+                const uint32_t m = n - h;
+                const uint32_t pairs = m >> 1;
+                const bool aligned = ((((uintptr_t)(out + o + h)) | (uintptr_t)smem_u32(stage + s + h)) & 15u) == 0;
+                if (h) out[o] = stage[s];
+                if (aligned) {
+                    if (pairs) bulk_s2g(out + o + h, stage + s + h, pairs * 16u);
+                } else {
+                    for (uint32_t i = 0; i < 2 * pairs; ++i) out[o + h + i] = stage[s + h + i];
+                }
+                if (m & 1u) out[o + n - 1] = stage[s + n - 1];
+            }
+        }
+        bulk_commit();
+    }
+    bulk_wait_read();
+    __syncthreads();  // the bulk stores are done with the buffers; cnt is zero
+}
+static_assert(kSTile + kBulkMaxBins + 2 < (1 << 16) && kSTile < (1 << 16), "staged start and count in 16 bits");
+
 // Shared-memory layout of the scatter kernels: two tile buffers, then cursor and delta (int64 per
 // bin), the bin counts (uint32 per bin) and the staged bins (uint16 per tile position).
 __device__ __forceinline__ void scatter_carve(unsigned char* smem, int max_bins, unsigned char*& inbuf,
@@ -380,6 +516,16 @@ __device__ __forceinline__ void scatter_carve(unsigned char* smem, int max_bins,
     delta = cursor + max_bins;
     cnt = reinterpret_cast<uint32_t*>(delta + max_bins);
     sbin = reinterpret_cast<uint16_t*>(cnt + max_bins);
+}
+
+// Shared-memory layout of the bulk scatter: two tile buffers of bulk_tile_buf(max_bins) bytes, then
+// the output cursors (int64 per bin), the bin counts and the staged starts (uint32 each).
+__device__ __forceinline__ void bulk_carve(unsigned char* smem, int max_bins, unsigned char*& inbuf,
+                                           int64_t*& cursor, uint32_t*& cnt, uint32_t*& spos) {
+    inbuf = smem;
+    cursor = reinterpret_cast<int64_t*>(smem + 2 * bulk_tile_buf(max_bins));
+    cnt = reinterpret_cast<uint32_t*>(cursor + max_bins);
+    spos = cnt + max_bins;
 }
 
 __device__ __forceinline__ void init_bars(uint64_t* bars) {
@@ -578,16 +724,17 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 // kPacked selects the slices this launch handles: false = tuples from the caller's key/value arrays,
 // true = S survivors of a level-1 Bloom probe, packed in cmp. One instantiation per input form keeps
 // each kernel within the 64 registers that two CTAs per SM allow.
-template <bool kPacked, int M>
+template <bool kPacked, int M, bool kBulk>
 __global__ void __launch_bounds__(kSThreads, 1)
 k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
              const int64_t* __restrict__ scan, unsigned long long* gwords, int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* inbuf;
-    int64_t *cursor, *delta;
-    uint32_t* cnt;
-    uint16_t* sbin;
-    scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
+    int64_t *cursor, *delta = nullptr;
+    uint32_t *cnt, *spos = nullptr;
+    uint16_t* sbin = nullptr;
+    if constexpr (kBulk) bulk_carve(smem, max_bins, inbuf, cursor, cnt, spos);  // max_bins <= kBulkMaxBins
+    else scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
     __shared__ uint32_t tmp[kSThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
@@ -610,14 +757,25 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         __syncthreads();
         const Bin1<M> bin{d.pf};
         if constexpr (kPacked) {
-            scatter_tiles(PackedTiles{R.cmp}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf,
-                          bars, ph, &gwords[kGErrors]);
+            const PackedTiles in{R.cmp};
+            if constexpr (kBulk)
+                scatter_tiles_bulk(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
+                                   bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors]);
+            else
+                scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph,
+                              &gwords[kGErrors]);
         } else {
             const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 3) == 0;
-            scatter_tiles(KvTiles{R.key, R.val, al}, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp,
-                          inbuf, bars, ph, &gwords[kGErrors]);
+            const KvTiles in{R.key, R.val, al};
+            if constexpr (kBulk)
+                scatter_tiles_bulk(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
+                                   bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors]);
+            else
+                scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph,
+                              &gwords[kGErrors]);
         }
     }
+    if constexpr (kBulk) bulk_wait_all();  // the bulk stores have written the output before the kernel ends
 }
 
 // Level-1 partition starts of every join with P2 == 1, or the level-2 input ranges otherwise:
@@ -804,7 +962,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 }
 
 // Level-2 scatter of one slice into its private runs of the level-2 buffer.
-template <int M>
+template <int M, bool kBulk>
 __global__ void __launch_bounds__(kSThreads, 1)
 k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
              const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
@@ -812,10 +970,11 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
              int max_bins) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* inbuf;
-    int64_t *cursor, *delta;
-    uint32_t* cnt;
-    uint16_t* sbin;
-    scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
+    int64_t *cursor, *delta = nullptr;
+    uint32_t *cnt, *spos = nullptr;
+    uint16_t* sbin = nullptr;
+    if constexpr (kBulk) bulk_carve(smem, max_bins, inbuf, cursor, cnt, spos);  // max_bins <= kBulkMaxBins
+    else scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
     __shared__ uint32_t tmp[kSThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
@@ -835,9 +994,15 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const int64_t* Sx = S2 + x.local_off * P2;
         for (uint32_t q = threadIdx.x; q < P2; q += kSThreads) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
         __syncthreads();
-        scatter_tiles(PackedTiles{bloom ? R.cmp : R.l1}, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2,
-                      R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph, &gwords[kGErrors]);
+        const PackedTiles in{bloom ? R.cmp : R.l1};
+        if constexpr (kBulk)
+            scatter_tiles_bulk(in, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2, R.n, cursor, cnt, spos, tmp, inbuf,
+                               bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors]);
+        else
+            scatter_tiles(in, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2, R.n, cursor, delta, cnt, sbin, tmp, inbuf,
+                          bars, ph, &gwords[kGErrors]);
     }
+    if constexpr (kBulk) bulk_wait_all();  // the bulk stores have written the output before the kernel ends
 }
 
 // Finest-partition starts from the level-2 scan: bounds[p*P2+q] = start of (p, q); bounds[P1*P2] =
@@ -1536,6 +1701,7 @@ size_t probe_smem_bytes(int table_cap, int emit_key) {
 // Shared memory of the scatter kernels: two bulk-copy tile buffers, the reordered tile, and a
 // cursor and a count per bin.
 static size_t scatter_smem(int max_bins) {
+    if (max_bins <= kBulkMaxBins) return 2 * bulk_tile_buf(max_bins) + (size_t)max_bins * (8 + 4 + 4);
     return 2 * kTileBuf + (size_t)max_bins * (8 + 8 + 4) + (size_t)kSTile * 2;
 }
 
@@ -1569,11 +1735,16 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     static thread_local bool attrs_done = false;
     cudaError_t err;
     if (!attrs_done) {
-        const void* l1s[] = {(const void*)k_l1_scatter<false, 0>, (const void*)k_l1_scatter<false, 1>,
-                             (const void*)k_l1_scatter<true, 0>, (const void*)k_l1_scatter<true, 1>};
+        const void* l1s[] = {(const void*)k_l1_scatter<false, 0, false>, (const void*)k_l1_scatter<false, 1, false>,
+                             (const void*)k_l1_scatter<true, 0, false>, (const void*)k_l1_scatter<true, 1, false>};
         for (const void* f : l1s)
             if ((err = set_smem_attr(f, scatter_smem(kMaxP1))) != cudaSuccess) return err;
-        const void* l2s[] = {(const void*)k_l2_scatter<0>, (const void*)k_l2_scatter<1>};
+        const void* bulks[] = {(const void*)k_l1_scatter<false, 0, true>, (const void*)k_l1_scatter<false, 1, true>,
+                               (const void*)k_l1_scatter<true, 0, true>,  (const void*)k_l1_scatter<true, 1, true>,
+                               (const void*)k_l2_scatter<0, true>,        (const void*)k_l2_scatter<1, true>};
+        for (const void* f : bulks)
+            if ((err = set_smem_attr(f, scatter_smem(kBulkMaxBins))) != cudaSuccess) return err;
+        const void* l2s[] = {(const void*)k_l2_scatter<0, false>, (const void*)k_l2_scatter<1, false>};
         for (const void* f : l2s)
             if ((err = set_smem_attr(f, scatter_smem(kMaxP2))) != cudaSuccess) return err;
         const void* bbs[] = {(const void*)k_bloom_build<0, 0>, (const void*)k_bloom_build<1, 0>,
@@ -1630,12 +1801,15 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             for_modes(a.modes, [&](auto mt) {
                 constexpr int M = decltype(mt)::value;
                 const dim3 grid(grid_for(a.total_slices[rel], sms, 1));
-                k_l1_scatter<false, M><<<grid, kSThreads, scatter_smem(a.max_p1), st>>>(
-                    a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
+                const bool bulk = a.max_p1 <= kBulkMaxBins;
+                (bulk ? k_l1_scatter<false, M, true> : k_l1_scatter<false, M, false>)<<<grid, kSThreads,
+                    scatter_smem(a.max_p1), st>>>(a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords,
+                                                  a.max_p1);
                 ++launches;
                 if (rel == 1 && a.any_bloom_l1) {
-                    k_l1_scatter<true, M><<<grid, kSThreads, scatter_smem(a.max_p1), st>>>(
-                        a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
+                    (bulk ? k_l1_scatter<true, M, true> : k_l1_scatter<true, M, false>)<<<grid, kSThreads,
+                        scatter_smem(a.max_p1), st>>>(a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords,
+                                                      a.max_p1);
                     ++launches;
                 }
             });
@@ -1678,7 +1852,8 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 return err;
             for_modes(a.modes, [&](auto mt) {
                 constexpr int M = decltype(mt)::value;
-                k_l2_scatter<M><<<grid_for(a.l2_slice_cap[rel], sms, 1), kSThreads, scatter_smem(a.max_p2), st>>>(
+                (a.max_p2 <= kBulkMaxBins ? k_l2_scatter<M, true> : k_l2_scatter<M, false>)<<<
+                    grid_for(a.l2_slice_cap[rel], sms, 1), kSThreads, scatter_smem(a.max_p2), st>>>(
                     a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2_scan, a.slice_cnt2,
                     a.gwords, a.max_p2);
                 ++launches;

@@ -27,9 +27,10 @@ def test_uniform_hash(bj, oracle, torch_cuda, n, bloom):
 
 
 @pytest.mark.parametrize("level", [1, 2])
-@pytest.mark.parametrize("mode,p1,p2", [(0, 16, 16), (0, 64, 64), (1, 100, 7), (1, 512, 67)])
+@pytest.mark.parametrize("mode,p1,p2", [(0, 16, 16), (0, 64, 64), (1, 100, 7), (1, 512, 67), (0, 4, 64)])
 def test_bloom_probe_levels(bj, oracle, torch_cuda, level, mode, p1, p2):
-    """The filter probed in S's first partition pass or fused into its second pass."""
+    """The filter probed in S's first partition pass or fused into its second pass (fan-out 4 gives
+    level-1 partitions of 100K keys, whose filter segments span about 125 KB)."""
     rk, rv, sk, sv = bj.gen_host(31 + level, 400_000, 600_000, 0.05)
     st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=1, bloom_probe_level=level,
                  partition_mode=mode, partition_size=p1, second_partition_size=p2)
