@@ -400,6 +400,10 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
 // step 1, by when they normally have).
 constexpr int kBulkMaxBins = 1024;
 static_assert(kBulkMaxBins <= kSThreads, "one bin per thread");
+// The level-2 scatter takes the bulk path up to 256 bins only: at 512 bins (640M x 640M, slices of
+// 16 tiles) the write-pass form measured 3.43 ms against 3.59 ms, while at the batch's fan-outs
+// (<= 64) the bulk form is faster (3.41 against 4.09 ms for the R side of 256 uneven joins).
+constexpr int kBulkMaxBinsL2 = 256;
 // One tile buffer of the bulk scatter: the tile plus one slot per bin, a multiple of 16 bytes.
 __host__ __device__ constexpr size_t bulk_tile_buf(int max_bins) {
     return (size_t)((kSTile + max_bins + 2 + 1) & ~1) * 8;
@@ -1368,12 +1372,51 @@ __device__ __forceinline__ void stage_matches(const JoinDesc& d, bool m, uint32_
 // its buckets over the lanes instead (duplicate-heavy build keys, e.g. Zipf-skewed matches).
 constexpr uint32_t kLockstepMax = 8;
 
+// The spread walk: the warp walks the concatenation of its candidates' buckets 32 entries at a
+// time, with a warp prefix sum of the bucket lengths and, per entry, a five-step shuffle binary
+// search for the candidate that owns it. A key repeated k times on the build side then costs about
+// k/32 steps instead of k. Lane l holds candidate e with bucket [lo, lo + len). Kept out of line
+// (it runs only for warps with a long bucket), so its registers do not weigh on the common path;
+// it takes and returns the warp's staging count by value. Returns the new count.
+__device__ __noinline__ int probe_spread(const JoinDesc* d, uint2 e, uint32_t lo, uint32_t len,
+                                         const uint2* table, bool bs, int emit_key, int lane, uint32_t* wr,
+                                         uint32_t* ws, uint32_t* wk, int count) {
+    WarpOut o{wr, ws, wk, count};
+    uint32_t inc = len;  // inclusive prefix of the bucket lengths over the lanes
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, s);
+        if (lane >= s) inc += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t g = base + (uint32_t)lane;
+        // owner: the first lane c with inc[c] > g (lanes with empty buckets are skipped over)
+        int c = 0;
+#pragma unroll
+        for (int s = 16; s > 0; s >>= 1) {
+            const uint32_t v = __shfl_sync(0xffffffffu, inc, c + s - 1);
+            if (v <= g) c += s;
+        }
+        const uint32_t c_lo = __shfl_sync(0xffffffffu, lo, c);
+        const uint32_t c_start = __shfl_sync(0xffffffffu, inc - len, c);
+        const uint32_t c_key = __shfl_sync(0xffffffffu, e.x, c);
+        const uint32_t c_val = __shfl_sync(0xffffffffu, e.y, c);
+        bool m = false;
+        uint32_t rv = 0;
+        if (g < total) {
+            const uint2 cc = table[c_lo + (g - c_start)];
+            m = (cc.x == c_key);
+            rv = cc.y;
+        }
+        stage_matches(*d, m, bs ? c_val : rv, bs ? rv : c_val, c_key, emit_key, lane, o);
+    }
+    return o.count;
+}
+
 // The warp scans the buckets of candidates q[0, n) (n <= 32), one per lane, and stages every match.
-// Short buckets are scanned in lock step, one entry per lane per step, so the warp takes as many
-// steps as its longest bucket. When that exceeds kLockstepMax the warp instead walks the
-// concatenation of all its buckets 32 entries at a time: a warp prefix sum of the bucket lengths,
-// and per entry a five-step shuffle binary search for the candidate that owns it. A key repeated k
-// times on the build side then costs about k/32 steps instead of k.
+// Buckets are scanned in lock step, one entry per lane per step, so the warp takes as many steps as
+// its longest bucket; above kLockstepMax steps it takes the spread walk instead.
 __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2* q, int n, const uint2* table,
                                                  const uint32_t* off, uint32_t mask, bool bs, int emit_key,
                                                  int lane, WarpOut& o) {
@@ -1385,37 +1428,8 @@ __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2*
         lo = off[bk];
         hi = off[bk + 1];
     }
-    const uint32_t len = hi - lo;
-    if (__reduce_max_sync(0xffffffffu, len) > kLockstepMax) {
-        uint32_t inc = len;  // inclusive prefix of the bucket lengths over the lanes
-#pragma unroll
-        for (int s = 1; s < 32; s <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, s);
-            if (lane >= s) inc += y;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-        for (uint32_t base = 0; base < total; base += 32) {
-            const uint32_t g = base + (uint32_t)lane;
-            // owner: the first lane c with inc[c] > g (lanes with empty buckets are skipped over)
-            int c = 0;
-#pragma unroll
-            for (int s = 16; s > 0; s >>= 1) {
-                const uint32_t v = __shfl_sync(0xffffffffu, inc, c + s - 1);
-                if (v <= g) c += s;
-            }
-            const uint32_t c_lo = __shfl_sync(0xffffffffu, lo, c);
-            const uint32_t c_start = __shfl_sync(0xffffffffu, inc - len, c);
-            const uint32_t c_key = __shfl_sync(0xffffffffu, e.x, c);
-            const uint32_t c_val = __shfl_sync(0xffffffffu, e.y, c);
-            bool m = false;
-            uint32_t rv = 0;
-            if (g < total) {
-                const uint2 cc = table[c_lo + (g - c_start)];
-                m = (cc.x == c_key);
-                rv = cc.y;
-            }
-            stage_matches(d, m, bs ? c_val : rv, bs ? rv : c_val, c_key, emit_key, lane, o);
-        }
+    if (__reduce_max_sync(0xffffffffu, hi - lo) > kLockstepMax) {
+        o.count = probe_spread(&d, e, lo, hi - lo, table, bs, emit_key, lane, o.wr, o.ws, o.wk, o.count);
         return;
     }
     while (__any_sync(0xffffffffu, lo < hi)) {
@@ -1477,6 +1491,30 @@ __device__ __forceinline__ void probe_stream(const JoinDesc& d, const uint2* __r
     }
 }
 
+// A task of the probe queue with its join's buffers resolved: the build and streamed ranges.
+struct ProbeTask {
+    const uint2* bsrc;
+    const uint2* psrc;
+    uint32_t b_len, p_len;
+    int32_t join;
+    int32_t bs;  // the build side is S
+};
+
+// Reads task t's record and its join's final buffers into `out` (t >= ntasks leaves it unset).
+__device__ __forceinline__ void resolve_task(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks,
+                                             long long t, long long ntasks, ProbeTask& out) {
+    if (t >= ntasks) return;
+    const Task tk = tasks[t];
+    const JoinDesc& d = J[tk.join];
+    const bool bs = (tk.flags & kTaskBuildS) != 0;
+    out.bsrc = final_buf(d, bs ? 1 : 0) + tk.b_begin;
+    out.psrc = final_buf(d, bs ? 0 : 1) + tk.p_begin;
+    out.b_len = tk.b_len;
+    out.p_len = tk.p_len;
+    out.join = tk.join;
+    out.bs = bs ? 1 : 0;
+}
+
 __global__ void __launch_bounds__(kThreads, 2)
 k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned long long* gwords,
         int table_cap, int emit_key) {
@@ -1489,6 +1527,7 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     uint32_t* wbuf = off + table_cap + 4;
     __shared__ uint32_t tmp[kThreads / 32];
     __shared__ long long s_task[2];
+    __shared__ ProbeTask s_info[2];  // the current task and the next one, resolved by thread 0
     __shared__ __align__(8) uint64_t bar;
     unsigned long long* errors = &gwords[kGErrors];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1503,7 +1542,9 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     uint32_t ph = 0;
     const long long ntasks = (long long)gwords[kGTasks];
     if (threadIdx.x == 0) {
-        s_task[0] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
+        const long long t0 = (long long)atomicAdd(&gwords[kGQueue], 1ull);
+        s_task[0] = t0;
+        resolve_task(J, tasks, t0, ntasks, s_info[0]);
         mbar_init(&bar, 1);
         mbar_init_fence();
     }
@@ -1511,20 +1552,20 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     for (int slot = 0;; slot ^= 1) {
         const long long t = s_task[slot];
         if (t >= ntasks) break;
-        const Task& tk = tasks[t];
+        const ProbeTask tk = s_info[slot];
         const JoinDesc& d = J[tk.join];
-        const bool bs = (tk.flags & kTaskBuildS) != 0;
-        const uint2* __restrict__ bsrc = final_buf(d, bs ? 1 : 0) + tk.b_begin;
-        const uint2* __restrict__ psrc = final_buf(d, bs ? 0 : 1) + tk.p_begin;
+        const bool bs = tk.bs != 0;
+        const uint2* __restrict__ bsrc = tk.bsrc;
+        const uint2* __restrict__ psrc = tk.psrc;
         const uint32_t pn = tk.p_len;
         const uint32_t first = pn < (uint32_t)kProbeFirst ? pn : (uint32_t)kProbeFirst;
         // the first probe chunk is copied into shared memory while the table is built
         if (threadIdx.x == 0) {
-            s_task[slot ^ 1] = (long long)atomicAdd(&gwords[kGQueue], 1ull);
             PackedTiles{psrc}.issue(0, (int)first, reinterpret_cast<unsigned char*>(pbuf), &bar);
             // the first two global iterations of the probe side go to L2 while the table is built
             if (pn > first)
                 prefetch_l2_range(psrc + first, psrc + min_i64((int64_t)pn, (int64_t)first + 2 * kProbeU * kThreads));
+            s_task[slot ^ 1] = (long long)atomicAdd(&gwords[kGQueue], 1ull);  // resolved after the probe
         }
         if (tk.join != cur) {
             if (cur >= 0 && o.count > 0) warp_flush(J[cur], o.wr, o.ws, o.wk, o.count, lane);
@@ -1566,10 +1607,11 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         if (nb == 8 * kThreads) scan_dir<8>(off, nb, tmp);
         else if (nb == 4 * kThreads) scan_dir<4>(off, nb, tmp);
         else block_scan_excl(off, (int)nb + 1, tmp);
+        // the build tuples are read again (cache hits) rather than held in registers across the scan
 #pragma unroll
         for (int k = 0; k < kBuildPer; ++k) {
             const int i = k * kThreads + threadIdx.x;
-            if (i < nr) table[off[br[k] >> 16] + (br[k] & 0xffffu)] = bt[k];
+            if (i < nr) table[off[br[k] >> 16] + (br[k] & 0xffffu)] = __ldg(bsrc + i);
         }
         mbar_wait(&bar, ph, errors);
         ph ^= 1u;
@@ -1581,6 +1623,13 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         if (pn > first)
             probe_stream<false, kProbeU>(d, psrc + first, pn - first, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
         if (qn > 0) probe_candidates(d, q, qn, table, off, mask, bs, emit_key, lane, o);
+        // the next task's record and buffers, read while the other warps finish this task, and its
+        // build chunk on its way into L2
+        if (threadIdx.x == 0) {
+            ProbeTask& nx = s_info[slot ^ 1];
+            resolve_task(J, tasks, s_task[slot ^ 1], ntasks, nx);
+            if (s_task[slot ^ 1] < ntasks) prefetch_l2_range(nx.bsrc, nx.bsrc + nx.b_len);
+        }
         __syncwarp();
         __syncthreads();
     }
@@ -1700,8 +1749,10 @@ size_t probe_smem_bytes(int table_cap, int emit_key) {
 
 // Shared memory of the scatter kernels: two bulk-copy tile buffers, the reordered tile, and a
 // cursor and a count per bin.
-static size_t scatter_smem(int max_bins) {
-    if (max_bins <= kBulkMaxBins) return 2 * bulk_tile_buf(max_bins) + (size_t)max_bins * (8 + 4 + 4);
+// Dynamic shared memory of a scatter kernel over at most max_bins bins: the bulk-store layout
+// (bulk_carve) or the write-pass layout (scatter_carve).
+static size_t scatter_smem(int max_bins, bool bulk) {
+    if (bulk) return 2 * bulk_tile_buf(max_bins) + (size_t)max_bins * (8 + 4 + 4);
     return 2 * kTileBuf + (size_t)max_bins * (8 + 8 + 4) + (size_t)kSTile * 2;
 }
 
@@ -1738,15 +1789,15 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
         const void* l1s[] = {(const void*)k_l1_scatter<false, 0, false>, (const void*)k_l1_scatter<false, 1, false>,
                              (const void*)k_l1_scatter<true, 0, false>, (const void*)k_l1_scatter<true, 1, false>};
         for (const void* f : l1s)
-            if ((err = set_smem_attr(f, scatter_smem(kMaxP1))) != cudaSuccess) return err;
+            if ((err = set_smem_attr(f, scatter_smem(kMaxP1, false))) != cudaSuccess) return err;
         const void* bulks[] = {(const void*)k_l1_scatter<false, 0, true>, (const void*)k_l1_scatter<false, 1, true>,
                                (const void*)k_l1_scatter<true, 0, true>,  (const void*)k_l1_scatter<true, 1, true>,
                                (const void*)k_l2_scatter<0, true>,        (const void*)k_l2_scatter<1, true>};
         for (const void* f : bulks)
-            if ((err = set_smem_attr(f, scatter_smem(kBulkMaxBins))) != cudaSuccess) return err;
+            if ((err = set_smem_attr(f, scatter_smem(kBulkMaxBins, true))) != cudaSuccess) return err;
         const void* l2s[] = {(const void*)k_l2_scatter<0, false>, (const void*)k_l2_scatter<1, false>};
         for (const void* f : l2s)
-            if ((err = set_smem_attr(f, scatter_smem(kMaxP2))) != cudaSuccess) return err;
+            if ((err = set_smem_attr(f, scatter_smem(kMaxP2, false))) != cudaSuccess) return err;
         const void* bbs[] = {(const void*)k_bloom_build<0, 0>, (const void*)k_bloom_build<1, 0>,
                              (const void*)k_bloom_build<0, kBloomFastK>, (const void*)k_bloom_build<1, kBloomFastK>};
         for (const void* f : bbs)
@@ -1803,12 +1854,12 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 const dim3 grid(grid_for(a.total_slices[rel], sms, 1));
                 const bool bulk = a.max_p1 <= kBulkMaxBins;
                 (bulk ? k_l1_scatter<false, M, true> : k_l1_scatter<false, M, false>)<<<grid, kSThreads,
-                    scatter_smem(a.max_p1), st>>>(a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords,
+                    scatter_smem(a.max_p1, bulk), st>>>(a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords,
                                                   a.max_p1);
                 ++launches;
                 if (rel == 1 && a.any_bloom_l1) {
                     (bulk ? k_l1_scatter<true, M, true> : k_l1_scatter<true, M, false>)<<<grid, kSThreads,
-                        scatter_smem(a.max_p1), st>>>(a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords,
+                        scatter_smem(a.max_p1, bulk), st>>>(a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords,
                                                       a.max_p1);
                     ++launches;
                 }
@@ -1852,8 +1903,9 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 return err;
             for_modes(a.modes, [&](auto mt) {
                 constexpr int M = decltype(mt)::value;
-                (a.max_p2 <= kBulkMaxBins ? k_l2_scatter<M, true> : k_l2_scatter<M, false>)<<<
-                    grid_for(a.l2_slice_cap[rel], sms, 1), kSThreads, scatter_smem(a.max_p2), st>>>(
+                const bool bulk2 = a.max_p2 <= kBulkMaxBinsL2;
+                (bulk2 ? k_l2_scatter<M, true> : k_l2_scatter<M, false>)<<<grid_for(a.l2_slice_cap[rel], sms, 1),
+                                                                          kSThreads, scatter_smem(a.max_p2, bulk2), st>>>(
                     a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2_scan, a.slice_cnt2,
                     a.gwords, a.max_p2);
                 ++launches;
