@@ -31,7 +31,11 @@ constexpr int kTile = 4096;           // unit of the level-2 slice length
 constexpr int kSThreads = 1024;       // threads per CTA of the scatter kernels (one CTA per SM)
 constexpr int kSTile = 8192;          // tuples per scatter tile staged in shared memory
 constexpr int kWarpBuf = 128;         // output pairs staged per warp before a global flush
-constexpr int64_t kL2Slice = 32 * kTile;  // tuples per level-2 slice (131072)
+// Tuples per level-2 slice: 262144, or 131072 for S when its second pass probes the Bloom filter
+// (the filter segments of the partitions in flight must stay in L2; with the longer slices twice
+// as many partitions are in flight).
+constexpr int64_t kL2Slice = 64 * kTile;
+constexpr int64_t kL2SliceBloom = 32 * kTile;
 
 // Per-join device counters (int64 each).
 enum Counter : int {
@@ -226,7 +230,7 @@ struct RelPlan {
     uint2* cmp;            // Bloom survivors staged per slice [n] (S with Bloom only)
     int64_t slice_len;     // tuples per level-1 slice
     int32_t nslices;       // level-1 slices
-    int32_t pad;
+    int32_t l2_slice;      // tuples per level-2 slice
     int64_t hist_base;     // offset of this relation's [P1][nslices]+1 histogram in the global array
     int64_t* b1;           // [P1 + 1] start of each level-1 partition in l1
     int64_t* bounds;       // [P1*P2 + 1] start of each finest partition in the final buffer

@@ -199,7 +199,8 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
                 ro.cmp = L.take((size_t)std::max<int64_t>(n[r], 1) * 8);
                 if (p.bloom_level == 1) ro.slice_cnt = L.take((size_t)ro.nslices * 4);
             }
-            if (two) sh.l2_slice_cap[r] += (int64_t)p.pf.P1 + n[r] / kL2Slice + 1;
+            ro.l2_slice = (r == 1 && p.bloom && p.bloom_level == 2) ? kL2SliceBloom : kL2Slice;
+            if (two) sh.l2_slice_cap[r] += (int64_t)p.pf.P1 + n[r] / ro.l2_slice + 1;
             ro.hist_base = sh.hist_len[0] + sh.hist_len[1];  // provisional, fixed below
             sh.total_slices[r] += ro.nslices;
         }
@@ -231,7 +232,7 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
         }
         sh.hist_len[r] = base - ((r == 0) ? 0 : sh.hist_len[0]);
     }
-    // Level-2 histograms [p][q][slice] per join, sized by the slice bound P1 + n / kL2Slice + 1.
+    // Level-2 histograms [p][q][slice] per join, sized by the slice bound P1 + n / l2_slice + 1.
     for (int r = 0; r < 2; ++r) {
         int64_t base = (r == 0) ? 0 : sh.h2_len[0];
         for (int j = 0; j < nj; ++j) {
@@ -240,7 +241,7 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
             ro.h2_base = base;
             if (p.pf.P2 > 1) {
                 const int64_t n = r == 0 ? p.nr : p.ns;
-                base += ((int64_t)p.pf.P1 + n / kL2Slice + 1) * p.pf.P2 + 1;
+                base += ((int64_t)p.pf.P1 + n / ro.l2_slice + 1) * p.pf.P2 + 1;
             }
         }
         sh.h2_len[r] = base - ((r == 0) ? 0 : sh.h2_len[0]);
@@ -436,6 +437,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
             R.cmp = ro.cmp ? reinterpret_cast<uint2*>(ws + ro.cmp) : nullptr;
             R.slice_len = ro.slice_len;
             R.nslices = ro.nslices;
+            R.l2_slice = (int32_t)ro.l2_slice;
             R.hist_base = ro.hist_base;
             R.b1 = reinterpret_cast<int64_t*>(ws + ro.b1);
             R.bounds = p.pf.P2 > 1 ? reinterpret_cast<int64_t*>(ws + ro.bounds) : R.b1;

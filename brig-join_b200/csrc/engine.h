@@ -55,6 +55,7 @@ struct RelOffs {
     int64_t slice_len = 0;
     int32_t nslices = 0;
     int64_t hist_base = 0;
+    int64_t l2_slice = 0;  // tuples per level-2 slice
 };
 struct JoinOffs {
     RelOffs rel[2];

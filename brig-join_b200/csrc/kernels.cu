@@ -798,7 +798,7 @@ __global__ void k_bounds_l1(const JoinDesc* __restrict__ J, int nj, int rel, con
 }
 
 // ---- Level 2 ------------------------------------------------------------------------------------
-// Every level-1 partition p is cut into slices of kL2Slice tuples, planned on the device
+// Every level-1 partition p is cut into slices of R.l2_slice tuples, planned on the device
 // (k_l2_plan + a scan of the slice counts). Slices are handed to CTAs in (join, p, slice) order,
 // so the CTAs running at any moment work on a few adjacent partitions: their output runs and, for
 // a level-2 Bloom probe, their filter segments stay in L2. Per join the level-2 histogram is laid
@@ -844,7 +844,7 @@ __global__ void k_l2_plan(const JoinDesc* __restrict__ J, int nj, int rel, const
         const RelPlan& R = J[j].rel[rel];
         const int64_t p = g - seg_prefix[j];
         const int64_t len = R.b1[p + 1] - R.b1[p];
-        seg_ns[g] = (uint32_t)max_i64(1, (len + kL2Slice - 1) / kL2Slice);
+        seg_ns[g] = (uint32_t)max_i64(1, (len + R.l2_slice - 1) / R.l2_slice);
     }
 }
 
@@ -868,8 +868,8 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         const JoinDesc& d = J[x.j];
         const RelPlan& R = d.rel[rel];
         const uint32_t P2 = d.pf.P2;
-        const int64_t begin = R.b1[x.p] + x.sl * kL2Slice;
-        const int64_t end = min_i64(R.b1[x.p + 1], begin + kL2Slice);
+        const int64_t begin = R.b1[x.p] + x.sl * R.l2_slice;
+        const int64_t end = min_i64(R.b1[x.p + 1], begin + R.l2_slice);
         const Bin2<M> bin{d.pf};
         const bool bloom = rel == 1 && d.bloom != nullptr && d.bloom_level == 2;
         if (bloom != kBloom || d.pf.mode != M || (kBloom && bloom_kclass(d) != K))
@@ -897,7 +897,7 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t* __restrict__ bloom = d.bloom;
             uint2* __restrict__ cmp = R.cmp;
             const uint32_t fbase = x.p * P2;
-            const int32_t len = (int32_t)(end - begin);  // at most kL2Slice
+            const int32_t len = (int32_t)(end - begin);  // at most one level-2 slice
             const uint2* __restrict__ src = l1 + begin;
             for (int32_t r0 = 0; r0 < len; r0 += kL2ProbeILP * kThreads) {
                 uint2 e[kL2ProbeILP];
@@ -990,9 +990,9 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         if (d.pf.mode != M) continue;  // the other instantiation's join (block-uniform)
         const RelPlan& R = d.rel[rel];
         const uint32_t P2 = d.pf.P2;
-        const int64_t begin = R.b1[x.p] + x.sl * kL2Slice;
+        const int64_t begin = R.b1[x.p] + x.sl * R.l2_slice;
         const bool bloom = rel == 1 && d.bloom != nullptr && d.bloom_level == 2;
-        const int64_t end = bloom ? begin + slice_cnt2[t] : min_i64(R.b1[x.p + 1], begin + kL2Slice);
+        const int64_t end = bloom ? begin + slice_cnt2[t] : min_i64(R.b1[x.p + 1], begin + R.l2_slice);
         const int64_t* S2 = scan2 + R.h2_base;
         const int64_t s0 = S2[0];
         const int64_t* Sx = S2 + x.local_off * P2;
