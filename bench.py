@@ -205,15 +205,15 @@ def stage_bytes(nr, ns, surv, matches, bloom_bits, bloom_level):
     }
 
 
-# DRAM bytes (read + write) per tuple of each stage's main kernel, from one ncu capture of the same
-# kernels on 2^26 x 2^26 (inputs 4x the L2, level-1 fan-out 512 as at 640M; level-2 fan-out 64) in the
+# DRAM bytes (read + write) per tuple of each stage's main kernel, from ncu captures of the same
+# kernels on 2^26 x 2^26 (inputs 4x the L2, level-1 fan-out 512 as at 640M) summarised in the
 # profiles directory: (bytes per tuple, which count the stage's launch processes). Used to scale the
 # measured traffic to the benchmarked launch; the per-tuple traffic of these streaming kernels does
 # not depend on the relation size once the inputs exceed the L2.
 NCU_TRAFFIC_PER_TUPLE = {
-    "r_hist": (4.07, "nr"), "r_scatter": (16.3, "nr"), "r_l2_hist": (8.06, "nr"), "r_l2_scatter": (15.4, "nr"),
-    "bloom_build": (8.44, "nr"), "s_hist_probe": (4.06, "ns"), "s_scatter": (16.3, "ns"),
-    "s_l2_hist": (10.06, "ns"), "probe": (9.61, "nr"),
+    "r_hist": (4.07, "nr"), "r_scatter": (16.1, "nr"), "r_l2_hist": (8.06, "nr"), "r_l2_scatter": (16.2, "nr"),
+    "bloom_build": (8.44, "nr"), "s_hist_probe": (4.06, "ns"), "s_scatter": (16.1, "ns"),
+    "s_l2_hist": (10.04, "ns"), "probe": (9.83, "nr"),
 }
 
 
