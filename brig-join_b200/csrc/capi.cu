@@ -165,6 +165,9 @@ int brig_join_get_stats(brig_join_t* h, brig_join_stats* st) {
     });
 }
 
+// Inputs of at least this many tuples overlap S's host-to-device copy with R's passes.
+constexpr int64_t kSplitCopyTuples = 1 << 23;
+
 int brig_join_run_host(brig_join_t* h, const uint32_t* r_key, const uint32_t* r_val, int64_t n_r,
                        const uint32_t* s_key, const uint32_t* s_val, int64_t n_s, uint32_t* out_r_val,
                        uint32_t* out_s_val, uint32_t* out_key, int64_t capacity, int64_t* count,
@@ -179,17 +182,27 @@ int brig_join_run_host(brig_join_t* h, const uint32_t* r_key, const uint32_t* r_
         Engine& e = *h->eng;
         e.ensure_host_io(n_r, n_s, capacity, out_key != nullptr);
         auto& b = e.hio;
+        // Large inputs: S is copied on the engine's copy stream after R, while R's passes and the
+        // Bloom build run on `st`; S's passes wait for its copy. Small ones: all copies on `st`.
+        const bool split = n_r > 0 && n_s > 0 && n_r + n_s >= kSplitCopyTuples;
         if (n_r > 0) {
             brig::cuda_check(cudaMemcpyAsync(b.rk, r_key, (size_t)n_r * 4, cudaMemcpyHostToDevice, st), "H2D R keys");
             brig::cuda_check(cudaMemcpyAsync(b.rv, r_val, (size_t)n_r * 4, cudaMemcpyHostToDevice, st), "H2D R vals");
         }
-        if (n_s > 0) {
-            brig::cuda_check(cudaMemcpyAsync(b.sk, s_key, (size_t)n_s * 4, cudaMemcpyHostToDevice, st), "H2D S keys");
-            brig::cuda_check(cudaMemcpyAsync(b.sv, s_val, (size_t)n_s * 4, cudaMemcpyHostToDevice, st), "H2D S vals");
+        cudaStream_t sst = st;
+        if (split) {
+            brig::cuda_check(cudaEventRecord(e.r_copied, st), "cudaEventRecord");
+            brig::cuda_check(cudaStreamWaitEvent(e.copy_stream, e.r_copied, 0), "cudaStreamWaitEvent");
+            sst = e.copy_stream;
         }
+        if (n_s > 0) {
+            brig::cuda_check(cudaMemcpyAsync(b.sk, s_key, (size_t)n_s * 4, cudaMemcpyHostToDevice, sst), "H2D S keys");
+            brig::cuda_check(cudaMemcpyAsync(b.sv, s_val, (size_t)n_s * 4, cudaMemcpyHostToDevice, sst), "H2D S vals");
+        }
+        if (split) brig::cuda_check(cudaEventRecord(e.s_copied, sst), "cudaEventRecord");
         brig_join_output o{b.outr, b.outs, out_key ? b.outk : nullptr, capacity, nullptr};
         brig::JoinIO io{b.rk, b.rv, b.sk, b.sv, n_r, n_s, o};
-        e.run({io}, st, e.config().use_cuda_graph != 0);
+        e.run({io}, st, e.config().use_cuda_graph != 0, split ? e.s_copied : nullptr);
         h->last_kind = 1;
         h->last_items = 1;
         std::vector<int64_t> c;

@@ -333,6 +333,9 @@ Engine::~Engine() {
             if (e) cudaEventDestroy(e);
     if (stage_free_) cudaEventDestroy(stage_free_);
     if (done_) cudaEventDestroy(done_);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (r_copied) cudaEventDestroy(r_copied);
+    if (s_copied) cudaEventDestroy(s_copied);
 }
 
 // Growing the workspace is stream-ordered (cudaFreeAsync / cudaMallocAsync on the run's stream,
@@ -399,6 +402,11 @@ void Engine::ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key) {
         hio.outk_alloc = true;
     }
     hio.cap_out = std::max(hio.cap_out, cap);
+    if (!copy_stream) {
+        cuda_check(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_check(cudaEventCreateWithFlags(&r_copied, cudaEventDisableTiming), "cudaEventCreate");
+        cuda_check(cudaEventCreateWithFlags(&s_copied, cudaEventDisableTiming), "cudaEventCreate");
+    }
 }
 
 void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const JoinIO* joins, int nj,
@@ -528,7 +536,8 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     a.l2_slice_cap[1] = sh.l2_slice_cap[1];
 }
 
-void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph) {
+void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph, cudaEvent_t s_ready) {
+    if (s_ready) use_graph = false;
     const int nj = (int)joins.size();
     if (nj <= 0) fail(BRIG_E_INVALID, "no joins");
     std::vector<int64_t> nr(nj), ns(nj);
@@ -557,6 +566,7 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
     // captured into a graph is only a dependency edge, not a timestamp).
     if (profiling_) use_graph = false;
     a.stage_events = profiling_ ? stage_ev_[runs_recorded_ % kStageRing] : nullptr;
+    a.s_ready = s_ready;
 
     auto enqueue_all = [&](cudaStream_t st) {
         cuda_check(cudaMemcpyAsync(meta, stage_, sh.meta_bytes, cudaMemcpyHostToDevice, st),

@@ -98,8 +98,10 @@ public:
     explicit Engine(const brig_join_config& cfg);
     ~Engine();
 
-    // Enqueues all joins on `stream` (asynchronous).
-    void run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph);
+    // Enqueues all joins on `stream` (asynchronous). With `s_ready`, the S passes wait for that
+    // event while R's passes and the Bloom build run (no graph: the event lives outside it).
+    void run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph,
+             cudaEvent_t s_ready = nullptr);
     // Times candidate configurations on `joins`, keeps the fastest in the handle and returns it.
     brig_join_config autotune(const std::vector<JoinIO>& joins, cudaStream_t stream);
     // Waits for the last run; copies per-join counters.
@@ -130,6 +132,10 @@ public:
         bool outk_alloc = false;
     } hio;
     void ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key);
+    // Stream and events of the host-array entry point: S's inputs are copied on copy_stream after
+    // R's (r_copied) while R's passes run; s_copied marks their arrival.
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t r_copied = nullptr, s_copied = nullptr;
 
 private:
     void ensure_workspace(size_t bytes, cudaStream_t stream);

@@ -1829,6 +1829,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 ++launches;
             });
         }
+        if (rel == 1 && a.s_ready && (err = cudaStreamWaitEvent(st, a.s_ready, 0)) != cudaSuccess) return err;
         if (rel == 1) mark(6);
         const int m0 = rel == 0 ? 1 : 7;  // first stage mark of this relation
         if (!part) {

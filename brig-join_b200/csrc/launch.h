@@ -44,6 +44,7 @@ struct PipelineArgs {
     int kclasses;                     // Bloom k classes present: bit 0 any k (or no filter), bit 1 k = 7
     int num_sms;
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
+    cudaEvent_t s_ready;              // when set, S's passes wait for it (its inputs are still arriving)
     int stages;                       // kRunPartR | kRunBloom | kRunPartS | kRunProbe
     // level 2 (planned on the device)
     uint32_t* seg_ns;                 // [total_segs + 1] slices per level-1 partition

@@ -173,6 +173,26 @@ def test_run_host_entry_point(bj, oracle):
     assert_same_pairs(oracle, r, s, exp_r, exp_s)
 
 
+@pytest.mark.parametrize("pinned", [False, True])
+def test_run_host_overlapped_copies(bj, oracle, torch_cuda, pinned):
+    """Host inputs of at least 2^23 tuples: S is copied on a second stream while R's passes run,
+    and S's passes wait for the copy (pageable arrays copy synchronously, pinned ones overlap)."""
+    rk, rv, sk, sv = bj.gen_host(77, 4_500_000, 4_000_000, 0.2)
+    if pinned:
+        arrs = []
+        for a in (rk, rv, sk, sv):
+            t = torch_cuda.empty(len(a), dtype=torch_cuda.int32, pin_memory=True)
+            t.numpy()[:] = a.view(np.int32)
+            arrs.append(t.numpy().view(np.uint32))
+        rk, rv, sk, sv = arrs
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    with bj.Join(use_bloom=1) as j:
+        for _ in range(2):  # the second run reuses the handle's buffers, stream and events
+            cnt, r, s = j.run_host(rk, rv, sk, sv, capacity=len(exp_r))
+            assert cnt == len(exp_r) == 800_000
+            assert_same_pairs(oracle, r, s, exp_r, exp_s)
+
+
 def test_device_generator_matches_host(bj, torch_cuda):
     n_r, n_s = 300_001, 500_003
     h = bj.gen_host(1234, n_r, n_s, 0.37)
