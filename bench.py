@@ -9,7 +9,9 @@ shared-memory hash build and probe, pair materialisation) over inputs resident i
   python bench.py [--gpus N --steps K --warmup W] [--workload c1|c0] [--impl reference]
 
 One JSON line on rank 0. `value` is the device-timed join throughput (|R|+|S|)/t over all ranks;
-`e2e` the same metric through the host-array C entry point (H2D inputs, join, D2H pairs);
+`e2e` the same metric through the host-array C entry point (H2D inputs, join, D2H pairs; S in
+16 chunks against R partitioned once when |S| >= 2^26, so each chunk's passes overlap the next
+chunk's copy);
 `roofline` the dominant pipeline stage's algorithmic bytes over its CUDA-event duration;
 `cpu_baseline` the reference's own CPU join (run_sanity_check) on a bounded sample on this host.
 With N > 1 every rank runs an independent replica of the join (the path is single-GPU).
@@ -422,6 +424,9 @@ def main():
     ap.add_argument("--p1", type=int, default=0, help="override the level-1 fan-out")
     ap.add_argument("--p2", type=int, default=0, help="override the level-2 fan-out")
     ap.add_argument("--table", type=int, default=0, help="override table_capacity")
+    ap.add_argument("--s-chunks", type=int, default=-1,
+                    help="e2e: copy and join S in this many chunks against R partitioned once (s_chunks); "
+                         "-1: 16 when |S| >= 2^26, else one piece")
     args = ap.parse_args()
     if args.steps > 64:
         ap.error("--steps above 64: per-stage events keep the last 64 runs")
@@ -535,12 +540,19 @@ def main():
         torch.cuda.synchronize()
         times = []
         cnt = None
+        jh = j
+        if args.s_chunks < 0:
+            args.s_chunks = 16 if ns >= (1 << 26) else 0
+        if args.s_chunks > 1:
+            jh = bj.Join(use_bloom=wl["bloom"], bloom_bits_per_key=wl["bpk"], bloom_num_hashes=wl["k"],
+                         bloom_probe_level=args.bloom_level, partition_size=args.p1, second_partition_size=args.p2,
+                         table_capacity=args.table, s_chunks=args.s_chunks)
         for it in range(args.e2e_steps + 1):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            cnt, _, _ = j.run_host(hk[0].numpy(), hk[1].numpy(), hk[2].numpy(), hk[3].numpy(), capacity=cap,
-                                   out=(ho_r.numpy(), ho_s.numpy(), None), stream=sp)
+            cnt, _, _ = jh.run_host(hk[0].numpy(), hk[1].numpy(), hk[2].numpy(), hk[3].numpy(), capacity=cap,
+                                    out=(ho_r.numpy(), ho_s.numpy(), None), stream=sp)
             e1.record(stream)
             torch.cuda.synchronize()
             if it > 0:
@@ -553,6 +565,8 @@ def main():
             e2e_ms = float(t.item())
         e2e = {"value": world * (nr + ns) / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
                "h2d_bytes_per_step": 8 * (nr + ns), "d2h_bytes_per_step": 8 * cnt + 8}
+        if args.s_chunks > 1:
+            e2e["s_chunks"] = args.s_chunks
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -67,7 +67,8 @@ class Config(C.Structure):
         ("profile_stages", C.c_int32),
         ("bloom_probe_level", C.c_int32),
         ("max_level1_bits", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("s_chunks", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -299,7 +300,7 @@ class Join:
                    np.empty(capacity, np.uint32) if emit_key else None)
         cnt = C.c_int64()
         ok = (BRIG_OK, BRIG_E_OVERFLOW) if allow_overflow else (BRIG_OK,)
-        check(lib().brig_join_run_host(self.h, _ptr(r_key), _ptr(r_val), n_r, _ptr(s_key), _ptr(s_val), n_s,
+        self.last_status = check(lib().brig_join_run_host(self.h, _ptr(r_key), _ptr(r_val), n_r, _ptr(s_key), _ptr(s_val), n_s,
                                        _ptr(out[0]), _ptr(out[1]), _ptr(out[2]), capacity, C.byref(cnt),
                                        _ptr(stream)), "brig_join_run_host", ok)
         n = min(cnt.value, capacity)

@@ -49,7 +49,7 @@ void check_cfg(const brig_join_config* cfg) {
     if (cfg->abi_version != BRIG_JOIN_ABI_VERSION) fail(BRIG_E_INVALID, "config ABI version mismatch");
     if (cfg->partition_size < 0 || cfg->second_partition_size < 0 || cfg->table_capacity < 0 ||
         cfg->s_chunk < 0 || cfg->bloom_num_hashes < 0 || cfg->bloom_num_bits < 0 ||
-        cfg->bloom_bits_per_key < 0)
+        cfg->bloom_bits_per_key < 0 || cfg->s_chunks < 0)
         fail(BRIG_E_INVALID, "negative config field");
     if (cfg->bloom_num_hashes > brig::kMaxBloomK) fail(BRIG_E_INVALID, "bloom_num_hashes > 16");
 }
@@ -166,7 +166,32 @@ int brig_join_get_stats(brig_join_t* h, brig_join_stats* st) {
 }
 
 // Inputs of at least this many tuples overlap S's host-to-device copy with R's passes.
-constexpr int64_t kSplitCopyTuples = 1 << 23;
+static constexpr int64_t kSplitCopyTuples = 1 << 23;
+
+// The end of a host-array join: waits for the counts, copies min(count, capacity) pairs back.
+static int finish_host_run(brig_join_t* h, uint32_t* out_r_val, uint32_t* out_s_val, uint32_t* out_key,
+                    int64_t capacity, int64_t* count, cudaStream_t st) {
+    Engine& e = *h->eng;
+    auto& b = e.hio;
+    h->last_kind = 1;
+    h->last_items = 1;
+    std::vector<int64_t> c;
+    int64_t errors = 0;
+    e.sync_counters(c, errors);
+    if (errors) fail(BRIG_E_INTERNAL, "device-side consistency check failed");
+    const int64_t cnt = c[brig::kCntMatches];
+    const int64_t n = std::min(cnt, capacity);
+    if (n > 0) {
+        brig::cuda_check(cudaMemcpyAsync(out_r_val, b.outr, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H r_val");
+        brig::cuda_check(cudaMemcpyAsync(out_s_val, b.outs, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H s_val");
+        if (out_key)
+            brig::cuda_check(cudaMemcpyAsync(out_key, b.outk, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H key");
+    }
+    brig::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    if (count) *count = cnt;
+    if (cnt > capacity) return (int)set_error(BRIG_E_OVERFLOW, "match count exceeds output capacity");
+    return (int)BRIG_OK;
+}
 
 int brig_join_run_host(brig_join_t* h, const uint32_t* r_key, const uint32_t* r_val, int64_t n_r,
                        const uint32_t* s_key, const uint32_t* s_val, int64_t n_s, uint32_t* out_r_val,
@@ -180,8 +205,13 @@ int brig_join_run_host(brig_join_t* h, const uint32_t* r_key, const uint32_t* r_
         if (capacity > 0 && (!out_r_val || !out_s_val)) fail(BRIG_E_INVALID, "null output arrays");
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         Engine& e = *h->eng;
-        e.ensure_host_io(n_r, n_s, capacity, out_key != nullptr);
         auto& b = e.hio;
+        const int chunks = e.config().s_chunks;
+        if (chunks > 1 && n_r > 0 && n_s > 0) {
+            e.run_host_chunked(r_key, r_val, n_r, s_key, s_val, n_s, chunks, capacity, out_key != nullptr, st);
+            return finish_host_run(h, out_r_val, out_s_val, out_key, capacity, count, st);
+        }
+        e.ensure_host_io(n_r, n_s, capacity, out_key != nullptr);
         // Large inputs: S is copied on the engine's copy stream after R, while R's passes and the
         // Bloom build run on `st`; S's passes wait for its copy. Small ones: all copies on `st`.
         const bool split = n_r > 0 && n_s > 0 && n_r + n_s >= kSplitCopyTuples;
@@ -203,24 +233,7 @@ int brig_join_run_host(brig_join_t* h, const uint32_t* r_key, const uint32_t* r_
         brig_join_output o{b.outr, b.outs, out_key ? b.outk : nullptr, capacity, nullptr};
         brig::JoinIO io{b.rk, b.rv, b.sk, b.sv, n_r, n_s, o};
         e.run({io}, st, e.config().use_cuda_graph != 0, split ? e.s_copied : nullptr);
-        h->last_kind = 1;
-        h->last_items = 1;
-        std::vector<int64_t> c;
-        int64_t errors = 0;
-        e.sync_counters(c, errors);
-        if (errors) fail(BRIG_E_INTERNAL, "device-side consistency check failed");
-        const int64_t cnt = c[brig::kCntMatches];
-        const int64_t n = std::min(cnt, capacity);
-        if (n > 0) {
-            brig::cuda_check(cudaMemcpyAsync(out_r_val, b.outr, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H r_val");
-            brig::cuda_check(cudaMemcpyAsync(out_s_val, b.outs, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H s_val");
-            if (out_key)
-                brig::cuda_check(cudaMemcpyAsync(out_key, b.outk, (size_t)n * 4, cudaMemcpyDeviceToHost, st), "D2H key");
-        }
-        brig::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
-        if (count) *count = cnt;
-        if (cnt > capacity) return (int)set_error(BRIG_E_OVERFLOW, "match count exceeds output capacity");
-        return (int)BRIG_OK;
+        return finish_host_run(h, out_r_val, out_s_val, out_key, capacity, count, st);
     });
 }
 

@@ -375,43 +375,32 @@ void gpu_main(std::vector<int>*, std::vector<int>*, const std::string& r_inputPa
         cfg.partition_size = override_partition_size > 0 ? override_partition_size : partition_size;
         if (override_second_partition_size > 0) cfg.second_partition_size = override_second_partition_size;
     }
-    const long long cap = (long long)((double)std::max(R, S) * std::max(1.0, answer_scale));
+    // The reference's S chunk loop (src/hash_kernel.cu:910-1131): R is partitioned and filtered once
+    // and S is copied and joined chunk by chunk (brig_join_config.s_chunks). The reference keeps its
+    // answers on the device and reports the count; the count here is exact with no pairs written.
+    (void)answer_scale;
+    cfg.s_chunks = s_chunks;
     brig_join_t* h = nullptr;
     if (brig_join_create(&cfg, &h) != BRIG_OK) {
         fprintf(stderr, "[brig compat] gpu_main: %s\n", brig_join_last_error());
         return;
     }
-    uint32_t *dk = nullptr, *dv = nullptr, *dsk = nullptr, *dsv = nullptr, *o_r = nullptr, *o_s = nullptr;
-    const long long chunk = (S + s_chunks - 1) / s_chunks;
     long long total = 0, overflow_tasks = 0;
-    bool ok = cudaMalloc(&dk, 4 * std::max(R, 1ll)) == cudaSuccess && cudaMalloc(&dv, 4 * std::max(R, 1ll)) == cudaSuccess &&
-              cudaMalloc(&dsk, 4 * std::max(chunk, 1ll)) == cudaSuccess &&
-              cudaMalloc(&dsv, 4 * std::max(chunk, 1ll)) == cudaSuccess &&
-              cudaMalloc(&o_r, 4 * std::max(cap, 1ll)) == cudaSuccess && cudaMalloc(&o_s, 4 * std::max(cap, 1ll)) == cudaSuccess;
     const auto t0 = std::chrono::steady_clock::now();
+    int64_t cnt = 0;
+    int rc = brig_join_run_host(h, reinterpret_cast<const uint32_t*>(tk.data()),
+                                reinterpret_cast<const uint32_t*>(tv.data()), R,
+                                reinterpret_cast<const uint32_t*>(sk.data()),
+                                reinterpret_cast<const uint32_t*>(sv.data()), S, nullptr, nullptr, nullptr, 0, &cnt,
+                                nullptr);
+    brig_join_stats st;
+    if (rc == BRIG_OK || rc == BRIG_E_OVERFLOW) rc = brig_join_get_stats(h, &st);
+    const bool ok = rc == BRIG_OK || rc == BRIG_E_OVERFLOW;
     if (ok) {
-        cudaMemcpy(dk, tk.data(), 4 * R, cudaMemcpyHostToDevice);
-        cudaMemcpy(dv, tv.data(), 4 * R, cudaMemcpyHostToDevice);
-        for (int c = 0; c < s_chunks && ok; ++c) {
-            const long long off = (long long)c * chunk, n = std::max(0ll, std::min(chunk, S - off));
-            if (n > 0) {
-                cudaMemcpy(dsk, sk.data() + off, 4 * n, cudaMemcpyHostToDevice);
-                cudaMemcpy(dsv, sv.data() + off, 4 * n, cudaMemcpyHostToDevice);
-            }
-            brig_join_output out{o_r, o_s, nullptr, cap, nullptr};
-            brig_join_stats st;
-            int rc = brig_join_run(h, dk, dv, R, dsk, dsv, n, &out, nullptr);
-            if (rc == BRIG_OK || rc == BRIG_E_OVERFLOW) rc = brig_join_get_stats(h, &st);
-            if (rc != BRIG_OK && rc != BRIG_E_OVERFLOW) {
-                fprintf(stderr, "[brig compat] gpu_main: %s\n", brig_join_last_error());
-                ok = false;
-                break;
-            }
-            total += st.count;
-            overflow_tasks += st.split_tasks;
-        }
+        total = st.count;
+        overflow_tasks = st.split_tasks;
     } else {
-        fprintf(stderr, "[brig compat] gpu_main: device allocation failed\n");
+        fprintf(stderr, "[brig compat] gpu_main: %s\n", brig_join_last_error());
     }
     const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (ok) {
@@ -419,7 +408,5 @@ void gpu_main(std::vector<int>*, std::vector<int>*, const std::string& r_inputPa
         printf("=== Grand Total Answer Count (all PEs): %lld ===\n", total);
         printf("[PE0] Total (H2D + join) %.4f sec, split tasks %lld\n", sec, overflow_tasks);
     }
-    for (uint32_t* p : {dk, dv, dsk, dsv, o_r, o_s})
-        if (p) cudaFree(p);
     brig_join_destroy(h);
 }

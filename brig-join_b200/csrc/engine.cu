@@ -336,6 +336,10 @@ Engine::~Engine() {
     if (copy_stream) cudaStreamDestroy(copy_stream);
     if (r_copied) cudaEventDestroy(r_copied);
     if (s_copied) cudaEventDestroy(s_copied);
+    for (int b = 0; b < 2; ++b) {
+        if (chunk_copied[b]) cudaEventDestroy(chunk_copied[b]);
+        if (chunk_free[b]) cudaEventDestroy(chunk_free[b]);
+    }
 }
 
 // Growing the workspace is stream-ordered (cudaFreeAsync / cudaMallocAsync on the run's stream,
@@ -406,7 +410,70 @@ void Engine::ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key) {
         cuda_check(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_check(cudaEventCreateWithFlags(&r_copied, cudaEventDisableTiming), "cudaEventCreate");
         cuda_check(cudaEventCreateWithFlags(&s_copied, cudaEventDisableTiming), "cudaEventCreate");
+        for (int b = 0; b < 2; ++b) {
+            cuda_check(cudaEventCreateWithFlags(&chunk_copied[b], cudaEventDisableTiming), "cudaEventCreate");
+            cuda_check(cudaEventCreateWithFlags(&chunk_free[b], cudaEventDisableTiming), "cudaEventCreate");
+        }
     }
+}
+
+void Engine::run_host_chunked(const uint32_t* rk, const uint32_t* rv, int64_t nr, const uint32_t* sk,
+                              const uint32_t* sv, int64_t ns, int chunks, int64_t cap, bool emit_key,
+                              cudaStream_t st) {
+    if (nr <= 0 || ns <= 0 || chunks < 2) fail(BRIG_E_INVALID, "chunked join needs R, S and at least 2 chunks");
+    const int64_t chunk = (ns + chunks - 1) / chunks;
+    const int64_t nc = (ns + chunk - 1) / chunk;
+    ensure_host_io(nr, 2 * chunk, cap, emit_key);  // waits for the handle's previous run
+    // One plan and one workspace layout for every chunk, sized by the largest chunk: R's buffers and
+    // the filter stay where they are, and a smaller last chunk only leaves trailing slices empty.
+    std::vector<JoinPlan> plans{plan_join(cfg_, nr, chunk)};
+    JoinOffs jo;
+    Shape sh;
+    layout_for(cfg_, plans.data(), 1, num_sms_, &jo, sh);
+    ensure_workspace(sh.total, st);
+    char* ws = ws_;
+    int64_t* counters = reinterpret_cast<int64_t*>(ws + sh.counters);
+    std::vector<char> meta(sh.meta_bytes);
+    const brig_join_output out{hio.outr, hio.outs, emit_key ? hio.outk : nullptr, cap, nullptr};
+    PipelineArgs a{};
+    // the descriptors go up from pageable memory: the copy returns once they are staged
+    auto launch = [&](const JoinIO& io, int stages, bool keep_errors) {
+        fill_pipeline(cfg_, plans.data(), &io, 1, sh, ws, meta.data(), num_sms_, a);
+        a.stages = stages;
+        a.keep_errors = keep_errors ? 1 : 0;
+        cuda_check(cudaMemcpyAsync(ws + sh.meta, meta.data(), sh.meta_bytes, cudaMemcpyHostToDevice, st),
+                   "descriptor upload");
+        cuda_check(enqueue_pipeline(a, st), "pipeline launch");
+    };
+    // R: copied once, then its two passes and the Bloom build
+    cuda_check(cudaMemcpyAsync(hio.rk, rk, (size_t)nr * 4, cudaMemcpyHostToDevice, st), "H2D R keys");
+    cuda_check(cudaMemcpyAsync(hio.rv, rv, (size_t)nr * 4, cudaMemcpyHostToDevice, st), "H2D R vals");
+    cuda_check(cudaEventRecord(r_copied, st), "cudaEventRecord");
+    cuda_check(cudaMemsetAsync(counters, 0, (size_t)kCntWords * 8, st), "counter reset");
+    launch(JoinIO{hio.rk, hio.rv, hio.sk, hio.sv, nr, std::min(chunk, ns), out}, kRunPartR | kRunBloom, false);
+    // S: chunk c into buffer c % 2; its copy waits for R's copy (first chunk) or for the end of the
+    // passes of chunk c - 2 (same buffer); its passes wait for its copy
+    for (int64_t c = 0; c < nc; ++c) {
+        const int b = (int)(c & 1);
+        const int64_t off = c * chunk, n = std::min(chunk, ns - off);
+        uint32_t* dk = hio.sk + (size_t)b * chunk;
+        uint32_t* dv = hio.sv + (size_t)b * chunk;
+        if (c == 0) cuda_check(cudaStreamWaitEvent(copy_stream, r_copied, 0), "cudaStreamWaitEvent");
+        if (c >= 2) cuda_check(cudaStreamWaitEvent(copy_stream, chunk_free[b], 0), "cudaStreamWaitEvent");
+        cuda_check(cudaMemcpyAsync(dk, sk + off, (size_t)n * 4, cudaMemcpyHostToDevice, copy_stream), "H2D S keys");
+        cuda_check(cudaMemcpyAsync(dv, sv + off, (size_t)n * 4, cudaMemcpyHostToDevice, copy_stream), "H2D S vals");
+        cuda_check(cudaEventRecord(chunk_copied[b], copy_stream), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(st, chunk_copied[b], 0), "cudaStreamWaitEvent");
+        launch(JoinIO{hio.rk, hio.rv, dk, dv, nr, n, out}, kRunPartS | kRunProbe, true);
+        cuda_check(cudaEventRecord(chunk_free[b], st), "cudaEventRecord");
+    }
+    cuda_check(cudaEventRecord(done_, st), "cudaEventRecord");
+    have_run_ = true;
+    plans_ = plans;
+    caps_.assign(1, cap);
+    d_counters_ = counters;
+    d_gwords_ = a.gwords;
+    nj_ = 1;
 }
 
 void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const JoinIO* joins, int nj,

@@ -133,9 +133,20 @@ public:
     } hio;
     void ensure_host_io(int64_t nr, int64_t ns, int64_t cap, bool key);
     // Stream and events of the host-array entry point: S's inputs are copied on copy_stream after
-    // R's (r_copied) while R's passes run; s_copied marks their arrival.
+    // R's (r_copied) while R's passes run; s_copied marks their arrival. With S in chunks, chunk c
+    // goes to buffer c % 2 (chunk_copied marks its arrival, chunk_free the end of its passes).
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t r_copied = nullptr, s_copied = nullptr;
+    cudaEvent_t chunk_copied[2] = {}, chunk_free[2] = {};
+
+    // Host-array join with S in `chunks` pieces (brig_join_config.s_chunks): R is copied, partitioned
+    // and filtered once; each S chunk is copied into one of two device buffers on copy_stream while
+    // the previous chunk's S passes and probe run on `stream` against the resident R, appending its
+    // pairs to the handle's host-io output buffers. Asynchronous; read the count with
+    // sync_counters.
+    void run_host_chunked(const uint32_t* rk, const uint32_t* rv, int64_t nr, const uint32_t* sk,
+                          const uint32_t* sv, int64_t ns, int chunks, int64_t cap, bool emit_key,
+                          cudaStream_t stream);
 
 private:
     void ensure_workspace(size_t bytes, cudaStream_t stream);

@@ -1813,8 +1813,11 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
     };
     mark(0);
     k_fill_word<<<1, 1, 0, st>>>(a.gwords + kGQueue, 0ull);
-    k_fill_word<<<1, 1, 0, st>>>(a.gwords + kGErrors, 0ull);
-    launches += 2;
+    ++launches;
+    if (!a.keep_errors) {
+        k_fill_word<<<1, 1, 0, st>>>(a.gwords + kGErrors, 0ull);
+        ++launches;
+    }
 
     // ---- R, then S: level 1 and level 2 (the Bloom build sits between them) -----------------
     for (int rel = 0; rel < 2; ++rel) {

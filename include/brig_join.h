@@ -82,7 +82,11 @@ typedef struct brig_join_config {
                                        comfortably in L2, else 2 */
     int32_t max_level1_bits;        /* largest automatic level-1 fan-out, as radix bits (hash mode);
                                        0 = 9 (512 partitions) */
-    int32_t reserved[4];
+    int32_t s_chunks;               /* brig_join_run_host only: S is copied and joined in this many
+                                       chunks against R partitioned once (the reference's s_chunks
+                                       loop, src/hash_kernel.cu:910-1131), so S may exceed device
+                                       memory; 0 or 1 = S in one piece */
+    int32_t reserved[3];
 } brig_join_config;
 
 /* Output of one join. Pairs are written in an unspecified order; the multiset is exact. When the

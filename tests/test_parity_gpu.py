@@ -193,6 +193,38 @@ def test_run_host_overlapped_copies(bj, oracle, torch_cuda, pinned):
             assert_same_pairs(oracle, r, s, exp_r, exp_s)
 
 
+@pytest.mark.parametrize("chunks,bloom,zipf", [(2, 1, 0.0), (3, 0, 0.0), (4, 1, 1.0), (7, 1, 0.0)])
+def test_run_host_s_chunks(bj, oracle, torch_cuda, chunks, bloom, zipf):
+    """S copied and joined in chunks against R partitioned and filtered once (the reference's
+    s_chunks loop): the same pairs as the one-piece join, with a smaller last chunk (|S| is not a
+    multiple of the chunk count), and again on the same handle."""
+    rk, rv, sk, sv = bj.gen_host(55 + chunks, 300_000, 1_000_003, 0.3, zipf_s=zipf)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    with bj.Join(use_bloom=bloom, s_chunks=chunks) as j:
+        for _ in range(2):
+            cnt, r, s = j.run_host(rk, rv, sk, sv, capacity=len(exp_r))
+            assert cnt == len(exp_r)
+            assert_same_pairs(oracle, r, s, exp_r, exp_s)
+        st = j.stats()
+        assert st.count == len(exp_r) and st.overflow == 0
+        assert st.count <= st.s_survivors <= len(sk)
+
+
+def test_run_host_s_chunks_keys_and_overflow(bj, oracle, torch_cuda):
+    rk, rv, sk, sv = bj.gen_host(91, 200_000, 600_000, 0.4)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    with bj.Join(use_bloom=1, s_chunks=5) as j:
+        cnt, r, s, k = j.run_host(rk, rv, sk, sv, capacity=len(exp_r), emit_key=True)
+        assert cnt == len(exp_r)
+        assert np.array_equal(k, rk[r]) and np.array_equal(k, sk[s])
+        # pairs past the capacity are counted but not written, across chunk boundaries
+        cap = len(exp_r) // 3
+        cnt, r, s = j.run_host(rk, rv, sk, sv, capacity=cap, allow_overflow=True)
+        assert cnt == len(exp_r) and len(r) == cap and j.last_status == bj.BRIG_E_OVERFLOW
+        exp = set(zip(exp_r.tolist(), exp_s.tolist()))
+        assert len(set(zip(r.tolist(), s.tolist()))) == cap and all(p in exp for p in zip(r.tolist(), s.tolist()))
+
+
 def test_device_generator_matches_host(bj, torch_cuda):
     n_r, n_s = 300_001, 500_003
     h = bj.gen_host(1234, n_r, n_s, 0.37)
