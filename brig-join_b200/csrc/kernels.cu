@@ -20,12 +20,15 @@
 //     input, the histogram pass records a per-(partition, slice) count, and one exclusive scan of
 //     the partition-major [P1][slices] matrix gives every slice a private output run per partition.
 //     The reference takes one 64-bit global atomic per tuple on P counters (:122,129).
-//   * Tiles are staged in shared memory and reordered by partition before they are written, so
-//     consecutive threads store consecutive addresses of the same partition run.
+//   * Tiles are staged in shared memory and reordered by partition before they are written: up to
+//     1024 partitions each partition's run of a tile goes out as one shared-to-global bulk copy
+//     (its staging slots are placed so the run's source and destination share their 16-byte
+//     alignment); above that consecutive threads store consecutive addresses of one run.
 //   * The probe is a persistent work-queue kernel over (join, partition-pair) tasks. An R partition
 //     larger than one shared-memory table is cut into table-sized chunks, each probed by the whole
 //     S partition, so duplicates are exact (the reference's split path stops at the first match,
-//     :371). A large S partition is cut into chunks that run as separate tasks.
+//     :371). A large S partition is cut into chunks that run as separate tasks. Buckets of
+//     repeated build keys are walked by the whole warp, 32 entries per step.
 //   * Matches are staged per warp in shared memory and written with one global atomic per flush
 //     (the reference takes one global atomic per output pair, :420).
 //   * The shared-memory table is bucketised (counting sort by bucket) rather than open addressing,
