@@ -23,7 +23,9 @@ def test_config_defaults(bj):
     assert cfg.abi_version == bj.ABI_VERSION
     assert cfg.partition_mode == bj.PART_HASH
     assert cfg.bloom_bits_per_key == 10.0 and cfg.use_bloom == 0 and cfg.device == -1
-    assert C.sizeof(bj.Config) == 88  # layout of brig_join_config
+    assert cfg.s_chunks == 0  # S in one piece
+    assert C.sizeof(bj.Config) == 88  # layout of brig_join_config (s_chunks took a reserved slot)
+    assert bj.Config.s_chunks.offset == 72 and bj.Config.reserved.offset == 76
 
 
 @pytest.mark.parametrize("n_r,n_s,kw,expect", [
@@ -54,6 +56,9 @@ def test_planner_rejects_bad_configs(bj):
     assert e.value.status == bj.BRIG_E_UNSUPPORTED
     with pytest.raises(bj.BrigError) as e:
         bj.plan(-1, 10)
+    assert e.value.status == bj.BRIG_E_INVALID
+    with pytest.raises(bj.BrigError) as e:
+        bj.plan(1000, 1000, s_chunks=-2)
     assert e.value.status == bj.BRIG_E_INVALID
     cfg = bj.make_config()
     cfg.abi_version = 99
