@@ -6,7 +6,7 @@ Default workload: the full-size single join, |R| = |S| = 640,000,000 uint32 (key
 with 7 hashes. A step is one complete join (partition R and S, build and probe the Bloom filter,
 shared-memory hash build and probe, pair materialisation) over inputs resident in HBM.
 
-  python bench.py [--gpus N --steps K --warmup W] [--workload c1|c0] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--workload c1|c0|batch|serve|sweep] [--impl reference]
 
 One JSON line on rank 0. `value` is the device-timed join throughput (|R|+|S|)/t over all ranks;
 `e2e` the same metric through the host-array C entry point (H2D inputs, join, D2H pairs; S in
@@ -315,6 +315,54 @@ def run_batch_workload(args):
     return 0
 
 
+# ---- selectivity and Bloom sweep ------------------------------------------------------------------
+def run_sweep_workload(args):
+    """|R| = 2^26, |S| = 2^30, a fraction of S drawn from R (0.1%, 1%, 10%, 100%), the filter off or on
+    at 8, 10 and 14 bits/key: device time per join, survivors and the chosen probe level. Every
+    count is checked against the constructed match count."""
+    import torch
+    import brig_join as bj
+    torch.cuda.set_device(0)
+    nr, ns = 1 << 26, 1 << 30
+    if args.rows > 0:
+        nr, ns = args.rows, 16 * args.rows
+    i32 = torch.int32
+    rk, rv = (torch.empty(nr, dtype=i32, device="cuda") for _ in range(2))
+    sk, sv = (torch.empty(ns, dtype=i32, device="cuda") for _ in range(2))
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+    rows = []
+    for frac in (0.001, 0.01, 0.1, 1.0):
+        bj.gen_device(7, nr, ns, frac, 0.0, rk, rv, sk, sv, stream=sp)
+        m = int(math.floor(frac * ns))
+        cap = m + 4096
+        out_r = torch.empty(cap, dtype=i32, device="cuda")
+        out_s = torch.empty(cap, dtype=i32, device="cuda")
+        for bpk in (0, 8.0, 10.0, 14.0):
+            kw = dict(use_bloom=1, bloom_bits_per_key=bpk) if bpk else dict(use_bloom=0)
+            with bj.Join(**kw) as j:
+                for _ in range(max(args.warmup, 1)):
+                    j.run(rk, rv, nr, sk, sv, ns, out_r, out_s, cap, stream=sp)
+                st = j.stats()
+                assert st.count == m, (frac, bpk, st.count, m)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                steps = max(1, min(args.steps, 5))
+                e0.record(stream)
+                for _ in range(steps):
+                    j.run(rk, rv, nr, sk, sv, ns, out_r, out_s, cap, stream=sp)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / steps
+                rows.append({"match": frac, "bloom_bits_per_key": bpk, "ms": round(ms, 3),
+                             "g_tuples_per_s": round((nr + ns) / ms / 1e6, 2), "count": st.count,
+                             "s_survivors": st.s_survivors, "bloom_num_hashes": st.bloom_num_hashes})
+        del out_r, out_s
+    line = {"metric": "join tuples/s ((|R|+|S|)/t) across selectivity and Bloom size", "unit": UNIT,
+            "n_r": nr, "n_s": ns, "data": "synthetic", "dtype": "u32", "sweep": rows}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---- served joins ---------------------------------------------------------------------------------
 def run_serve_workload(args):
     """Poisson stream of join requests against a 120 GB budget: p50/p99 latency and aggregate
@@ -408,7 +456,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["batch", "serve"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["batch", "serve", "sweep"])
     ap.add_argument("--joins", type=int, default=256, help="batch workload: number of joins")
     ap.add_argument("--pool", type=int, default=24, help="serve workload: distinct requests")
     ap.add_argument("--requests", type=int, default=64, help="serve workload: requests per load point")
@@ -432,6 +480,8 @@ def main():
         ap.error("--steps above 64: per-stage events keep the last 64 runs")
     if args.workload == "batch":
         return run_batch_workload(args)
+    if args.workload == "sweep":
+        return run_sweep_workload(args)
     if args.workload == "serve":
         return run_serve_workload(args)
     wl = dict(WORKLOADS[args.workload])
