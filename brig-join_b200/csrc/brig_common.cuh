@@ -198,19 +198,22 @@ BRIG_HD void bloom_place(uint64_t g, uint32_t seg_blocks, BloomKey& bk) {
     bk.wb = bk.wa + 1u;
 }
 
-// Compile-time k class of a join's filter: the Bloom kernels are instantiated for k = 7 (the usual
-// 10 bits/key setting) and for any k, and each instantiation skips the other's joins.
-constexpr int kBloomFastK = 7;
+// Compile-time mask class of a join's filter: the Bloom kernels are instantiated for the pattern
+// tables below (every join whose k is the k the launch's tables were filled for: all of them, as
+// the joins of one launch share their configuration) and for the bit arithmetic of bloom_masks (any
+// other k), and each instantiation skips the other's joins.
+constexpr int kBloomFastK = 7;  // template tag of the pattern-table instantiations
 
-// For k = 7 the masks are pattern-blocked (Lang et al., as above): hash bits 0..9 pick one of 1024
-// 4-bit patterns for the even word and bits 10..19 one of 1024 3-bit patterns for the odd
-// word. Pattern i of word w is the OR of 1 << (5-bit fields of a SplitMix64 hash of (w, i)), so the
-// two table look-ups replace the shifts of seven bit positions. The kernels that build or probe a
-// k = 7 filter keep both tables (8 KB) in shared memory.
+// The masks are pattern-blocked (Lang et al., as above): hash bits 0..9 pick one of 1024 patterns
+// of ceil(k/2) bits for the even word and bits 10..19 one of 1024 patterns of floor(k/2) bits for
+// the odd word. Pattern i of word w is the OR of 1 << (5-bit fields of a SplitMix64 hash of (w, i)),
+// so two table look-ups replace the shifts of k bit positions. The kernels that build or probe a
+// filter keep both tables (8 KB), filled for the launch's k, in shared memory. For k = 7 (4 + 3
+// bits) the tables are the ones the k = 7 filters have always used.
 constexpr int kPatterns = 1024;
-BRIG_HD uint32_t bloom_pattern(int word, uint32_t i) {
+BRIG_HD uint32_t bloom_pattern(int word, uint32_t i, int k) {
     const uint64_t h = mix64(((uint64_t)(word + 1) << 32) ^ (uint64_t)i ^ 0x243f6a8885a308d3ull);
-    const int nb = word == 0 ? 4 : 3;
+    const int nb = word == 0 ? (k + 1) / 2 : k / 2;  // at most 8 fields of 5 bits
     uint32_t m = 0;
     for (int b = 0; b < nb; ++b) m |= 1u << ((uint32_t)(h >> (5 * b)) & 31u);
     return m;
@@ -254,7 +257,7 @@ struct JoinDesc {
     int32_t bloom_level;   // S pass that probes the filter: 1 first (fused with the histogram of
                            // S's level-1 pass), 2 second (fused with S's level-2 pass)
     int32_t bloom_group;   // consecutive finest partitions per Bloom build CTA
-    int32_t pad0;
+    int32_t bloom_pat;     // 1: the masks come from the launch's pattern tables (bloom_k is their k)
     int64_t dom_base;      // offset of this join's task domains in the global task-count array
     int64_t fine_base;     // unused (kept zero)
     int32_t table_cap;     // max build-side tuples per probe task

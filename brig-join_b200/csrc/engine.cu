@@ -483,6 +483,11 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     if (T < kMinTable || T > kMaxTable || !is_pow2(T))
         fail(BRIG_E_INVALID, "table_capacity must be a power of two in [256, 4096]");
     if (C < 1) fail(BRIG_E_INVALID, "s_chunk must be >= 1");
+    // The Bloom kernels fill their pattern tables for the k of the first filtered join: the joins of
+    // one run share their configuration, so that is every filtered join's k.
+    int pat_k = 0;
+    for (int j = 0; j < nj && !pat_k; ++j)
+        if (plans[j].bloom) pat_k = plans[j].k;
     JoinDesc* hJ = reinterpret_cast<JoinDesc*>(meta_host);
     int64_t* hpre = reinterpret_cast<int64_t*>(meta_host + (size_t)nj * sizeof(JoinDesc));
     int64_t* sp0 = hpre;
@@ -533,6 +538,7 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
         d.fine_base = 0;
         d.dom_base = finep[j];
         d.bloom_group = p.bloom_group;
+        d.bloom_pat = (p.bloom && p.k == pat_k) ? 1 : 0;
         d.table_cap = T;
         d.s_chunk = C;
         hJ[j] = d;
@@ -585,8 +591,9 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     a.any_bloom_l2 = sh.any_bloom_l2 ? 1 : 0;
     a.modes = 0;
     for (int j = 0; j < nj; ++j) a.modes |= plans[j].pf.mode == 0 ? 1 : 2;
+    a.pat_k = pat_k;
     a.kclasses = 0;
-    for (int j = 0; j < nj; ++j) a.kclasses |= (plans[j].bloom && plans[j].k == kBloomFastK) ? 2 : 1;
+    for (int j = 0; j < nj; ++j) a.kclasses |= (plans[j].bloom && plans[j].k == a.pat_k) ? 2 : 1;
     a.num_sms = num_sms;
     a.stage_events = nullptr;
     a.stages = kRunAll;

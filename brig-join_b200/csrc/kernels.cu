@@ -546,21 +546,21 @@ __device__ __forceinline__ void init_bars(uint64_t* bars) {
 
 // Bloom probe, split in two so a thread can have several block loads in flight: the address of a
 // key's 32-byte block in the segment of its finest partition f, then the test of the loaded words.
-// Bit masks of a key with hash g: the shared-memory pattern tables for k = 7 (pat), the bit
-// arithmetic for any other k.
+// Bit masks of a key with hash g: the shared-memory pattern tables (pat), or the bit arithmetic for
+// a join whose k differs from the tables' k.
 template <int K>
 __device__ __forceinline__ void key_masks(const uint32_t* pat, uint64_t g, int k, uint32_t& ma, uint32_t& mb) {
     if constexpr (K == kBloomFastK) bloom_pattern_masks(pat, g, ma, mb);
     else bloom_masks<0>(g, k, ma, mb);
 }
-// Fills the two pattern tables of a k = 7 kernel (block-wide; the caller synchronises).
-__device__ __forceinline__ void fill_patterns(uint32_t* pat) {
-    for (int i = threadIdx.x; i < 2 * kPatterns; i += blockDim.x) pat[i] = bloom_pattern(i / kPatterns, i % kPatterns);
+// Fills the two pattern tables for k (block-wide; the caller synchronises).
+__device__ __forceinline__ void fill_patterns(uint32_t* pat, int k) {
+    for (int i = threadIdx.x; i < 2 * kPatterns; i += blockDim.x) pat[i] = bloom_pattern(i / kPatterns, i % kPatterns, k);
 }
 
-// The Bloom k class of a join (the K of the kernel instantiation that handles it).
+// The Bloom mask class of a join (the K of the kernel instantiation that handles it).
 __device__ __forceinline__ int bloom_kclass(const JoinDesc& d) {
-    return (d.bloom != nullptr && d.bloom_k == kBloomFastK) ? kBloomFastK : 0;
+    return (d.bloom != nullptr && d.bloom_pat) ? kBloomFastK : 0;
 }
 
 // Address of the first word of a key's block in the segment of finest partition f.
@@ -579,11 +579,11 @@ constexpr int kL2ProbeILP = 6;  // keys per thread with their filter words in fl
 template <int M, int K>
 __global__ void __launch_bounds__(kThreads, 2)
 k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
-          uint32_t* __restrict__ hist, unsigned long long* gwords) {
+          uint32_t* __restrict__ hist, unsigned long long* gwords, int pat_k) {
     extern __shared__ uint32_t sh_cnt[];  // [max P1]
     __shared__ uint32_t s_cursor;
-    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // k = 7 pattern tables
-    if constexpr (K == kBloomFastK) fill_patterns(s_pat);  // synchronised by the slice loop's first barrier
+    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // pattern tables
+    if constexpr (K == kBloomFastK) fill_patterns(s_pat, pat_k);  // synchronised by the slice loop's first barrier
     const int lane = threadIdx.x & 31;
     const int64_t total = slice_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
@@ -859,11 +859,12 @@ template <bool kBloom, int M, int K>
 __global__ void __launch_bounds__(kThreads, 2)
 k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
           const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
-          uint32_t* __restrict__ hist2, uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords) {
+          uint32_t* __restrict__ hist2, uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords,
+          int pat_k) {
     extern __shared__ uint32_t cnt[];  // [max P2]
     __shared__ uint32_t s_surv;
-    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // k = 7 pattern tables
-    if constexpr (K == kBloomFastK && kBloom) fill_patterns(s_pat);  // synchronised by the slice loop's first barrier
+    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // pattern tables
+    if constexpr (K == kBloomFastK && kBloom) fill_patterns(s_pat, pat_k);  // synchronised by the slice loop's first barrier
     const int lane = threadIdx.x & 31;
     const int64_t total = (int64_t)gwords[kGL2Slices + rel];
     for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
@@ -1045,10 +1046,10 @@ __global__ void k_l2_bounds(const JoinDesc* __restrict__ J, int nj, int rel, con
 template <int M, int K>
 __global__ void __launch_bounds__(kThreads)
 k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ bloom_prefix,
-              int smem_words, unsigned long long* gwords) {
+              int smem_words, unsigned long long* gwords, int pat_k) {
     extern __shared__ __align__(16) uint32_t seg[];
-    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // k = 7 pattern tables
-    if constexpr (K == kBloomFastK) fill_patterns(s_pat);  // synchronised by the group loop's first barrier
+    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // pattern tables
+    if constexpr (K == kBloomFastK) fill_patterns(s_pat, pat_k);  // synchronised by the group loop's first barrier
     const int64_t total = bloom_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(bloom_prefix, nj, g);
@@ -1831,7 +1832,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 constexpr int M = decltype(mt)::value, K = decltype(kt)::value;
                 k_bloom_build<M, K><<<grid_for(a.total_bloom_groups, sms, 4), kThreads,
                                    (size_t)a.bloom_smem_words * 4, st>>>(a.J, a.nj, a.bloom_prefix,
-                                                                         a.bloom_smem_words, a.gwords);
+                                                                         a.bloom_smem_words, a.gwords, a.pat_k);
                 ++launches;
             });
         }
@@ -1846,7 +1847,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
             for_mode_k(a.modes, a.kclasses, [&](auto mt, auto kt) {
                 constexpr int M = decltype(mt)::value, K = decltype(kt)::value;
                 k_l1_hist<M, K><<<grid_for(a.total_slices[rel], sms, 4), kThreads, (size_t)a.max_p1 * 4, st>>>(
-                    a.J, a.nj, rel, a.slice_prefix[rel], a.hist, a.gwords);
+                    a.J, a.nj, rel, a.slice_prefix[rel], a.hist, a.gwords, a.pat_k);
                 ++launches;
             });
         }
@@ -1892,7 +1893,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 const dim3 grid(grid_for(a.l2_slice_cap[rel], sms, 4));
                 k_l2_hist<false, M, 0><<<grid, kThreads, (size_t)a.max_p2 * 4, st>>>(
                     a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2,
-                    a.gwords);
+                    a.gwords, 0);
                 ++launches;
             });
             if (rel == 1 && a.any_bloom_l2) {
@@ -1900,7 +1901,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                     constexpr int M = decltype(mt)::value, K = decltype(kt)::value;
                     k_l2_hist<true, M, K><<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4,
                                             st>>>(a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs,
-                                                  a.hist2, a.slice_cnt2, a.gwords);
+                                                  a.hist2, a.slice_cnt2, a.gwords, a.pat_k);
                     ++launches;
                 });
             }

@@ -41,7 +41,9 @@ struct PipelineArgs {
     int any_bloom_l1;                 // some join probes its filter in S's first pass
     int any_bloom_l2;                 // some join probes its filter in S's second pass
     int modes;                        // partition modes present: bit 0 hash, bit 1 modulo
-    int kclasses;                     // Bloom k classes present: bit 0 any k (or no filter), bit 1 k = 7
+    int kclasses;                     // Bloom mask classes present: bit 0 bit arithmetic (or no filter),
+                                      // bit 1 pattern tables
+    int pat_k;                        // k the Bloom kernels fill their pattern tables for
     int num_sms;
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
     cudaEvent_t s_ready;              // when set, S's passes wait for it (its inputs are still arriving)

@@ -37,6 +37,20 @@ def test_bloom_probe_levels(bj, oracle, torch_cuda, level, mode, p1, p2):
     assert st.count == 30_000 and st.count <= st.s_survivors < 600_000 // 4
 
 
+@pytest.mark.parametrize("bpk,k", [(8.0, 0), (14.0, 0), (10.0, 1), (10.0, 4), (16.0, 16)])
+@pytest.mark.parametrize("level", [1, 2])
+def test_bloom_pattern_tables_any_k(bj, oracle, torch_cuda, bpk, k, level):
+    """The filter's masks come from pattern tables filled for the join's k (ceil(k/2) bits in one
+    word of the pair, floor(k/2) in the other) for every k, not only k = 7: exact pairs, and the
+    survivors stay a small superset of the matches."""
+    rk, rv, sk, sv = bj.gen_host(61 + level, 400_000, 600_000, 0.05)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=1, bloom_bits_per_key=bpk,
+                 bloom_num_hashes=k, bloom_probe_level=level, partition_size=16, second_partition_size=16)
+    assert st.count == 30_000
+    assert st.bloom_num_hashes == (k or round(bpk * 0.6931471805599453))
+    assert st.count <= st.s_survivors < 600_000 // 4
+
+
 @pytest.mark.parametrize("p1,p2", [(16, 16), (64, 8), (1, 1), (4096, 1), (2, 1024)])
 def test_two_level_hash_fanouts(bj, oracle, torch_cuda, p1, p2):
     rk, rv, sk, sv = bj.gen_host(11, 300_000, 200_000, 0.3)
