@@ -571,7 +571,7 @@ def main():
     avg = stages
     blvl = 0
     if wl["bloom"]:
-        blvl = args.bloom_level or (1 if st.bloom_num_bits // 8 <= (64 << 20) or st.second_partition_size <= 1
+        blvl = args.bloom_level or (1 if st.bloom_num_bits // 8 <= (96 << 20) or st.second_partition_size <= 1
                                     else 2)
     sb = stage_bytes(nr, ns, st.s_survivors, st.count, st.bloom_num_bits, blvl)
     dom = max(avg, key=avg.get)

@@ -28,7 +28,11 @@ static int ceil_log2(int64_t x) {
 }
 static bool is_pow2(int64_t x) { return x > 0 && (x & (x - 1)) == 0; }
 
-// Filter bytes that a first-pass Bloom probe may touch and still find in L2.
+// Filter bytes up to which one join probes its filter in S's first pass: 96 MB. At |R| = 2^26,
+// |S| = 2^30 an 80 MB filter probed there took 10.4 ms against 12.5 ms in the second pass at a 0.1%
+// match rate (14.7 against 14.6 ms at 10%); 112 MB and up are faster in the second pass.
+constexpr int64_t kL1FilterBytes = 96ll << 20;
+// Filter bytes that the first-pass probes of one batch may touch together (they share L2).
 constexpr int64_t kL2FilterBytes = 64ll << 20;
 
 JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
@@ -107,7 +111,7 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
         // while the filter stays in the 126 MB L2. A larger filter is probed in S's second pass,
         // one level-1 partition (a contiguous run of segments) at a time.
         int lvl = cfg.bloom_probe_level;
-        if (lvl == 0) lvl = (p.bloom_bits / 8 <= kL2FilterBytes) ? 1 : 2;
+        if (lvl == 0) lvl = (p.bloom_bits / 8 <= kL1FilterBytes) ? 1 : 2;
         if (lvl != 1 && lvl != 2) fail(BRIG_E_INVALID, "bloom_probe_level must be 0, 1 or 2");
         if (f.P2 == 1) lvl = 1;
         p.bloom_level = lvl;
@@ -118,7 +122,7 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
 std::vector<JoinPlan> plan_batch(const brig_join_config& cfg, const int64_t* nr, const int64_t* ns, int nj) {
     std::vector<JoinPlan> plans(nj);
     for (int j = 0; j < nj; ++j) plans[j] = plan_join(cfg, nr[j], ns[j]);
-    if (cfg.bloom_probe_level != 0) return plans;
+    if (cfg.bloom_probe_level != 0 || nj <= 1) return plans;
     // One first-pass probe launch covers every join of the batch, so their filters share L2.
     // While they do not fit, the largest joins that have a second pass probe there instead.
     int64_t l1 = 0;

@@ -36,9 +36,9 @@ struct JoinPlan {
     int64_t bloom_bits = 0;     // allocated bits
 };
 JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns);
-// Plans of the joins of one pipeline run: plan_join for each, then (with bloom_probe_level 0) the
-// largest two-level joins move their Bloom probe to S's second pass until the filters probed in
-// the first pass fit L2 together.
+// Plans of the joins of one pipeline run: plan_join for each, then (with bloom_probe_level 0 and
+// more than one join) the largest two-level joins move their Bloom probe to S's second pass until
+// the filters probed in the first pass fit the batch's L2 budget together.
 std::vector<JoinPlan> plan_batch(const brig_join_config& cfg, const int64_t* nr, const int64_t* ns, int nj);
 
 // One join of a pipeline run, as given by the caller.
