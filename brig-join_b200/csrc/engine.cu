@@ -119,10 +119,11 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
     return p;
 }
 
-std::vector<JoinPlan> plan_batch(const brig_join_config& cfg, const int64_t* nr, const int64_t* ns, int nj) {
+std::vector<JoinPlan> plan_batch(const brig_join_config& cfg, const int64_t* nr, const int64_t* ns, int nj,
+                                 bool shared_l2) {
     std::vector<JoinPlan> plans(nj);
     for (int j = 0; j < nj; ++j) plans[j] = plan_join(cfg, nr[j], ns[j]);
-    if (cfg.bloom_probe_level != 0 || nj <= 1) return plans;
+    if (cfg.bloom_probe_level != 0 || (nj <= 1 && !shared_l2)) return plans;
     // One first-pass probe launch covers every join of the batch, so their filters share L2.
     // While they do not fit, the largest joins that have a second pass probe there instead.
     int64_t l1 = 0;
@@ -623,7 +624,7 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
         nr[j] = joins[j].nr;
         ns[j] = joins[j].ns;
     }
-    std::vector<JoinPlan> plans = plan_batch(cfg_, nr.data(), ns.data(), nj);
+    std::vector<JoinPlan> plans = plan_batch(cfg_, nr.data(), ns.data(), nj, shared_l2_);
     std::vector<JoinOffs> jo(nj);
     Shape sh;
     layout_for(cfg_, plans.data(), nj, num_sms_, jo.data(), sh);

@@ -36,10 +36,12 @@ struct JoinPlan {
     int64_t bloom_bits = 0;     // allocated bits
 };
 JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns);
-// Plans of the joins of one pipeline run: plan_join for each, then (with bloom_probe_level 0 and
-// more than one join) the largest two-level joins move their Bloom probe to S's second pass until
-// the filters probed in the first pass fit the batch's L2 budget together.
-std::vector<JoinPlan> plan_batch(const brig_join_config& cfg, const int64_t* nr, const int64_t* ns, int nj);
+// Plans of the joins of one pipeline run: plan_join for each, then (with bloom_probe_level 0, and
+// more than one join or an L2 shared with other runs in flight) the largest two-level joins move
+// their Bloom probe to S's second pass until the filters probed in the first pass fit the shared
+// L2 budget together.
+std::vector<JoinPlan> plan_batch(const brig_join_config& cfg, const int64_t* nr, const int64_t* ns, int nj,
+                                 bool shared_l2 = false);
 
 // One join of a pipeline run, as given by the caller.
 struct JoinIO {
@@ -114,6 +116,10 @@ public:
         ensure_workspace(bytes, stream);
     }
     const brig_join_config& config() const { return cfg_; }
+    // Runs of this engine share the GPU's L2 with other engines' runs in flight (the serving
+    // loop's slots): first-pass Bloom probes keep to the shared budget even for one join.
+    void set_shared_l2(bool on) { shared_l2_ = on; }
+    bool shared_l2() const { return shared_l2_; }
     int device() const { return device_; }
     const std::vector<int64_t>& last_caps() const { return caps_; }
     // Mean milliseconds of each pipeline stage over the runs since the previous call (at most the
@@ -162,6 +168,7 @@ private:
     cudaEvent_t stage_free_ = nullptr;  // recorded after the staging copy
     cudaEvent_t done_ = nullptr;        // recorded after the last run
     bool have_run_ = false;
+    bool shared_l2_ = false;
     std::vector<JoinPlan> plans_;
     std::vector<int64_t> caps_;
     int64_t* d_counters_ = nullptr;  // [nj * kCntWords] of the last run

@@ -72,8 +72,7 @@ struct Server {
     }
     // io_bytes plus the workspace of the request joined alone (the admission bound).
     int64_t footprint(const brig_serve_request& r, int64_t cap) const {
-        const JoinPlan p = plan_join(jcfg, r.n_r, r.n_s);
-        return Engine::workspace_needed(jcfg, {p}, num_sms) + io_bytes(r, cap);
+        return Engine::workspace_needed(jcfg, plan_batch(jcfg, &r.n_r, &r.n_s, 1, true), num_sms) + io_bytes(r, cap);
     }
     int64_t wave_workspace(const std::vector<Req*>& w) const {
         std::vector<int64_t> nr, ns;
@@ -81,7 +80,7 @@ struct Server {
             nr.push_back(q->in.n_r);
             ns.push_back(q->in.n_s);
         }
-        return Engine::workspace_needed(jcfg, plan_batch(jcfg, nr.data(), ns.data(), (int)w.size()), num_sms);
+        return Engine::workspace_needed(jcfg, plan_batch(jcfg, nr.data(), ns.data(), (int)w.size(), true), num_sms);
     }
 
     // Request buffers are stream-ordered allocations on the slot's stream, so allocating and
@@ -322,6 +321,7 @@ int brig_serve_create(const brig_join_config* jcfg, const brig_serve_config* scf
                 brig::cuda_check(cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking), "cudaStreamCreate");
                 brig::cuda_check(cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming), "cudaEventCreate");
                 sl.eng = new brig::Engine(s->jcfg);
+                sl.eng->set_shared_l2(true);  // the slots' waves run side by side
             }
         } catch (...) {
             for (auto& sl : s->slots) {
