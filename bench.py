@@ -36,11 +36,12 @@ METRIC = "join tuples/s ((|R|+|S|)/t)"
 UNIT = "tuples/s"
 WORKLOADS = {
     "c1": dict(name="join 640M x 640M, 10% match, Bloom 10 bits/key k=7", n_r=640_000_000,
-               n_s=640_000_000, match=0.1, bloom=1, bpk=10.0, k=7),
-    "c0": dict(name="join 16M x 16M, 10% match, Bloom 10 bits/key k=7", n_r=1 << 24, n_s=1 << 24,
-               match=0.1, bloom=1, bpk=10.0, k=7),
+               n_s=640_000_000, match=0.1, bloom=1, bpk=10.0, k=7, mode=0, p1=0),
+    # the reference's README preset: --partition_size 512, i.e. first-level fan-out 512 by key % 512
+    # (second level auto: 67, the reference's starting odd fan-out)
+    "c0": dict(name="join 16M x 16M, 10% match, Bloom 10 bits/key k=7, fan-out 512 (key % 512)",
+               n_r=1 << 24, n_s=1 << 24, match=0.1, bloom=1, bpk=10.0, k=7, mode=1, p1=512),
 }
-CPU_SAMPLE = 1 << 25  # rows per relation in the bounded CPU-baseline sample
 
 
 def peaks():
@@ -106,59 +107,65 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-# ---- CPU baseline: the reference's run_sanity_check on a bounded sample ---------------------------
-def cpu_reference_sample(bj, n, match, seed, min_seconds, max_reps):
+# ---- CPU baseline and reference arm: the reference's run_sanity_check on the benchmark's inputs ----
+def workload_config(wl, world):
+    """The workload's `config` object, identical in both arms."""
+    nr, ns = wl["n_r"], wl["n_s"]
+    return {"workload": wl["name"], "n_r": nr, "n_s": ns, "match_frac": wl["match"],
+            "bloom_bits_per_key": wl["bpk"] if wl["bloom"] else 0, "bloom_hashes": wl["k"] if wl["bloom"] else 0,
+            "partition_mode": "modulo" if wl["mode"] == 1 else "hash",
+            "partition_size": wl["p1"] if wl["p1"] else "auto",
+            "l2": f"no flush: each step streams {8 * (nr + ns) / 1e9:.2f} GB of inputs"
+                  + (", far above the 126 MB L2" if 8 * (nr + ns) > 4 * 126e6 else ", a few times the 126 MB L2"),
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def cpu_join_runs(rk, sk, reps, min_seconds=0.0):
+    """Times the reference's own run_sanity_check (oracle/_ref, built from its sources) on int32
+    views of the keys, or the oracle's restatement of it where the reference was not built:
+    (kind, cores, seconds per run, count)."""
     from oracle import oracle as o
-    rk, _, sk, _ = bj.gen_host(seed, n, n, match)
     times, count = [], None
-    if o.ref_available():
-        kind, cores = "reference", o.ref_threads()
-        t_end = time.time() + min_seconds
-        while len(times) < max_reps and (len(times) < 2 or time.time() < t_end):
-            c, sec = o.ref_count(rk, sk)
-            times.append(sec)
-            count = c
-    else:
-        kind, cores = "port", 1
-        t_end = time.time() + min_seconds
-        while len(times) < max_reps and (len(times) < 2 or time.time() < t_end):
+    t_end = time.time() + min_seconds
+    while len(times) < reps or (time.time() < t_end and len(times) < 4 * reps):
+        if o.ref_available():
+            count, sec = o.ref_count(rk, sk)
+        else:
             t0 = time.perf_counter()
             count = o.count(rk, sk)
-            times.append(time.perf_counter() - t0)
-    return kind, cores, times, count
+            sec = time.perf_counter() - t0
+        times.append(sec)
+    if o.ref_available():
+        return "reference", o.ref_threads(), times, count
+    return "port", 1, times, count
 
 
 def run_reference_arm(args, wl):
+    """The reference's CPU join on the full workload: inputs from the oracle's restatement of the
+    generator (row-identical to the engine's, checked in the tests), W untimed and K timed runs of
+    run_sanity_check. Loads no engine library."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return 0
-    import brig_join as bj
     from oracle import oracle as o
-    n = CPU_SAMPLE
-    rk, _, sk, _ = bj.gen_host(42, n, n, wl["match"])
-    if o.ref_available():
-        kind, cores = "reference", o.ref_threads()
-        fn = lambda: o.ref_count(rk, sk)[1]
-    else:
-        kind, cores = "port", 1
-
-        def fn():
-            t0 = time.perf_counter()
-            o.count(rk, sk)
-            return time.perf_counter() - t0
-    for _ in range(args.warmup):
-        fn()
-    secs = [fn() for _ in range(args.steps)]
+    nr, ns = wl["n_r"], wl["n_s"]
+    rk, _, sk, _ = o.gen(42, nr, ns, wl["match"], want_vals=False)
+    m = int(math.floor(wl["match"] * ns))
+    kind, cores, _, c = cpu_join_runs(rk, sk, max(args.warmup, 0))
+    assert args.warmup == 0 or c == m, f"reference count {c} != {m}"
+    kind, cores, secs, c = cpu_join_runs(rk, sk, args.steps)
+    assert c == m, f"reference count {c} != {m}"
     t = sum(secs)
-    value = args.steps * 2 * n / t
+    value = args.steps * (nr + ns) / t
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": wl["name"], "n_r": wl["n_r"], "n_s": wl["n_s"], "match_frac": wl["match"]},
+        "config": workload_config(wl, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"{n} x {n} rows of the same generator ({wl['match']:.0%} matching), "
-                                   f"one run_sanity_check per step (count only, as the reference)"},
+                         "sample": f"the full workload ({nr} x {ns} rows, {m} matches), one run_sanity_check "
+                                   f"(count only, as the reference) per step on {cores} host threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -471,6 +478,7 @@ def main():
                     help="override |R| = |S| (a smaller case of the same generator, e.g. for ncu)")
     ap.add_argument("--p1", type=int, default=0, help="override the level-1 fan-out")
     ap.add_argument("--p2", type=int, default=0, help="override the level-2 fan-out")
+    ap.add_argument("--mode", type=int, default=None, help="override the partition mode (0 hash, 1 modulo)")
     ap.add_argument("--table", type=int, default=0, help="override table_capacity")
     ap.add_argument("--s-chunks", type=int, default=-1,
                     help="e2e: copy and join S in this many chunks against R partitioned once (s_chunks); "
@@ -487,6 +495,10 @@ def main():
     wl = dict(WORKLOADS[args.workload])
     if args.bloom is not None:
         wl["bloom"] = args.bloom
+    if args.p1:
+        wl["p1"] = args.p1
+    if args.mode is not None:
+        wl["mode"] = args.mode
     if args.rows > 0:
         wl["n_r"] = wl["n_s"] = args.rows
         wl["name"] = f"join {args.rows} x {args.rows}, 10% match" + (
@@ -521,9 +533,10 @@ def main():
     cap = m + m // 50 + 4096
     out_r = torch.empty(cap, dtype=i32, device="cuda")
     out_s = torch.empty(cap, dtype=i32, device="cuda")
-    j = bj.Join(use_bloom=wl["bloom"], bloom_bits_per_key=wl["bpk"], bloom_num_hashes=wl["k"],
-                bloom_probe_level=args.bloom_level, use_cuda_graph=1, profile_stages=1,
-                partition_size=args.p1, second_partition_size=args.p2, table_capacity=args.table)
+    jcfg = dict(use_bloom=wl["bloom"], bloom_bits_per_key=wl["bpk"], bloom_num_hashes=wl["k"],
+                bloom_probe_level=args.bloom_level, partition_mode=wl["mode"], partition_size=wl["p1"],
+                second_partition_size=args.p2, table_capacity=args.table)
+    j = bj.Join(use_cuda_graph=1, profile_stages=1, **jcfg)
 
     def step():
         j.run(rk, rv, nr, sk, sv, ns, out_r, out_s, cap, stream=sp)
@@ -594,9 +607,7 @@ def main():
         if args.s_chunks < 0:
             args.s_chunks = 16 if ns >= (1 << 26) else 0
         if args.s_chunks > 1:
-            jh = bj.Join(use_bloom=wl["bloom"], bloom_bits_per_key=wl["bpk"], bloom_num_hashes=wl["k"],
-                         bloom_probe_level=args.bloom_level, partition_size=args.p1, second_partition_size=args.p2,
-                         table_capacity=args.table, s_chunks=args.s_chunks)
+            jh = bj.Join(s_chunks=args.s_chunks, **jcfg)
         for it in range(args.e2e_steps + 1):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
@@ -620,23 +631,27 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        kind, cores, secs, _ = cpu_reference_sample(bj, CPU_SAMPLE, wl["match"], 42, min_seconds=10.0, max_reps=12)
-        cpu = {"value": 2 * CPU_SAMPLE / (sum(secs) / len(secs)), "unit": UNIT, "cores": cores, "kind": kind,
-               "sample": f"{CPU_SAMPLE} x {CPU_SAMPLE} rows of the same generator, {len(secs)} runs of "
-                         f"run_sanity_check (count only)"}
+        # the reference's CPU join on this run's own inputs (the keys, as the int32 it takes)
+        if e2e is not None:
+            hr, hs = hk[0].numpy(), hk[2].numpy()
+        else:
+            hr, hs = rk.cpu().numpy(), sk.cpu().numpy()
+        kind, cores, secs, c = cpu_join_runs(hr, hs, 2, min_seconds=10.0)
+        assert c == m, f"CPU join count {c} != {m}"
+        cpu = {"value": (nr + ns) / (sum(secs) / len(secs)), "unit": UNIT, "cores": cores, "kind": kind,
+               "sample": f"the full workload ({nr} x {ns} rows), {len(secs)} runs of run_sanity_check "
+                         f"(count only) on {cores} host threads"}
+        del hr, hs
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": wl["name"], "n_r": nr, "n_s": ns, "match_frac": wl["match"],
-                       "bloom_bits_per_key": wl["bpk"] if wl["bloom"] else 0,
-                       "bloom_hashes": st.bloom_num_hashes, "partition_size": st.partition_size,
-                       "second_partition_size": st.second_partition_size,
-                       "l2": f"no flush: each step streams {8 * (nr + ns) / 1e9:.2f} GB of inputs"
-                             + (", far above the 126 MB L2" if 8 * (nr + ns) > 4 * 126e6 else ""),
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "config": workload_config(wl, world),
+            "plan": {"partition_size": st.partition_size, "second_partition_size": st.second_partition_size,
+                     "bloom_hashes": st.bloom_num_hashes, "bloom_num_bits": st.bloom_num_bits,
+                     "bloom_probe_level": blvl},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": stage_traffic(dom, nr, ns, blvl),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per tuple on "

@@ -68,7 +68,8 @@ class Config(C.Structure):
         ("bloom_probe_level", C.c_int32),
         ("max_level1_bits", C.c_int32),
         ("s_chunks", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("wait_poll_limit", C.c_int32),
+        ("reserved", C.c_int32 * 2),
     ]
 
 

@@ -35,6 +35,7 @@ constexpr int kWarpBuf = 128;         // output pairs staged per warp before a g
 // (the filter segments of the partitions in flight must stay in L2; with the longer slices twice
 // as many partitions are in flight).
 constexpr int64_t kL2Slice = 64 * kTile;
+constexpr uint32_t kDefaultWaitPolls = 1u << 22;  // polls of a bounded wait before it gives up
 constexpr int64_t kL2SliceBloom = 32 * kTile;
 
 // Per-join device counters (int64 each).
@@ -288,6 +289,7 @@ enum GlobalWord : int {
     kGTasks = 1,           // total tasks (written by the task builder)
     kGErrors = 2,          // device-side consistency failures
     kGL2Slices = 3,        // level-2 slices of R (word 3) and of S (word 4)
+    kGWaitPolls = 5,       // polls after which a bounded wait gives up and counts an error
     kGWords = 8
 };
 

@@ -600,6 +600,9 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     a.kclasses = 0;
     for (int j = 0; j < nj; ++j) a.kclasses |= (plans[j].bloom && plans[j].k == a.pat_k) ? 2 : 1;
     a.num_sms = num_sms;
+    if (cfg.wait_poll_limit < -1) fail(BRIG_E_INVALID, "wait_poll_limit must be >= -1");
+    a.wait_polls = cfg.wait_poll_limit == 0 ? kDefaultWaitPolls
+                   : cfg.wait_poll_limit < 0 ? 0u : (uint32_t)cfg.wait_poll_limit;
     a.stage_events = nullptr;
     a.stages = kRunAll;
     a.seg_ns = reinterpret_cast<uint32_t*>(ws + sh.seg_ns);

@@ -37,6 +37,7 @@
 //     word the host reads instead of writing out of bounds.
 #include <cstdio>
 #include <algorithm>
+#include <mutex>
 #include <type_traits>
 #include "launch.h"
 
@@ -201,13 +202,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-constexpr uint32_t kMaxPolls = 1u << 22;  // each poll may suspend for a bounded hardware interval
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long* err) {
-    for (uint32_t it = 0; it < kMaxPolls; ++it)
+// Polls of the bounded waits. The first bound is a runtime value (the pipeline's state word
+// kGWaitPolls, kDefaultPolls unless the caller's configuration sets it): when it runs out the wait
+// counts an error, which the host reports as BRIG_E_INTERNAL, and then waits once more, at most
+// kDefaultPolls polls, for the copy in flight, so that no copy is outstanding when the CTA moves on
+// or exits. A first bound of 0 makes every wait count an error at once (the error path's test).
+constexpr uint32_t kDefaultPolls = kDefaultWaitPolls;  // each poll may suspend for a bounded hardware interval
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, unsigned long long* err,
+                                          uint32_t polls) {
+    for (uint32_t it = 0; it < polls; ++it)
         if (mbar_try_wait(bar, parity)) return;
     if (threadIdx.x == 0) atomicAdd(err, 1ull);
-    for (uint32_t it = 0; it < kMaxPolls; ++it)
+    for (uint32_t it = 0; it < kDefaultPolls; ++it)
         if (mbar_try_wait(bar, parity)) return;
+}
+__device__ __forceinline__ uint32_t wait_polls(const unsigned long long* gwords) {
+    return (uint32_t)gwords[kGWaitPolls];
 }
 
 // Where the tuples of a tile come from. PackedTiles: (key, value) pairs in an engine buffer; a tile
@@ -320,7 +330,7 @@ template <class In, class Bin>
 __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
                               uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, int64_t* delta,
                               uint32_t* cnt, uint16_t* sbin, uint32_t* tmp, unsigned char* inbuf, uint64_t* bars,
-                              uint32_t& ph, unsigned long long* errors) {
+                              uint32_t& ph, unsigned long long* errors, uint32_t polls) {
     constexpr int kItems = kSTile / kSThreads;
     const int64_t ntiles = (end - begin + kSTile - 1) / kSTile;
     if (ntiles <= 0) return;
@@ -330,7 +340,7 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
         const int64_t t0 = begin + t * kSTile;
         const int tn = (int)min_i64(kSTile, end - t0);
         const int b = (int)(t & 1);
-        mbar_wait(&bars[b], (ph >> b) & 1u, errors);
+        mbar_wait(&bars[b], (ph >> b) & 1u, errors, polls);
         ph ^= 1u << b;
         // Every thread is past the previous tile's write pass, which read buffer b ^ 1 as `stage`
         // (and cnt is zero again): the next tile may now be copied into b ^ 1.
@@ -416,7 +426,7 @@ template <class In, class Bin>
 __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
                                    uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, uint32_t* cnt,
                                    uint32_t* spos, uint32_t* tmp, unsigned char* inbuf, size_t buf_stride,
-                                   uint64_t* bars, uint32_t& ph, unsigned long long* errors) {
+                                   uint64_t* bars, uint32_t& ph, unsigned long long* errors, uint32_t polls) {
     constexpr int kItems = kSTile / kSThreads;
     constexpr int kWarps = kSThreads / 32;
     const int64_t ntiles = (end - begin + kSTile - 1) / kSTile;
@@ -430,7 +440,7 @@ __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, con
         const int64_t t0 = begin + t * kSTile;
         const int tn = (int)min_i64(kSTile, end - t0);
         const int b = (int)(t & 1);
-        mbar_wait(&bars[b], (ph >> b) & 1u, errors);
+        mbar_wait(&bars[b], (ph >> b) & 1u, errors, polls);
         ph ^= 1u << b;
         unsigned char* buf = inbuf + b * buf_stride;
         const auto lay = in.layout(t0, tn);
@@ -746,6 +756,7 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
     uint32_t ph = 0;
+    const uint32_t polls = wait_polls(gwords);
     const int64_t total = slice_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(slice_prefix, nj, g);
@@ -767,19 +778,19 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
             const PackedTiles in{R.cmp};
             if constexpr (kBulk)
                 scatter_tiles_bulk(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
-                                   bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors]);
+                                   bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors], polls);
             else
                 scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph,
-                              &gwords[kGErrors]);
+                              &gwords[kGErrors], polls);
         } else {
             const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 3) == 0;
             const KvTiles in{R.key, R.val, al};
             if constexpr (kBulk)
                 scatter_tiles_bulk(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
-                                   bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors]);
+                                   bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors], polls);
             else
                 scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph,
-                              &gwords[kGErrors]);
+                              &gwords[kGErrors], polls);
         }
     }
     if constexpr (kBulk) bulk_wait_all();  // the bulk stores have written the output before the kernel ends
@@ -987,6 +998,7 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
     __shared__ __align__(8) uint64_t bars[2];
     init_bars(bars);
     uint32_t ph = 0;
+    const uint32_t polls = wait_polls(gwords);
     const int64_t total = (int64_t)gwords[kGL2Slices + rel];
     for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
         const L2Slice x = l2_decode(seg_prefix, nj, seg_off, seg_ns, total_segs, t);
@@ -1005,10 +1017,10 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const PackedTiles in{bloom ? R.cmp : R.l1};
         if constexpr (kBulk)
             scatter_tiles_bulk(in, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2, R.n, cursor, cnt, spos, tmp, inbuf,
-                               bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors]);
+                               bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors], polls);
         else
             scatter_tiles(in, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2, R.n, cursor, delta, cnt, sbin, tmp, inbuf,
-                          bars, ph, &gwords[kGErrors]);
+                          bars, ph, &gwords[kGErrors], polls);
     }
     if constexpr (kBulk) bulk_wait_all();  // the bulk stores have written the output before the kernel ends
 }
@@ -1534,6 +1546,7 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     __shared__ ProbeTask s_info[2];  // the current task and the next one, resolved by thread 0
     __shared__ __align__(8) uint64_t bar;
     unsigned long long* errors = &gwords[kGErrors];
+    const uint32_t polls = wait_polls(gwords);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int words_per_warp = kWarpBuf * (emit_key ? 3 : 2);
     WarpOut o;
@@ -1617,7 +1630,7 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
             const int i = k * kThreads + threadIdx.x;
             if (i < nr) table[off[br[k] >> 16] + (br[k] & 0xffffu)] = __ldg(bsrc + i);
         }
-        mbar_wait(&bar, ph, errors);
+        mbar_wait(&bar, ph, errors, polls);
         ph ^= 1u;
         __syncthreads();
         // ---- probe: the first chunk from shared memory, the rest straight from global memory
@@ -1640,11 +1653,14 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     if (cur >= 0 && o.count > 0) warp_flush(J[cur], o.wr, o.ws, o.wk, o.count, lane);
 }
 
-// Copies each join's match count to the caller's device int64 (if requested).
-__global__ void k_publish_counts(const JoinDesc* __restrict__ J, int nj) {
+// Copies each join's match count to the caller's device int64 (if requested), or -1 when a
+// device-side consistency check of this run failed (the host reports BRIG_E_INTERNAL), so that a
+// caller that reads only the device count, without a host synchronisation, sees the failure too.
+__global__ void k_publish_counts(const JoinDesc* __restrict__ J, int nj, const unsigned long long* gwords) {
+    const bool failed = gwords[kGErrors] != 0;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nj; j += gridDim.x * blockDim.x) {
         const JoinDesc& d = J[j];
-        if (d.user_count) *d.user_count = d.counters[kCntMatches];
+        if (d.user_count) *d.user_count = failed ? -1 : d.counters[kCntMatches];
     }
 }
 
@@ -1704,7 +1720,13 @@ __global__ void __launch_bounds__(kThreads) k_scan_down(const uint32_t* __restri
     }
 }
 
-__global__ void k_fill_word(unsigned long long* p, unsigned long long v) { *p = v; }
+// Resets the run's state words: the task queue, the error count (unless the run continues an earlier
+// launch's count) and the bound of the waits.
+__global__ void k_init_words(unsigned long long* g, int keep_errors, uint32_t polls) {
+    g[kGQueue] = 0ull;
+    if (!keep_errors) g[kGErrors] = 0ull;
+    g[kGWaitPolls] = polls;
+}
 
 }  // namespace
 
@@ -1786,42 +1808,55 @@ static int grid_for(int64_t work, int num_sms, int per_sm) {
     return (int)std::max<int64_t>(g, 1);
 }
 
-cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
-    static thread_local bool attrs_done = false;
+static cudaError_t set_kernel_attrs() {
     cudaError_t err;
-    if (!attrs_done) {
-        const void* l1s[] = {(const void*)k_l1_scatter<false, 0, false>, (const void*)k_l1_scatter<false, 1, false>,
-                             (const void*)k_l1_scatter<true, 0, false>, (const void*)k_l1_scatter<true, 1, false>};
-        for (const void* f : l1s)
-            if ((err = set_smem_attr(f, scatter_smem(kMaxP1, false))) != cudaSuccess) return err;
-        const void* bulks[] = {(const void*)k_l1_scatter<false, 0, true>, (const void*)k_l1_scatter<false, 1, true>,
-                               (const void*)k_l1_scatter<true, 0, true>,  (const void*)k_l1_scatter<true, 1, true>,
-                               (const void*)k_l2_scatter<0, true>,        (const void*)k_l2_scatter<1, true>};
-        for (const void* f : bulks)
-            if ((err = set_smem_attr(f, scatter_smem(kBulkMaxBins, true))) != cudaSuccess) return err;
-        const void* l2s[] = {(const void*)k_l2_scatter<0, false>, (const void*)k_l2_scatter<1, false>};
-        for (const void* f : l2s)
-            if ((err = set_smem_attr(f, scatter_smem(kMaxP2, false))) != cudaSuccess) return err;
-        const void* bbs[] = {(const void*)k_bloom_build<0, 0>, (const void*)k_bloom_build<1, 0>,
-                             (const void*)k_bloom_build<0, kBloomFastK>, (const void*)k_bloom_build<1, kBloomFastK>};
-        for (const void* f : bbs)
-            if ((err = set_smem_attr(f, kBloomSmemWords * 4)) != cudaSuccess) return err;
-        if ((err = set_smem_attr((const void*)k_probe, probe_smem_bytes(kMaxTable, 1))) != cudaSuccess)
-            return err;
-        attrs_done = true;
+    const void* l1s[] = {(const void*)k_l1_scatter<false, 0, false>, (const void*)k_l1_scatter<false, 1, false>,
+                         (const void*)k_l1_scatter<true, 0, false>, (const void*)k_l1_scatter<true, 1, false>};
+    for (const void* f : l1s)
+        if ((err = set_smem_attr(f, scatter_smem(kMaxP1, false))) != cudaSuccess) return err;
+    const void* bulks[] = {(const void*)k_l1_scatter<false, 0, true>, (const void*)k_l1_scatter<false, 1, true>,
+                           (const void*)k_l1_scatter<true, 0, true>,  (const void*)k_l1_scatter<true, 1, true>,
+                           (const void*)k_l2_scatter<0, true>,        (const void*)k_l2_scatter<1, true>};
+    for (const void* f : bulks)
+        if ((err = set_smem_attr(f, scatter_smem(kBulkMaxBins, true))) != cudaSuccess) return err;
+    const void* l2s[] = {(const void*)k_l2_scatter<0, false>, (const void*)k_l2_scatter<1, false>};
+    for (const void* f : l2s)
+        if ((err = set_smem_attr(f, scatter_smem(kMaxP2, false))) != cudaSuccess) return err;
+    const void* bbs[] = {(const void*)k_bloom_build<0, 0>, (const void*)k_bloom_build<1, 0>,
+                         (const void*)k_bloom_build<0, kBloomFastK>, (const void*)k_bloom_build<1, kBloomFastK>};
+    for (const void* f : bbs)
+        if ((err = set_smem_attr(f, kBloomSmemWords * 4)) != cudaSuccess) return err;
+    if ((err = set_smem_attr((const void*)k_probe, probe_smem_bytes(kMaxTable, 1))) != cudaSuccess)
+        return err;
+    return cudaSuccess;
+}
+
+// Kernel attributes (the dynamic shared-memory limits above 48 KB) hold per device: they are set once
+// for every device the process launches on.
+static std::mutex g_attr_mu;
+static uint64_t g_attr_done = 0;  // bit d: attributes set on device d (ordinals 0..63)
+
+cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
+    cudaError_t err;
+    int dev = 0;
+    if ((err = cudaGetDevice(&dev)) != cudaSuccess) return err;
+    {
+        std::lock_guard<std::mutex> lk(g_attr_mu);
+        const bool known = dev >= 0 && dev < 64;
+        if (!known || !((g_attr_done >> dev) & 1u)) {
+            if ((err = set_kernel_attrs()) != cudaSuccess) return err;
+            if (known) g_attr_done |= 1ull << dev;
+        }
     }
     const int sms = a.num_sms;
+
     int launches = 0;
     auto mark = [&](int i) {
         if (a.stage_events) cudaEventRecord(a.stage_events[i], st);
     };
     mark(0);
-    k_fill_word<<<1, 1, 0, st>>>(a.gwords + kGQueue, 0ull);
+    k_init_words<<<1, 1, 0, st>>>(a.gwords, a.keep_errors, a.wait_polls);
     ++launches;
-    if (!a.keep_errors) {
-        k_fill_word<<<1, 1, 0, st>>>(a.gwords + kGErrors, 0ull);
-        ++launches;
-    }
 
     // ---- R, then S: level 1 and level 2 (the Bloom build sits between them) -----------------
     for (int rel = 0; rel < 2; ++rel) {
@@ -1957,7 +1992,7 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
         occ = std::max(occ, 1);
         k_probe<<<sms * occ, kThreads, smem, st>>>(a.J, a.tasks, a.gwords, a.table_cap, a.emit_key);
         mark(13);
-        k_publish_counts<<<1, 256, 0, st>>>(a.J, a.nj);
+        k_publish_counts<<<1, 256, 0, st>>>(a.J, a.nj, a.gwords);
         launches += 2;
     }
     note_launches(launches);

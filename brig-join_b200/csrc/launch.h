@@ -48,6 +48,7 @@ struct PipelineArgs {
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
     cudaEvent_t s_ready;              // when set, S's passes wait for it (its inputs are still arriving)
     int keep_errors;                  // 1: the error word keeps the counts of earlier launches of the run
+    uint32_t wait_polls;              // first bound of the kernels' bounded waits (polls)
     int stages;                       // kRunPartR | kRunBloom | kRunPartS | kRunProbe
     // level 2 (planned on the device)
     uint32_t* seg_ns;                 // [total_segs + 1] slices per level-1 partition

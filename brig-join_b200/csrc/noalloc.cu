@@ -13,8 +13,11 @@
 //     BRIG_NOALLOC_SCRATCH_BYTES; larger requests are rejected with BRIG_E_UNSUPPORTED;
 //   * every GPU that loads the library holds the array until the process exits;
 //   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) and
-//     the first call on a host thread sets kernel attributes; make that first call before any
-//     stream capture;
+//     sets the kernels' attributes on that device; the entry point refuses to run under stream
+//     capture (BRIG_E_UNSUPPORTED): it uploads its descriptors from a stack buffer, which a
+//     captured graph could not replay;
+//   * a device-side consistency failure (a bounds check, a wait that gave up) writes -1 to
+//     out->d_count instead of the count, since this entry point has no handle to report it through;
 //   * all calls on a device share the one array and it keeps the last call's contents: the
 //     pipeline clears what must start at zero (counters, queue words) and fully writes everything
 //     else before reading it, but two calls whose work overlaps on the GPU race on the array, so
@@ -71,6 +74,11 @@ extern "C" int brig_join_run_noalloc(const brig_join_config* cfg, const uint32_t
             fail(BRIG_E_INVALID, "bad output");
         if (!out->d_count) fail(BRIG_E_INVALID, "d_count is required: it is the only way the count comes back");
         if (cfg->device >= 0) cuda_check(cudaSetDevice(cfg->device), "cudaSetDevice");
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        cuda_check(cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap), "cudaStreamIsCapturing");
+        if (cap != cudaStreamCaptureStatusNone)
+            fail(BRIG_E_UNSUPPORTED, "brig_join_run_noalloc cannot be captured into a CUDA graph (its descriptor "
+                                     "upload reads a stack buffer); call it directly");
         int dev = 0, sms = 0;
         cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
         cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");

@@ -86,7 +86,14 @@ typedef struct brig_join_config {
                                        chunks against R partitioned once (the reference's s_chunks
                                        loop, src/hash_kernel.cu:910-1131), so S may exceed device
                                        memory; 0 or 1 = S in one piece */
-    int32_t reserved[3];
+    int32_t wait_poll_limit;        /* polls after which a kernel's bounded wait for a bulk copy gives
+                                       up, counts a device-side error (the run then reports
+                                       BRIG_E_INTERNAL and d_count reads -1) and waits once more, at
+                                       most the default bound, for the copy in flight; 0 = 2^22 (the
+                                       default), -1 = none, so every such wait reports the error at
+                                       once (a test of the error path; the results stay exact). The
+                                       reference's waits are unbounded (src/join_executor.cu:49) */
+    int32_t reserved[2];
 } brig_join_config;
 
 /* Output of one join. Pairs are written in an unspecified order; the multiset is exact. When the
@@ -98,7 +105,8 @@ typedef struct brig_join_output {
     uint32_t* s_val;     /* device [capacity]: S value of each pair (GPU_answer_s_val) */
     uint32_t* key;       /* device [capacity] or NULL: key of each pair (GPU_answer) */
     int64_t   capacity;  /* number of pair slots */
-    int64_t*  d_count;   /* device int64 or NULL: receives the exact match count, stream-ordered */
+    int64_t*  d_count;   /* device int64 or NULL: receives the exact match count, stream-ordered, or
+                            -1 when a device-side consistency check of the run failed */
 } brig_join_output;
 
 /* What the last run did, read after it completes. */
@@ -273,11 +281,14 @@ int brig_gen_host(uint64_t seed, int64_t n_r, int64_t n_s, double match_frac, do
  * loading the library holds until the process exits; no handle, no cudaMalloc/cudaFree/
  * cudaMallocHost. Limit: at most BRIG_NOALLOC_MAX_TUPLES tuples per relation, and the join's layout
  * must fit the array (the default planner and the modulo preset with partition_size 512 do);
- * larger requests return BRIG_E_UNSUPPORTED. The count is written to out->d_count (required).
- * The first call on a device looks up the array's address and the first call on a host thread sets
- * kernel attributes: make it before any stream capture. All calls on a device share the array and
- * it keeps the last call's contents (the pipeline clears what must start at zero); calls whose work
- * overlaps on the GPU race on it, so order them on one stream or with events. */
+ * larger requests return BRIG_E_UNSUPPORTED. The count is written to out->d_count (required), or -1
+ * when a device-side consistency check failed (there is no handle to report BRIG_E_INTERNAL through).
+ * The first call on a device looks up the array's address and sets the kernels' attributes on that
+ * device. It must not be called under stream capture (it returns BRIG_E_UNSUPPORTED there): its
+ * descriptor upload reads a stack buffer that a replayed graph could not reach. All calls on a
+ * device share the array and it keeps the last call's contents (the pipeline clears what must start
+ * at zero); calls whose work overlaps on the GPU race on it, so order them on one stream or with
+ * events. */
 #define BRIG_NOALLOC_MAX_TUPLES 262144
 #define BRIG_NOALLOC_SCRATCH_BYTES (16u << 20)
 int brig_join_run_noalloc(const brig_join_config* cfg,

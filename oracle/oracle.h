@@ -28,6 +28,12 @@ int oracle_sort_pairs(uint32_t* a, uint32_t* b, int64_t n);
 /* FNV-1a fingerprint of a sorted pair list. */
 uint64_t oracle_pairs_digest(const uint32_t* a, const uint32_t* b, int64_t n);
 
+/* The benchmark's synthetic inputs (gen.c): distinct R keys in [1, 2^31), a fraction match_frac of
+ * S rows drawn uniformly from R's keys, the rest distinct in [2^31, 2^32 - 1), values = row index.
+ * Any output pointer may be NULL. Returns 0, or -1 for bad arguments. */
+int oracle_gen(uint64_t seed, int64_t nr, int64_t ns, double match_frac, uint32_t* rk, uint32_t* rv,
+               uint32_t* sk, uint32_t* sv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,6 +42,8 @@ def lib():
         L.oracle_sort_pairs.restype = C.c_int
         L.oracle_pairs_digest.argtypes = [vp, vp, C.c_int64]
         L.oracle_pairs_digest.restype = C.c_uint64
+        L.oracle_gen.argtypes = [C.c_uint64, C.c_int64, C.c_int64, C.c_double, vp, vp, vp, vp]
+        L.oracle_gen.restype = C.c_int
         _o = L
     return _o
 
@@ -94,6 +96,19 @@ def sort_pairs(a, b):
 def digest(a, b) -> int:
     a, b = _u32(a), _u32(b)
     return int(lib().oracle_pairs_digest(a.ctypes.data, b.ctypes.data, len(a)))
+
+
+def gen(seed, n_r, n_s, match_frac=0.1, want_vals=True):
+    """The benchmark's synthetic inputs (uniform matches) computed on the host by gen.c:
+    (r_key, r_val, s_key, s_val) as uint32 arrays (values None when want_vals is False)."""
+    rk = np.empty(n_r, np.uint32)
+    sk = np.empty(n_s, np.uint32)
+    rv = np.empty(n_r, np.uint32) if want_vals else None
+    sv = np.empty(n_s, np.uint32) if want_vals else None
+    p = lambda a: a.ctypes.data if a is not None else None
+    if lib().oracle_gen(seed, n_r, n_s, match_frac, p(rk), p(rv), p(sk), p(sv)) != 0:
+        raise ValueError("oracle_gen: bad arguments")
+    return rk, rv, sk, sv
 
 
 # ---- the reference's own CPU join ---------------------------------------------------------------

@@ -24,8 +24,10 @@ def test_config_defaults(bj):
     assert cfg.partition_mode == bj.PART_HASH
     assert cfg.bloom_bits_per_key == 10.0 and cfg.use_bloom == 0 and cfg.device == -1
     assert cfg.s_chunks == 0  # S in one piece
-    assert C.sizeof(bj.Config) == 88  # layout of brig_join_config (s_chunks took a reserved slot)
-    assert bj.Config.s_chunks.offset == 72 and bj.Config.reserved.offset == 76
+    assert cfg.wait_poll_limit == 0  # default bound of the kernels' waits
+    assert C.sizeof(bj.Config) == 88  # layout of brig_join_config (s_chunks and wait_poll_limit took
+    assert bj.Config.s_chunks.offset == 72  # reserved slots)
+    assert bj.Config.wait_poll_limit.offset == 76 and bj.Config.reserved.offset == 80
 
 
 @pytest.mark.parametrize("n_r,n_s,kw,expect", [

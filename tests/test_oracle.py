@@ -106,3 +106,15 @@ def test_generator_known_answer(bj, oracle):
     for frac in (0.0, 0.001, 0.1, 0.5, 1.0):
         rk, rv, sk, sv = bj.gen_host(77, 50_000, 80_000, frac)
         assert oracle.count(rk, sk) == int(np.floor(frac * 80_000))
+
+
+@pytest.mark.parametrize("seed,nr,ns,frac", [(42, 1000, 1000, 0.1), (7, 123457, 98765, 0.3), (3, 1, 1, 1.0),
+                                             (9, 0, 10, 0.5), (5, 10, 0, 0.1), (11, 1 << 20, 1 << 21, 0.001)])
+def test_oracle_generator_matches_engine_generator(bj, oracle, seed, nr, ns, frac):
+    """The benchmark's CPU baseline and reference arm generate their inputs with the oracle's C
+    restatement of the generator (so they load no engine library); it must equal the engine's own
+    host generator row for row."""
+    a = bj.gen_host(seed, nr, ns, frac)
+    b = oracle.gen(seed, nr, ns, frac)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)

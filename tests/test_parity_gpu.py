@@ -247,3 +247,46 @@ def test_device_generator_matches_host(bj, torch_cuda):
     torch_cuda.cuda.synchronize()
     for a, b in zip(h, d):
         assert np.array_equal(a, b.cpu().numpy().view(np.uint32))
+
+
+@pytest.mark.parametrize("preset", ["reference_fanout_512", "planner"])
+def test_config0_16M_x_16M(bj, oracle, torch_cuda, preset):
+    """The plain single join at its stated size: |R| = |S| = 2^24, 10% of S matching, Bloom filter on
+    (10 bits/key, k = 7). `reference_fanout_512` is the reference's README preset --partition_size
+    512, i.e. first-level fan-out 512 by key % 512 (second level auto: 67); `planner` is the engine's
+    own choice. Exact count and identical sorted pair multiset against the oracle."""
+    n = 1 << 24
+    rk, rv, sk, sv = bj.gen_host(42, n, n, 0.1)
+    cfg = dict(use_bloom=1, bloom_bits_per_key=10.0, bloom_num_hashes=7)
+    if preset == "reference_fanout_512":
+        cfg.update(partition_mode=bj.PART_MODULO, partition_size=512)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, **cfg)
+    assert st.count == 1_677_721 and st.bloom_num_hashes == 7
+    assert st.count <= st.s_survivors < n // 4
+    if preset == "reference_fanout_512":
+        assert (st.partition_size, st.second_partition_size) == (512, 67)
+
+
+def test_bounded_waits_report_internal_error_and_stay_exact(bj, oracle, torch_cuda):
+    """wait_poll_limit = -1 gives every bounded wait of the kernels (the bulk-copy mbarriers of the
+    scatters and the probe) no polls: each one counts a device-side error at once and then waits
+    for its copy with the default bound. The run must end (no hang), report BRIG_E_INTERNAL, publish
+    -1 as the device count, keep its pairs exact, and leave the context usable for the next run."""
+    rk, rv, sk, sv = bj.gen_host(77, 300_000, 400_000, 0.2)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    cap = len(exp_r) + 16
+    d = [torch_cuda.from_numpy(a.view(np.int32)).cuda() for a in (rk, rv, sk, sv)]
+    out_r = torch_cuda.empty(cap, dtype=torch_cuda.int32, device="cuda")
+    out_s = torch_cuda.empty(cap, dtype=torch_cuda.int32, device="cuda")
+    d_count = torch_cuda.zeros(1, dtype=torch_cuda.int64, device="cuda")
+    with bj.Join(use_bloom=1, partition_size=16, second_partition_size=8, wait_poll_limit=-1) as j:
+        j.run(d[0], d[1], len(rk), d[2], d[3], len(sk), out_r, out_s, cap, d_count=d_count)
+        with pytest.raises(bj.BrigError) as e:
+            j.stats()
+        assert e.value.status == bj.BRIG_E_INTERNAL
+        assert int(d_count.item()) == -1
+    n = len(exp_r)
+    assert_same_pairs(oracle, out_r[:n].cpu().numpy().view(np.uint32), out_s[:n].cpu().numpy().view(np.uint32),
+                      exp_r, exp_s)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=1, partition_size=16, second_partition_size=8)
+    assert st.count == n

@@ -14,7 +14,7 @@ from gpu_helpers import assert_same_pairs, dev, run_device
 pytestmark = pytest.mark.gpu
 
 
-def _run_noalloc(bj, torch, rk, rv, sk, sv, cap, **cfg):
+def _run_noalloc(bj, torch, rk, rv, sk, sv, cap, expect=None, **cfg):
     c = bj.make_config(**cfg)
     d = [dev(torch, a) for a in (rk, rv, sk, sv)]
     out_r = torch.empty(cap, dtype=torch.int32, device="cuda")
@@ -26,7 +26,7 @@ def _run_noalloc(bj, torch, rk, rv, sk, sv, cap, **cfg):
     assert st == bj.BRIG_OK, bj.last_error()
     torch.cuda.synchronize()
     n = int(d_count.item())
-    m = min(n, cap)
+    m = min(max(n, 0), cap)
     return n, out_r[:m].cpu().numpy().view(np.uint32), out_s[:m].cpu().numpy().view(np.uint32)
 
 
@@ -41,6 +41,19 @@ def test_noalloc_matches_allocating_entry_point_on_two_calls(bj, oracle, torch_c
         n, r, s = _run_noalloc(bj, torch_cuda, rk, rv, sk, sv, ns, **cfg)
         assert n == st.count == int(frac * ns)
         assert_same_pairs(oracle, r, s, r_ref, s_ref)
+        assert_same_pairs(oracle, r, s, *oracle.pairs(rk, rv, sk, sv))
+
+
+def test_noalloc_reports_device_errors_through_the_count(bj, oracle, torch_cuda):
+    """With no handle to report BRIG_E_INTERNAL through, a device-side failure reaches the caller as
+    -1 in d_count: every bounded wait is made to give up at once (wait_poll_limit = -1), then a
+    default call on the same scratch gives the exact count again."""
+    rk, rv, sk, sv = bj.gen_host(950, 100_000, 150_000, 0.2)
+    n, _, _ = _run_noalloc(bj, torch_cuda, rk, rv, sk, sv, 150_000, use_bloom=1, wait_poll_limit=-1)
+    assert n == -1
+    n, r, s = _run_noalloc(bj, torch_cuda, rk, rv, sk, sv, 150_000, use_bloom=1)
+    assert n == 30_000
+    assert_same_pairs(oracle, r, s, *oracle.pairs(rk, rv, sk, sv))
 
 
 def test_noalloc_rejects_sizes_beyond_its_limit(bj, torch_cuda):
