@@ -29,7 +29,8 @@ constexpr int kMaxBloomK = 16;
 constexpr int kThreads = 512;         // threads per CTA of every partition and probe kernel
 constexpr int kTile = 4096;           // unit of the level-2 slice length
 constexpr int kSThreads = 1024;       // threads per CTA of the scatter kernels (one CTA per SM)
-constexpr int kSTile = 8192;          // tuples per scatter tile staged in shared memory
+constexpr int kSTile = 12288;         // tuples per tile of the bulk-store scatter (slice lengths are
+                                      // multiples of it)
 constexpr int kWarpBuf = 128;         // output pairs staged per warp before a global flush
 // Tuples per level-2 slice: 262144, or 131072 for S when its second pass probes the Bloom filter
 // (the filter segments of the partitions in flight must stay in L2; with the longer slices twice
@@ -133,84 +134,39 @@ BRIG_HD uint32_t bucket_of(uint32_t key, uint32_t nb_mask) { return mix32(key) &
 // The reference uses 256-bit blocks with k bit positions anywhere in the block and one segment
 // per first-level partition (src/bloom.cu:698-722, src/hash_kernel.cu:555-582).
 //
-// Hash bits (g = bloom_hash(key)): bits 40..63 pick the block, bits 35..36 the word pair, bits
-// 5i..5i+4 the position of bit i for i < 7 (k != 7); positions of bits 7.. come from mix64(g).
-struct BloomKey {
-    uint32_t block;   // block index inside the segment
-    uint32_t wa, wb;  // the pair's even and odd word (wb = wa + 1)
-    uint32_t ma, mb;  // bits to set/test in them
-};
+// Hash bits (g = bloom_hash(key)): bits 40..63 pick the block, bits 35..36 the word pair, bits 0..9
+// the pattern pair (below).
 
 // The Bloom hash is mix32(key) (which the partition functions compute anyway) times an odd 64-bit
 // constant: multiplication by an odd constant is a bijection modulo every power of two, so each
 // field of the product is uniform when mix32(key) is, and the top bits depend on every input bit.
 BRIG_HD uint64_t bloom_hash(uint32_t key) { return (uint64_t)mix32(key) * 0x9e3779b97f4a7c15ull; }
 
-// Bits 40..63 of the hash pick the block (24-bit multiply-shift range reduction).
-BRIG_HD uint32_t bloom_block_of(uint64_t g, uint32_t seg_blocks) {
-    return (uint32_t)(((g >> 40) * (uint64_t)seg_blocks) >> 24);
+// Masks. For k = 7 (10 bits per key, the default) the bit positions are seven 5-bit fields of g
+// (bits 0..34): fields 0..3 in the even word, 4..6 in the odd word, one funnel shift each.
+// Every other k takes pattern-blocked masks (Lang et al., as above): hash bits 0..9 pick one of
+// 1024 pattern pairs, ceil(k/2) bits for the even word and floor(k/2) bits for the odd word;
+// pattern i of word w is the OR of 1 << (5-bit fields of a SplitMix64 hash of (w, i)). The kernels
+// keep the pairs (8 KB), filled for the launch's k, in shared memory, so those masks cost one 8-byte
+// shared-memory load. Measured at 640M keys: the compile-time shifts take the level-2 probe from
+// 3.45 to 3.19 ms (its random filter loads keep the L1 pipe busy, and the look-ups compete with
+// them) and the build from 1.51 to 1.61 ms; two look-ups per key, or seven shifts recomputed from
+// the key, cost more in both.
+constexpr int kBloomFastK = 7;  // template tag of the compile-time k = 7 instantiations
+BRIG_HD uint32_t bloom_bit(uint32_t p) {  // 1 << (p mod 32): one funnel shift on the device
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_l(0u, 1u, p);
+#else
+    return 1u << (p & 31u);
+#endif
 }
-
-// Bit masks of a key with hash g. K > 0: k == K known at compile time (a handful of shifts and ORs);
-// K == 0: any k in [1, 16].
-template <int K>
-BRIG_HD void bloom_masks(uint64_t g, int k, uint32_t& ma, uint32_t& mb) {
+BRIG_HD uint2 bloom_masks7(uint64_t g) {
     const uint32_t lo = (uint32_t)g, hi = (uint32_t)(g >> 32);
-    auto bit = [&](int i) -> uint32_t {  // i < 7: bits 5i..5i+4 of g
-        const uint32_t p = i < 6 ? (lo >> (5 * i)) : ((lo >> 30) | (hi << 2));
-        return 1u << (p & 31u);
-    };
-    if constexpr (K > 0 && K <= 7) {
-        constexpr int ka = (K + 1) / 2;
-        uint32_t a = 0, b = 0;
-#pragma unroll
-        for (int i = 0; i < K; ++i) {
-            if (i < ka) a |= bit(i); else b |= bit(i);
-        }
-        ma = a;
-        mb = b;
-    } else {
-        const int ka = (k + 1) >> 1;
-        uint32_t a = 0, b = 0;
-#pragma unroll
-        for (int i = 0; i < 7; ++i) {
-            const uint32_t v = bit(i);
-            a |= i < ka ? v : 0u;
-            b |= (i >= ka && i < k) ? v : 0u;
-        }
-        if (k > 7) {
-            const uint64_t g2 = mix64(g);
-            for (int i = 7; i < k; ++i) {
-                const uint32_t v = 1u << ((uint32_t)(g2 >> (5 * (i - 7))) & 31u);
-                if (i < ka) a |= v; else b |= v;
-            }
-        }
-        ma = a;
-        mb = b;
-    }
+    uint2 r;
+    r.x = bloom_bit(lo) | bloom_bit(lo >> 5) | bloom_bit(lo >> 10) | bloom_bit(lo >> 15);
+    r.y = bloom_bit(lo >> 20) | bloom_bit(lo >> 25) | bloom_bit((lo >> 30) | (hi << 2));
+    return r;
 }
-
-// Where a key with hash g lives: its block and the two words in it (masks are separate). The
-// kernels use the word pair layout: hash bits 35..36 pick one of the block's four 8-byte word
-// pairs, so a probe reads both words with one 8-byte load.
-BRIG_HD void bloom_place(uint64_t g, uint32_t seg_blocks, BloomKey& bk) {
-    bk.block = bloom_block_of(g, seg_blocks);
-    bk.wa = 2u * ((uint32_t)(g >> 35) & 3u);
-    bk.wb = bk.wa + 1u;
-}
-
-// Compile-time mask class of a join's filter: the Bloom kernels are instantiated for the pattern
-// tables below (every join whose k is the k the launch's tables were filled for: all of them, as
-// the joins of one launch share their configuration) and for the bit arithmetic of bloom_masks (any
-// other k), and each instantiation skips the other's joins.
-constexpr int kBloomFastK = 7;  // template tag of the pattern-table instantiations
-
-// The masks are pattern-blocked (Lang et al., as above): hash bits 0..9 pick one of 1024 patterns
-// of ceil(k/2) bits for the even word and bits 10..19 one of 1024 patterns of floor(k/2) bits for
-// the odd word. Pattern i of word w is the OR of 1 << (5-bit fields of a SplitMix64 hash of (w, i)),
-// so two table look-ups replace the shifts of k bit positions. The kernels that build or probe a
-// filter keep both tables (8 KB), filled for the launch's k, in shared memory. For k = 7 (4 + 3
-// bits) the tables are the ones the k = 7 filters have always used.
 constexpr int kPatterns = 1024;
 BRIG_HD uint32_t bloom_pattern(int word, uint32_t i, int k) {
     const uint64_t h = mix64(((uint64_t)(word + 1) << 32) ^ (uint64_t)i ^ 0x243f6a8885a308d3ull);
@@ -219,9 +175,30 @@ BRIG_HD uint32_t bloom_pattern(int word, uint32_t i, int k) {
     for (int b = 0; b < nb; ++b) m |= 1u << ((uint32_t)(h >> (5 * b)) & 31u);
     return m;
 }
-BRIG_HD void bloom_pattern_masks(const uint32_t* pat, uint64_t g, uint32_t& ma, uint32_t& mb) {
-    ma = pat[(uint32_t)g & (kPatterns - 1)];
-    mb = pat[kPatterns + ((uint32_t)(g >> 10) & (kPatterns - 1))];
+
+// Where a key's filter bits live: the word index of its word pair in the whole filter (32-bit: the
+// planner keeps a filter below 2^32 words) and its pattern index. m = mix32(key), fine = the key's
+// finest partition (its segment), or its index relative to a group of segments. Of g =
+// bloom_hash(key): the block is ((g >> 40) * seg_blocks) >> 24 (a multiply-high), the word pair
+// (g >> 35) & 3, the pattern pair g & 1023.
+struct BloomSlot {
+    uint32_t widx;  // index of the pair's even word
+    uint32_t pidx;  // pattern pair (k != 7)
+    uint64_t g;     // the Bloom hash (its low 35 bits place the k = 7 bits)
+};
+BRIG_HD BloomSlot bloom_slot(uint32_t m, uint32_t fine, uint32_t seg_blocks) {
+    const uint64_t g = (uint64_t)m * 0x9e3779b97f4a7c15ull;  // bloom_hash
+    const uint32_t lo = (uint32_t)g, hi = (uint32_t)(g >> 32);
+#if defined(__CUDA_ARCH__)
+    const uint32_t blk = __umulhi(hi & 0xffffff00u, seg_blocks);
+#else
+    const uint32_t blk = (uint32_t)(((uint64_t)(hi & 0xffffff00u) * seg_blocks) >> 32);
+#endif
+    BloomSlot s;
+    s.widx = ((fine * seg_blocks + blk) << 3) + ((hi >> 2) & 6u);
+    s.pidx = lo & (kPatterns - 1);
+    s.g = g;
+    return s;
 }
 
 // ---- per-join descriptor (device resident) ------------------------------------------------------
@@ -258,7 +235,6 @@ struct JoinDesc {
     int32_t bloom_level;   // S pass that probes the filter: 1 first (fused with the histogram of
                            // S's level-1 pass), 2 second (fused with S's level-2 pass)
     int32_t bloom_group;   // consecutive finest partitions per Bloom build CTA
-    int32_t bloom_pat;     // 1: the masks come from the launch's pattern tables (bloom_k is their k)
     int64_t dom_base;      // offset of this join's task domains in the global task-count array
     int64_t fine_base;     // unused (kept zero)
     int32_t table_cap;     // max build-side tuples per probe task

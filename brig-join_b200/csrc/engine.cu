@@ -102,6 +102,9 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
         k = std::min(std::max(k, 1), kMaxBloomK);
         const int64_t blocks = (bits + 255) / 256;
         p.seg_blocks = (uint32_t)std::max<int64_t>(1, (blocks + p.nfine - 1) / p.nfine);
+        // the kernels index filter words with 32 bits
+        if (p.nfine * (int64_t)p.seg_blocks * 8 >= (1ll << 32))
+            fail(BRIG_E_UNSUPPORTED, "Bloom filter above 2^37 bits (16 GB)");
         p.bloom = true;
         p.k = k;
         p.bloom_bits = p.nfine * (int64_t)p.seg_blocks * 256;
@@ -488,11 +491,12 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     if (T < kMinTable || T > kMaxTable || !is_pow2(T))
         fail(BRIG_E_INVALID, "table_capacity must be a power of two in [256, 4096]");
     if (C < 1) fail(BRIG_E_INVALID, "s_chunk must be >= 1");
-    // The Bloom kernels fill their pattern tables for the k of the first filtered join: the joins of
-    // one run share their configuration, so that is every filtered join's k.
-    int pat_k = 0;
-    for (int j = 0; j < nj && !pat_k; ++j)
-        if (plans[j].bloom) pat_k = plans[j].k;
+    // The Bloom kernels fill their pattern table for the k of the first filtered join; the joins of
+    // one run share their configuration, so that is every filtered join's k (checked below).
+    int run_k = 0;
+    for (int j = 0; j < nj && !run_k; ++j)
+        if (plans[j].bloom) run_k = plans[j].k;
+    const int pat_k = run_k == kBloomFastK ? 0 : run_k;  // k = 7 masks need no table
     JoinDesc* hJ = reinterpret_cast<JoinDesc*>(meta_host);
     int64_t* hpre = reinterpret_cast<int64_t*>(meta_host + (size_t)nj * sizeof(JoinDesc));
     int64_t* sp0 = hpre;
@@ -543,7 +547,8 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
         d.fine_base = 0;
         d.dom_base = finep[j];
         d.bloom_group = p.bloom_group;
-        d.bloom_pat = (p.bloom && p.k == pat_k) ? 1 : 0;
+        if (p.bloom && p.k != run_k)
+            fail(BRIG_E_INVALID, "the filtered joins of one run must share their number of Bloom hashes");
         d.table_cap = T;
         d.s_chunk = C;
         hJ[j] = d;
@@ -598,7 +603,10 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     for (int j = 0; j < nj; ++j) a.modes |= plans[j].pf.mode == 0 ? 1 : 2;
     a.pat_k = pat_k;
     a.kclasses = 0;
-    for (int j = 0; j < nj; ++j) a.kclasses |= (plans[j].bloom && plans[j].k == a.pat_k) ? 2 : 1;
+    for (int j = 0; j < nj; ++j) a.kclasses |= (plans[j].bloom && plans[j].k == kBloomFastK) ? 2 : 1;
+    a.all_bloom_l2 = 1;
+    for (int j = 0; j < nj; ++j)
+        if (plans[j].pf.P2 > 1 && !(plans[j].bloom && plans[j].bloom_level == 2)) a.all_bloom_l2 = 0;
     a.num_sms = num_sms;
     if (cfg.wait_poll_limit < -1) fail(BRIG_E_INVALID, "wait_poll_limit must be >= -1");
     a.wait_polls = cfg.wait_poll_limit == 0 ? kDefaultWaitPolls

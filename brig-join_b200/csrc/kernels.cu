@@ -222,14 +222,16 @@ __device__ __forceinline__ uint32_t wait_polls(const unsigned long long* gwords)
 
 // Where the tuples of a tile come from. PackedTiles: (key, value) pairs in an engine buffer; a tile
 // is copied from the 16-byte boundary at or below its first tuple (engine buffers are padded, so
-// reading up to 8 bytes past either end stays inside the workspace). KvTiles: the caller's separate
-// key and value arrays; the 16-byte-aligned span of each array inside the tile is bulk-copied (the
-// two arrays may be misaligned differently) and the up to 3 + 3 tuples at its edges are read with
-// ordinary loads, so nothing outside the caller's arrays is read. mis(t0, tn) is the per-tile
-// layout word, issue() is called by one thread and arms `bar` (with no bytes when nothing is
-// copied), item() reads tuple i of the tile.
-constexpr size_t kTileBuf = (size_t)(kSTile + 2) * 8;  // one scatter input buffer
-
+// reading up to 8 bytes past either end stays inside the workspace). KvTiles<TILE>: the caller's
+// separate key and value arrays, keys at the start of a tile buffer and values TILE * 4 bytes in;
+// the 16-byte-aligned span of each array inside the tile is bulk-copied (the two arrays may be
+// misaligned differently) and the up to 3 + 3 tuples at its edges are read with ordinary loads, so
+// nothing outside the caller's arrays is read. mis(t0, tn) is the per-tile layout word, issue() is
+// called by one thread and arms `bar` (with no bytes when nothing is copied), item() reads tuple i
+// of the tile. fast(layout) says whether load_full() may read a whole tile of NITEMS tuples per
+// thread straight from shared memory with 16-byte loads and no bounds tests (the tuples of thread
+// x are its slots x, x + NT, ... of the load width; the scatter does not care which tuples a
+// thread holds).
 struct PackedTiles {
     const uint2* p;
     __device__ __forceinline__ uint32_t mis(int64_t t0, int = 0) const {
@@ -251,12 +253,21 @@ struct PackedTiles {
     __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t, int i, int, Layout m) const {
         return reinterpret_cast<const uint2*>(buf)[i + m];
     }
+    __device__ __forceinline__ bool fast(Layout) const { return true; }
+    template <int NITEMS, int NT>
+    __device__ __forceinline__ void load_full(const unsigned char* buf, Layout m, uint2 (&it)[NITEMS]) const {
+        const uint2* s = reinterpret_cast<const uint2*>(buf) + m;
+#pragma unroll
+        for (int j = 0; j < NITEMS; ++j) it[j] = s[j * NT + threadIdx.x];
+    }
 };
 
+template <int TILE>
 struct KvTiles {
     const uint32_t* k;
     const uint32_t* v;
     bool bulk;  // both arrays are 4-byte aligned (uint32 arrays always are, unless misused)
+    static constexpr size_t kValOff = (size_t)TILE * 4;  // byte offset of the values in a tile buffer
     // Per tile: the 16-byte-aligned span of each array inside [t0, t0 + tn), packed as
     // hk | hv << 2 | nk << 4 | nv << 18 (h: first aligned offset from t0, n: aligned count).
     __device__ __forceinline__ static uint32_t span(const uint32_t* p, int64_t t0, int tn, uint32_t& n) {
@@ -280,7 +291,7 @@ struct KvTiles {
         }
         mbar_arrive_tx(bar, 4u * (nk + nv));
         if (nk) bulk_g2s(buf, k + t0 + hk, nk * 4u, bar);
-        if (nv) bulk_g2s(buf + (size_t)kSTile * 4, v + t0 + hv, nv * 4u, bar);
+        if (nv) bulk_g2s(buf + kValOff, v + t0 + hv, nv * 4u, bar);
     }
     // The tile layout word decoded once per tile.
     struct Layout {
@@ -296,12 +307,28 @@ struct KvTiles {
     __device__ __forceinline__ uint2 item(const unsigned char* buf, int64_t t0, int i, int, const Layout& l) const {
         if (l.whole)  // tile-uniform
             return make_uint2(reinterpret_cast<const uint32_t*>(buf)[i],
-                              reinterpret_cast<const uint32_t*>(buf + (size_t)kSTile * 4)[i]);
+                              reinterpret_cast<const uint32_t*>(buf + kValOff)[i]);
         const uint32_t ik = (uint32_t)i - l.hk, iv = (uint32_t)i - l.hv;  // wrap below the span
         const uint32_t key = ik < l.nk ? reinterpret_cast<const uint32_t*>(buf)[ik] : __ldcs(k + t0 + i);
-        const uint32_t val = iv < l.nv ? reinterpret_cast<const uint32_t*>(buf + (size_t)kSTile * 4)[iv]
+        const uint32_t val = iv < l.nv ? reinterpret_cast<const uint32_t*>(buf + kValOff)[iv]
                                        : __ldcs(v + t0 + i);
         return make_uint2(key, val);
+    }
+    __device__ __forceinline__ bool fast(const Layout& l) const { return l.whole; }
+    template <int NITEMS, int NT>
+    __device__ __forceinline__ void load_full(const unsigned char* buf, const Layout&, uint2 (&it)[NITEMS]) const {
+        static_assert(NITEMS % 4 == 0, "four tuples per 16-byte load");
+        const uint4* ks = reinterpret_cast<const uint4*>(buf);
+        const uint4* vs = reinterpret_cast<const uint4*>(buf + kValOff);
+#pragma unroll
+        for (int j = 0; j < NITEMS / 4; ++j) {
+            const uint4 kk = ks[j * NT + threadIdx.x];
+            const uint4 vv = vs[j * NT + threadIdx.x];
+            it[4 * j] = make_uint2(kk.x, vv.x);
+            it[4 * j + 1] = make_uint2(kk.y, vv.y);
+            it[4 * j + 2] = make_uint2(kk.z, vv.z);
+            it[4 * j + 3] = make_uint2(kk.w, vv.w);
+        }
     }
 };
 
@@ -316,29 +343,40 @@ struct Bin2 {
     __device__ __forceinline__ uint32_t operator()(uint32_t key) const { return part2_m<M>(f, key); }
 };
 
+// Tiles of the two scatter forms. The bulk-store form (up to kBulkMaxBins bins) takes 12288-tuple
+// tiles, one third more than the write-pass form (whose staged-bin array and per-bin deltas leave
+// room for 8192 at 4096 bins): longer runs per bin and tile, and the per-tile scan, barriers and
+// run stores amortised over more tuples (level-1 scatter at 640M keys: 2.85 ms with 8192, 2.40 ms
+// with 12288).
+constexpr int kSTileW = 8192;    // write-pass form
+constexpr int kSTileB = kSTile;  // bulk-store form
+static_assert(kSTileB % (4 * kSThreads) == 0 && kSTileW % (4 * kSThreads) == 0, "whole 16-byte loads per thread");
+
 // Scatters tuples [begin, end) of `in` into `out`. cursor[b] is the next output position of bin
-// b; it advances as tiles are written. Each tile of kSTile tuples arrives by bulk copy into one of
+// b; it advances as tiles are written. Each tile of kSTileW tuples arrives by bulk copy into one of
 // the two input buffers while the previous tile is processed. Per tile every thread holds its
-// kSTile / kSThreads tuples in registers, takes a rank inside its tuple's bin with one shared-memory
-// atomic, and after a scan of the bin counts writes the tuple to its bin-ordered position in
-// `stage` (the tile's own input buffer, free once the tuples are in registers) with its bin in
-// `sbin`. The write pass then stores consecutive staged positions from consecutive threads, i.e.
-// runs of one bin to consecutive addresses; delta[b] = cursor[b] - (first staged position of b)
+// kSTileW / kSThreads tuples in registers, takes a rank inside its tuple's bin with one
+// shared-memory atomic, and after a scan of the bin counts writes the tuple to its bin-ordered
+// position in `stage` (the tile's own input buffer, free once the tuples are in registers) with its
+// bin in `sbin`. The write pass then stores consecutive staged positions from consecutive threads,
+// i.e. runs of one bin to consecutive addresses; delta[b] = cursor[b] - (first staged position of b)
 // turns a staged position into its output position with one add.
 // `inbuf` holds two tile buffers, `bars` their mbarriers, `ph` the parity of each barrier.
+constexpr size_t kTileBufW = (size_t)(kSTileW + 2) * 8;  // one write-pass input buffer
+
 template <class In, class Bin>
 __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
                               uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, int64_t* delta,
                               uint32_t* cnt, uint16_t* sbin, uint32_t* tmp, unsigned char* inbuf, uint64_t* bars,
                               uint32_t& ph, unsigned long long* errors, uint32_t polls) {
-    constexpr int kItems = kSTile / kSThreads;
-    const int64_t ntiles = (end - begin + kSTile - 1) / kSTile;
+    constexpr int kItems = kSTileW / kSThreads;
+    const int64_t ntiles = (end - begin + kSTileW - 1) / kSTileW;
     if (ntiles <= 0) return;
     for (int x = threadIdx.x; x < nbins; x += kSThreads) cnt[x] = 0;
-    if (threadIdx.x == 0) in.issue(begin, (int)min_i64(kSTile, end - begin), inbuf, &bars[0]);
+    if (threadIdx.x == 0) in.issue(begin, (int)min_i64(kSTileW, end - begin), inbuf, &bars[0]);
     for (int64_t t = 0; t < ntiles; ++t) {
-        const int64_t t0 = begin + t * kSTile;
-        const int tn = (int)min_i64(kSTile, end - t0);
+        const int64_t t0 = begin + t * kSTileW;
+        const int tn = (int)min_i64(kSTileW, end - t0);
         const int b = (int)(t & 1);
         mbar_wait(&bars[b], (ph >> b) & 1u, errors, polls);
         ph ^= 1u << b;
@@ -346,18 +384,28 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
         // (and cnt is zero again): the next tile may now be copied into b ^ 1.
         __syncthreads();
         if (threadIdx.x == 0 && t + 1 < ntiles)
-            in.issue(t0 + kSTile, (int)min_i64(kSTile, end - t0 - kSTile), inbuf + (b ^ 1) * kTileBuf, &bars[b ^ 1]);
-        unsigned char* buf = inbuf + b * kTileBuf;
+            in.issue(t0 + kSTileW, (int)min_i64(kSTileW, end - t0 - kSTileW), inbuf + (b ^ 1) * kTileBufW, &bars[b ^ 1]);
+        unsigned char* buf = inbuf + b * kTileBufW;
         const auto lay = in.layout(t0, tn);
+        const bool full = tn == kSTileW && in.fast(lay);  // block-uniform
         uint2 it[kItems];
         uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
+        if (full) {
+            in.template load_full<kItems, kSThreads>(buf, lay, it);
 #pragma unroll
-        for (int k = 0; k < kItems; ++k) {
-            const int i = k * kSThreads + threadIdx.x;
-            if (i < tn) {
-                it[k] = in.item(buf, t0, i, tn, lay);
+            for (int k = 0; k < kItems; ++k) {
                 const uint32_t bb = bin(it[k].x);
                 br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kItems; ++k) {
+                const int i = k * kSThreads + threadIdx.x;
+                if (i < tn) {
+                    it[k] = in.item(buf, t0, i, tn, lay);
+                    const uint32_t bb = bin(it[k].x);
+                    br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
+                }
             }
         }
         __syncthreads();
@@ -372,8 +420,7 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
         uint2* stage = reinterpret_cast<uint2*>(buf);
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
-            const int i = k * kSThreads + threadIdx.x;
-            if (i < tn) {
+            if (full || k * kSThreads + (int)threadIdx.x < tn) {
                 const uint32_t bb = br[k] >> 16;
                 const uint32_t pos = cnt[bb] + (br[k] & 0xffffu);
                 stage[pos] = it[k];
@@ -398,7 +445,8 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
 // The same scatter for at most kBulkMaxBins bins, with each bin's run of a tile written by the
 // bulk-copy engine instead of a write pass over the tile. Thread x owns bin x. Per tile:
 //   1. every thread takes its tuples from the tile buffer into registers and ranks them within
-//      their bins (one shared-memory atomic each);
+//      their bins (one shared-memory atomic each); a whole tile is read with 16-byte loads and no
+//      bounds tests;
 //   2. a scan of the bin counts gives each bin its staged start: bin b gets count + 1 slots, and
 //      its run starts on the slot whose parity equals the parity of its output position, so the
 //      run's source and destination are 16-byte aligned together;
@@ -413,13 +461,12 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
 // step 1, by when they normally have).
 constexpr int kBulkMaxBins = 1024;
 static_assert(kBulkMaxBins <= kSThreads, "one bin per thread");
-// The level-2 scatter takes the bulk path up to 256 bins only: at 512 bins (640M x 640M, slices of
-// 16 tiles) the write-pass form measured 3.43 ms against 3.59 ms, while at the batch's fan-outs
-// (<= 64) the bulk form is faster (3.41 against 4.09 ms for the R side of 256 uneven joins).
-constexpr int kBulkMaxBinsL2 = 256;
+// The level-2 scatter takes the bulk path up to the same bin count: with 12288-tuple tiles it beats
+// the write-pass form at 512 bins too (R's level-2 scatter at 640M keys: 3.14 against 3.28 ms).
+constexpr int kBulkMaxBinsL2 = kBulkMaxBins;
 // One tile buffer of the bulk scatter: the tile plus one slot per bin, a multiple of 16 bytes.
 __host__ __device__ constexpr size_t bulk_tile_buf(int max_bins) {
-    return (size_t)((kSTile + max_bins + 2 + 1) & ~1) * 8;
+    return (size_t)((kSTileB + max_bins + 2 + 1) & ~1) * 8;
 }
 
 template <class In, class Bin>
@@ -427,38 +474,48 @@ __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, con
                                    uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, uint32_t* cnt,
                                    uint32_t* spos, uint32_t* tmp, unsigned char* inbuf, size_t buf_stride,
                                    uint64_t* bars, uint32_t& ph, unsigned long long* errors, uint32_t polls) {
-    constexpr int kItems = kSTile / kSThreads;
+    constexpr int kItems = kSTileB / kSThreads;
     constexpr int kWarps = kSThreads / 32;
-    const int64_t ntiles = (end - begin + kSTile - 1) / kSTile;
+    const int64_t ntiles = (end - begin + kSTileB - 1) / kSTileB;
     if (ntiles <= 0) return;
     const int x = threadIdx.x, lane = x & 31, wid = x >> 5;
     const bool owner = x < nbins;
     if (owner) cnt[x] = 0;
-    if (x == 0) in.issue(begin, (int)min_i64(kSTile, end - begin), inbuf, &bars[0]);
+    if (x == 0) in.issue(begin, (int)min_i64(kSTileB, end - begin), inbuf, &bars[0]);
     __syncthreads();  // cnt is zero
     for (int64_t t = 0; t < ntiles; ++t) {
-        const int64_t t0 = begin + t * kSTile;
-        const int tn = (int)min_i64(kSTile, end - t0);
+        const int64_t t0 = begin + t * kSTileB;
+        const int tn = (int)min_i64(kSTileB, end - t0);
         const int b = (int)(t & 1);
         mbar_wait(&bars[b], (ph >> b) & 1u, errors, polls);
         ph ^= 1u << b;
         unsigned char* buf = inbuf + b * buf_stride;
         const auto lay = in.layout(t0, tn);
+        const bool full = tn == kSTileB && in.fast(lay);  // block-uniform
         uint2 it[kItems];
         uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
+        if (full) {
+            in.template load_full<kItems, kSThreads>(buf, lay, it);
 #pragma unroll
-        for (int k = 0; k < kItems; ++k) {
-            const int i = k * kSThreads + x;
-            if (i < tn) {
-                it[k] = in.item(buf, t0, i, tn, lay);
+            for (int k = 0; k < kItems; ++k) {
                 const uint32_t bb = bin(it[k].x);
                 br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kItems; ++k) {
+                const int i = k * kSThreads + x;
+                if (i < tn) {
+                    it[k] = in.item(buf, t0, i, tn, lay);
+                    const uint32_t bb = bin(it[k].x);
+                    br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
+                }
             }
         }
         bulk_wait_read();  // this thread's bulk stores of the previous tile have read buffer b ^ 1
         __syncthreads();
         if (x == 0 && t + 1 < ntiles)
-            in.issue(t0 + kSTile, (int)min_i64(kSTile, end - t0 - kSTile), inbuf + (b ^ 1) * buf_stride, &bars[b ^ 1]);
+            in.issue(t0 + kSTileB, (int)min_i64(kSTileB, end - t0 - kSTileB), inbuf + (b ^ 1) * buf_stride, &bars[b ^ 1]);
         // exclusive scan of the counts, one bin per thread (every warp scans the warp totals itself);
         // cursor[x] (the next output position of bin x) and spos[x] (staged start | count << 16)
         // stay in shared memory until the owner stores the run, which keeps registers free for the
@@ -487,10 +544,15 @@ __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, con
         }
         __syncthreads();
         uint2* stage = reinterpret_cast<uint2*>(buf);
+        if (full) {
 #pragma unroll
-        for (int k = 0; k < kItems; ++k) {
-            const int i = k * kSThreads + x;
-            if (i < tn) stage[(spos[br[k] >> 16] & 0xffffu) + (br[k] & 0xffffu)] = it[k];
+            for (int k = 0; k < kItems; ++k) stage[(spos[br[k] >> 16] & 0xffffu) + (br[k] & 0xffffu)] = it[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < kItems; ++k) {
+                const int i = k * kSThreads + x;
+                if (i < tn) stage[(spos[br[k] >> 16] & 0xffffu) + (br[k] & 0xffffu)] = it[k];
+            }
         }
         fence_proxy_async();  // the staging stores before the bulk engine reads them
         __syncthreads();
@@ -521,7 +583,7 @@ __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, con
     bulk_wait_read();
     __syncthreads();  // the bulk stores are done with the buffers; cnt is zero
 }
-static_assert(kSTile + kBulkMaxBins + 2 < (1 << 16) && kSTile < (1 << 16), "staged start and count in 16 bits");
+static_assert(kSTileB + kBulkMaxBins + 2 < (1 << 16) && kSTileB < (1 << 16), "staged start and count in 16 bits");
 
 // Shared-memory layout of the scatter kernels: two tile buffers, then cursor and delta (int64 per
 // bin), the bin counts (uint32 per bin) and the staged bins (uint16 per tile position).
@@ -529,7 +591,7 @@ __device__ __forceinline__ void scatter_carve(unsigned char* smem, int max_bins,
                                               int64_t*& cursor, int64_t*& delta, uint32_t*& cnt,
                                               uint16_t*& sbin) {
     inbuf = smem;
-    cursor = reinterpret_cast<int64_t*>(smem + 2 * kTileBuf);
+    cursor = reinterpret_cast<int64_t*>(smem + 2 * kTileBufW);
     delta = cursor + max_bins;
     cnt = reinterpret_cast<uint32_t*>(delta + max_bins);
     sbin = reinterpret_cast<uint16_t*>(cnt + max_bins);
@@ -554,32 +616,38 @@ __device__ __forceinline__ void init_bars(uint64_t* bars) {
     __syncthreads();
 }
 
-// Bloom probe, split in two so a thread can have several block loads in flight: the address of a
-// key's 32-byte block in the segment of its finest partition f, then the test of the loaded words.
-// Bit masks of a key with hash g: the shared-memory pattern tables (pat), or the bit arithmetic for
-// a join whose k differs from the tables' k.
+// The Bloom kernels keep the launch's pattern table (one pair of masks per pattern index, filled for
+// the launch's k, which every filtered join of a launch shares) in shared memory. Fill is
+// block-wide; the caller synchronises. k == 0: no filter.
+__device__ __forceinline__ void fill_patterns(uint2* pat, int k) {
+    if (k == 0) return;
+    for (int i = threadIdx.x; i < kPatterns; i += blockDim.x)
+        pat[i] = make_uint2(bloom_pattern(0, (uint32_t)i, k), bloom_pattern(1, (uint32_t)i, k));
+}
+// Masks of a key at slot s: compile-time shifts (K == kBloomFastK) or the pattern table.
 template <int K>
-__device__ __forceinline__ void key_masks(const uint32_t* pat, uint64_t g, int k, uint32_t& ma, uint32_t& mb) {
-    if constexpr (K == kBloomFastK) bloom_pattern_masks(pat, g, ma, mb);
-    else bloom_masks<0>(g, k, ma, mb);
+__device__ __forceinline__ uint2 slot_masks(const uint2* pat, const BloomSlot& s) {
+    if constexpr (K == kBloomFastK) return bloom_masks7(s.g);
+    else return pat[s.pidx];
 }
-// Fills the two pattern tables for k (block-wide; the caller synchronises).
-__device__ __forceinline__ void fill_patterns(uint32_t* pat, int k) {
-    for (int i = threadIdx.x; i < 2 * kPatterns; i += blockDim.x) pat[i] = bloom_pattern(i / kPatterns, i % kPatterns, k);
-}
-
-// The Bloom mask class of a join (the K of the kernel instantiation that handles it).
+// Shared-memory entries of the pattern table of a kernel of class K (none for k = 7).
+template <int K>
+constexpr int pat_entries() { return K == kBloomFastK ? 1 : kPatterns; }
+// The mask class of a join (the K of the instantiation that handles it).
 __device__ __forceinline__ int bloom_kclass(const JoinDesc& d) {
-    return (d.bloom != nullptr && d.bloom_pat) ? kBloomFastK : 0;
+    return (d.bloom != nullptr && d.bloom_k == kBloomFastK) ? kBloomFastK : 0;
 }
-
-// Address of the first word of a key's block in the segment of finest partition f.
-__device__ __forceinline__ const uint32_t* bloom_words(const uint32_t* __restrict__ bloom, uint32_t seg_blocks,
-                                                       uint32_t f, uint32_t block) {
-    return bloom + ((int64_t)f * seg_blocks + block) * 8;
+// A word pair passes when it holds every bit of both masks.
+__device__ __forceinline__ bool bloom_pass(uint2 w, uint2 mk) {
+    return (((w.x & mk.x) ^ mk.x) | ((w.y & mk.y) ^ mk.y)) == 0u;
+}
+// Finest partition of a key with mix m (hash mode: the top b1 + b2 bits) or key (modulo mode).
+template <int M>
+__device__ __forceinline__ uint32_t fine_of(const PartFn& f, uint32_t key, uint32_t m) {
+    if constexpr (M == 0) return (uint32_t)(((uint64_t)m << (f.b1 + f.b2)) >> 32);
+    else return fastmod(key, f.M1, f.P1) * f.P2 + fastmod(key, f.M2, f.P2);
 }
 constexpr int kProbeILP = 6;  // keys per thread with their filter words in flight together
-constexpr int kL2ProbeILP = 6;  // keys per thread with their filter words in flight in the level-2 probe
 
 // ---------------------------------------------------------------------------------------------
 // Level 1, pass 1: per-slice histogram over P1 partitions (R, or S without Bloom), or the fused
@@ -592,8 +660,8 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
           uint32_t* __restrict__ hist, unsigned long long* gwords, int pat_k) {
     extern __shared__ uint32_t sh_cnt[];  // [max P1]
     __shared__ uint32_t s_cursor;
-    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // pattern tables
-    if constexpr (K == kBloomFastK) fill_patterns(s_pat, pat_k);  // synchronised by the slice loop's first barrier
+    __shared__ uint2 s_pat[pat_entries<K>()];  // pattern table (k != 7)
+    if (K != kBloomFastK && rel == 1) fill_patterns(s_pat, pat_k);  // synchronised by the slice loop's first barrier
     const int lane = threadIdx.x & 31;
     const int64_t total = slice_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
@@ -655,7 +723,6 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t* __restrict__ val = R.val;
             // descriptor fields in registers: the stores below could alias the descriptor, so
             // fields read through `d` inside the loop would be reloaded after every store
-            const int bk = d.bloom_k;
             const uint32_t seg_blocks = d.seg_blocks;
             const uint32_t* __restrict__ bloom = d.bloom;
             uint2* __restrict__ cmp = R.cmp;
@@ -663,7 +730,7 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             const uint32_t* __restrict__ skey = key + b;
             for (int32_t r0 = 0; r0 < len; r0 += kProbeILP * kThreads) {
                 uint32_t kk[kProbeILP];
-                uint32_t va[kProbeILP], vb[kProbeILP];
+                uint2 wv[kProbeILP], mk[kProbeILP];
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
@@ -672,25 +739,17 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
-                    if (r < len) {
-                        BloomKey bkey;
-                        bloom_place(bloom_hash(kk[u]), seg_blocks, bkey);
-                        const uint32_t* w =
-                            bloom_words(bloom, seg_blocks, part_fine_m<M>(pf, kk[u]), bkey.block);
-                        const uint2 pair = __ldg(reinterpret_cast<const uint2*>(w + bkey.wa));
-                        va[u] = pair.x;
-                        vb[u] = pair.y;
-                    }
+                    const uint32_t m = mix32(kk[u]);
+                    const BloomSlot sl = bloom_slot(m, fine_of<M>(pf, kk[u], m), seg_blocks);
+                    wv[u] = make_uint2(0u, 0u);
+                    if (r < len) wv[u] = __ldg(reinterpret_cast<const uint2*>(bloom + sl.widx));
+                    mk[u] = slot_masks<K>(s_pat, sl);
                 }
                 uint32_t pm = 0;  // bit u: tuple u passed the filter
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
                     const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
-                    if (r < len) {
-                        uint32_t ma, mb;
-                        key_masks<K>(s_pat, bloom_hash(kk[u]), bk, ma, mb);
-                        if ((va[u] & ma) == ma && (vb[u] & mb) == mb) pm |= 1u << u;
-                    }
+                    if (r < len && bloom_pass(wv[u], mk[u])) pm |= 1u << u;
                 }
                 // survivors: one shared-memory atomic per warp for the whole group
                 uint32_t bal[kProbeILP];
@@ -784,13 +843,15 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
                               &gwords[kGErrors], polls);
         } else {
             const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 3) == 0;
-            const KvTiles in{R.key, R.val, al};
-            if constexpr (kBulk)
+            if constexpr (kBulk) {
+                const KvTiles<kSTileB> in{R.key, R.val, al};
                 scatter_tiles_bulk(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
                                    bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors], polls);
-            else
+            } else {
+                const KvTiles<kSTileW> in{R.key, R.val, al};
                 scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph,
                               &gwords[kGErrors], polls);
+            }
         }
     }
     if constexpr (kBulk) bulk_wait_all();  // the bulk stores have written the output before the kernel ends
@@ -862,21 +923,14 @@ __global__ void k_l2_plan(const JoinDesc* __restrict__ J, int nj, int rel, const
     }
 }
 
-// Level-2 histogram of one slice: counts by level-2 id, or (S with a level-2 Bloom probe) tests
-// every key and compacts the survivors into cmp[slice begin, + survivors).
-// kBloom selects the slices this launch handles (S slices of joins probing their filter at level 2,
-// or all others); one instantiation per form keeps each within 64 registers.
-template <bool kBloom, int M, int K>
+// Level-2 histogram of one slice: counts by level-2 id. Handles every slice except those of S in
+// joins that probe their filter at level 2 (k_l2_bloom does those).
+template <int M>
 __global__ void __launch_bounds__(kThreads, 2)
 k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
           const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
-          uint32_t* __restrict__ hist2, uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords,
-          int pat_k) {
+          uint32_t* __restrict__ hist2, unsigned long long* gwords) {
     extern __shared__ uint32_t cnt[];  // [max P2]
-    __shared__ uint32_t s_surv;
-    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // pattern tables
-    if constexpr (K == kBloomFastK && kBloom) fill_patterns(s_pat, pat_k);  // synchronised by the slice loop's first barrier
-    const int lane = threadIdx.x & 31;
     const int64_t total = (int64_t)gwords[kGL2Slices + rel];
     for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
         const L2Slice x = l2_decode(seg_prefix, nj, seg_off, seg_ns, total_segs, t);
@@ -887,92 +941,142 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         const int64_t end = min_i64(R.b1[x.p + 1], begin + R.l2_slice);
         const Bin2<M> bin{d.pf};
         const bool bloom = rel == 1 && d.bloom != nullptr && d.bloom_level == 2;
-        if (bloom != kBloom || d.pf.mode != M || (kBloom && bloom_kclass(d) != K))
-            continue;  // another instantiation's slice (block-uniform)
+        if (bloom || d.pf.mode != M) continue;  // another kernel's slice (block-uniform)
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cnt[q] = 0;
-        if (threadIdx.x == 0) s_surv = 0;
         __syncthreads();
         const uint2* __restrict__ l1 = R.l1;
-        if constexpr (!kBloom) {
-            for (int64_t i0 = begin + threadIdx.x; i0 < end; i0 += 8 * kThreads) {
-                uint32_t kk[8];
+        for (int64_t i0 = begin + threadIdx.x; i0 < end; i0 += 8 * kThreads) {
+            uint32_t kk[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int64_t i = i0 + u * kThreads;
-                    kk[u] = i < end ? __ldcs(&l1[i].x) : 0u;
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u)
-                    if (i0 + u * kThreads < end) atomicAdd(&cnt[bin(kk[u])], 1u);
+            for (int u = 0; u < 8; ++u) {
+                const int64_t i = i0 + u * kThreads;
+                kk[u] = i < end ? __ldcs(&l1[i].x) : 0u;
             }
-        } else {
-            // the filter segments of this level-1 partition are shared by every CTA working on it
-            const int bk = d.bloom_k;
-            const uint32_t seg_blocks = d.seg_blocks;
-            const uint32_t* __restrict__ bloom = d.bloom;
-            uint2* __restrict__ cmp = R.cmp;
-            const uint32_t fbase = x.p * P2;
-            const int32_t len = (int32_t)(end - begin);  // at most one level-2 slice
-            const uint2* __restrict__ src = l1 + begin;
-            for (int32_t r0 = 0; r0 < len; r0 += kL2ProbeILP * kThreads) {
-                uint2 e[kL2ProbeILP];
-                uint32_t va[kL2ProbeILP], vb[kL2ProbeILP];
 #pragma unroll
-                for (int u = 0; u < kL2ProbeILP; ++u) {
-                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
-                    e[u] = r < len ? __ldcs(src + r) : make_uint2(0u, 0u);
-                }
-#pragma unroll
-                for (int u = 0; u < kL2ProbeILP; ++u) {
-                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
-                    if (r < len) {
-                        BloomKey bkey;
-                        bloom_place(bloom_hash(e[u].x), seg_blocks, bkey);
-                        const uint32_t* w = bloom_words(bloom, seg_blocks, fbase + bin(e[u].x), bkey.block);
-                        const uint2 pair = __ldg(reinterpret_cast<const uint2*>(w + bkey.wa));
-                        va[u] = pair.x;
-                        vb[u] = pair.y;
-                    }
-                }
-                uint32_t pm = 0;  // bit u: tuple u passed the filter
-#pragma unroll
-                for (int u = 0; u < kL2ProbeILP; ++u) {
-                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
-                    if (r < len) {
-                        uint32_t ma, mb;
-                        key_masks<K>(s_pat, bloom_hash(e[u].x), bk, ma, mb);
-                        if ((va[u] & ma) == ma && (vb[u] & mb) == mb) pm |= 1u << u;
-                    }
-                }
-                // survivors: one shared-memory atomic per warp for the whole group
-                uint32_t bal[kL2ProbeILP];
-                uint32_t tot = 0;
-#pragma unroll
-                for (int u = 0; u < kL2ProbeILP; ++u) {
-                    bal[u] = __ballot_sync(0xffffffffu, (pm >> u) & 1u);
-                    tot += __popc(bal[u]);
-                }
-                if (tot) {
-                    uint32_t base = 0;
-                    if (lane == 0) base = atomicAdd(&s_surv, tot);
-                    base = __shfl_sync(0xffffffffu, base, 0);
-#pragma unroll
-                    for (int u = 0; u < kL2ProbeILP; ++u) {
-                        if ((pm >> u) & 1u) {
-                            atomicAdd(&cnt[bin(e[u].x)], 1u);
-                            const int64_t dst = begin + base + __popc(bal[u] & lanemask_lt());
-                            if (dst < end) cmp[dst] = e[u];
-                            else atomicAdd(&gwords[kGErrors], 1ull);
-                        }
-                        base += __popc(bal[u]);
-                    }
-                }
-            }
+            for (int u = 0; u < 8; ++u)
+                if (i0 + u * kThreads < end) atomicAdd(&cnt[bin(kk[u])], 1u);
         }
         __syncthreads();
         uint32_t* H = hist2 + R.h2_base + x.local_off * P2;
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) H[(int64_t)q * x.ns + x.sl] = cnt[q];
-        if (threadIdx.x == 0 && bloom) {
+        __syncthreads();
+    }
+}
+
+// Level-2 pass of S for joins that probe their filter at level 2: every key of the slice is tested
+// against the filter segment of its finest partition, and the survivors are compacted into
+// cmp[slice begin, + survivors) and counted by level-2 id. The filter segments of one level-1
+// partition are contiguous (1.5 MB at 640M keys, 10 bits/key) and the slices of neighbouring
+// partitions run together, so the filter words come from L2. The pass is bound by the integer ALU
+// pipe, so the per-key work is kept to the minimum: one mix of the key from which its level-2 id,
+// block, word pair (bloom_slot) and pattern index derive, one 8-byte filter load, one 8-byte pattern
+// load and a two-word test; full groups of U keys per thread run without bounds tests. Survivors
+// are re-ranked per warp with one ballot per key and one shared atomic per warp group, and their
+// level-2 ids recomputed (about one key in nine survives at 10% matches).
+constexpr int kL2BloomU = 6;  // keys per thread with their filter words in flight
+
+// One group of U keys per thread starting at slice offset r0; kTail: the group may end past len.
+template <int M, int K, bool kTail>
+__device__ __forceinline__ void l2_bloom_group(const uint2* __restrict__ src, int32_t r0, int32_t len,
+                                               const uint32_t* __restrict__ bloom, uint32_t seg_blocks,
+                                               uint32_t fine0, const PartFn& pf, const uint2* pat,
+                                               uint2* __restrict__ cmp, uint32_t* cnt,
+                                               uint32_t* s_surv, unsigned long long* errors, int lane) {
+    constexpr int U = kL2BloomU;
+    uint2 e[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+        e[u] = (!kTail || r < len) ? __ldcs(src + r) : make_uint2(0u, 0u);
+    }
+    uint2 wv[U], mk[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+        const uint32_t m = mix32(e[u].x);
+        uint32_t q;
+        if constexpr (M == 0) q = (uint32_t)(((uint64_t)(m << pf.b1) << pf.b2) >> 32);
+        else q = fastmod(e[u].x, pf.M2, pf.P2);
+        const BloomSlot sl = bloom_slot(m, fine0 + q, seg_blocks);
+        wv[u] = make_uint2(0u, 0u);
+        if (!kTail || r < len) wv[u] = __ldg(reinterpret_cast<const uint2*>(bloom + sl.widx));
+        mk[u] = slot_masks<K>(pat, sl);
+    }
+    uint32_t pm = 0;  // bit u: key u passed the filter
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
+        if ((!kTail || r < len) && bloom_pass(wv[u], mk[u])) pm |= 1u << u;
+    }
+    // survivors: one shared-memory atomic per warp for the whole group
+    uint32_t bal[U];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        bal[u] = __ballot_sync(0xffffffffu, (pm >> u) & 1u);
+        tot += __popc(bal[u]);
+    }
+    if (tot) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(s_surv, tot);
+        base = __shfl_sync(0xffffffffu, base, 0);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if ((pm >> u) & 1u) {
+                atomicAdd(&cnt[part2_m<M>(pf, e[u].x)], 1u);
+                const uint32_t dst = base + __popc(bal[u] & lanemask_lt());
+                if ((int32_t)dst < len) cmp[dst] = e[u];
+                else atomicAdd(errors, 1ull);
+            }
+            base += __popc(bal[u]);
+        }
+    }
+}
+
+template <int M, int K>
+__global__ void __launch_bounds__(kThreads, 2)
+k_l2_bloom(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ seg_prefix,
+           const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
+           uint32_t* __restrict__ hist2, uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords, int pat_k) {
+    constexpr int U = kL2BloomU;
+    extern __shared__ uint32_t cnt[];  // [max P2]
+    __shared__ uint32_t s_surv;
+    __shared__ uint2 s_pat[pat_entries<K>()];  // pattern table (k != 7)
+    if (K != kBloomFastK) fill_patterns(s_pat, pat_k);  // synchronised by the slice loop's first barrier
+    const int lane = threadIdx.x & 31;
+    const int64_t total = (int64_t)gwords[kGL2Slices + 1];
+    for (int64_t t = blockIdx.x; t < total; t += gridDim.x) {
+        const L2Slice x = l2_decode(seg_prefix, nj, seg_off, seg_ns, total_segs, t);
+        const JoinDesc& d = J[x.j];
+        if (d.bloom == nullptr || d.bloom_level != 2 || d.pf.mode != M || bloom_kclass(d) != K)
+            continue;  // another kernel's slice (block-uniform)
+        const RelPlan& R = d.rel[1];
+        const PartFn pf = d.pf;
+        const uint32_t P2 = pf.P2;
+        const int64_t begin = R.b1[x.p] + x.sl * R.l2_slice;
+        const int64_t end = min_i64(R.b1[x.p + 1], begin + R.l2_slice);
+        for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cnt[q] = 0;
+        if (threadIdx.x == 0) s_surv = 0;
+        __syncthreads();
+        // descriptor fields in registers: the stores below could alias the descriptor
+        const uint32_t seg_blocks = d.seg_blocks;
+        const uint32_t* __restrict__ bloom = d.bloom;
+        uint2* __restrict__ cmp = R.cmp + begin;
+        const uint2* __restrict__ src = R.l1 + begin;
+        const int32_t len = (int32_t)(end - begin);  // at most one level-2 slice
+        const int32_t full = len - len % (U * kThreads);
+        const uint32_t fine0 = x.p * P2;
+        int32_t r0 = 0;
+        for (; r0 < full; r0 += U * kThreads)
+            l2_bloom_group<M, K, false>(src, r0, len, bloom, seg_blocks, fine0, pf, s_pat, cmp, cnt,
+                                     &s_surv, &gwords[kGErrors], lane);
+        if (r0 < len)
+            l2_bloom_group<M, K, true>(src, r0, len, bloom, seg_blocks, fine0, pf, s_pat, cmp, cnt,
+                                    &s_surv, &gwords[kGErrors], lane);
+        __syncthreads();
+        uint32_t* H = hist2 + R.h2_base + x.local_off * P2;
+        for (uint32_t q = threadIdx.x; q < P2; q += kThreads) H[(int64_t)q * x.ns + x.sl] = cnt[q];
+        if (threadIdx.x == 0) {
             slice_cnt2[t] = s_surv;
             atomicAdd(reinterpret_cast<unsigned long long*>(&d.counters[kCntSurvivors]), (unsigned long long)s_surv);
         }
@@ -1053,15 +1157,46 @@ __global__ void k_l2_bounds(const JoinDesc* __restrict__ J, int nj, int rel, con
 // Bloom build: one CTA per group of G consecutive finest partitions of a Bloom-enabled join
 // (G = JoinDesc::bloom_group, chosen so the group's segments fit in shared memory). The group's R
 // tuples are contiguous in the final R buffer; every key sets its bits in its two words with two
-// 32-bit atomicOr in the shared-memory copy of its segment, and the segments are written out whole, so the filter needs
-// no clearing. A segment too large for shared memory (G = 1 then) is built with global atomicOr.
+// 32-bit atomicOr in the shared-memory copy of its segment, and the segments are written out
+// whole, so the filter needs no clearing. A segment too large for shared memory (G = 1 then) is
+// built with global atomicOr. The kernel is bound by the integer ALU pipe: per key one mix, the
+// slot arithmetic of bloom_slot on the group-relative segment index, one pattern look-up and the two
+// atomics, with 32-bit indices and no bounds tests in full groups.
+template <int M, int K, bool kTail>
+__device__ __forceinline__ void bloom_build_group(const uint2* __restrict__ buf, int32_t i0, int32_t n,
+                                                  uint32_t* dst, uint32_t f0, uint32_t nf, const PartFn& pf,
+                                                  uint32_t seg_blocks, const uint2* pat, unsigned long long* errors) {
+    uint32_t kk[kProbeILP];
+#pragma unroll
+    for (int u = 0; u < kProbeILP; ++u) {
+        const int32_t i = i0 + u * kThreads + (int32_t)threadIdx.x;
+        kk[u] = (!kTail || i < n) ? __ldcs(&buf[i].x) : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < kProbeILP; ++u) {
+        const int32_t i = i0 + u * kThreads + (int32_t)threadIdx.x;
+        if (kTail && i >= n) continue;
+        const uint32_t m = mix32(kk[u]);
+        const uint32_t local = fine_of<M>(pf, kk[u], m) - f0;
+        if (local >= nf) {  // a key outside the group's partitions: a partitioning fault
+            atomicAdd(errors, 1ull);
+            continue;
+        }
+        const BloomSlot sl = bloom_slot(m, local, seg_blocks);  // word index relative to the group
+        const uint2 mk = slot_masks<K>(pat, sl);
+        atomicOr(dst + sl.widx, mk.x);
+        if (mk.y) atomicOr(dst + sl.widx + 1, mk.y);
+    }
+}
+
 template <int M, int K>
 __global__ void __launch_bounds__(kThreads)
 k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ bloom_prefix,
               int smem_words, unsigned long long* gwords, int pat_k) {
     extern __shared__ __align__(16) uint32_t seg[];
-    __shared__ uint32_t s_pat[K == kBloomFastK ? 2 * kPatterns : 1];  // pattern tables
-    if constexpr (K == kBloomFastK) fill_patterns(s_pat, pat_k);  // synchronised by the group loop's first barrier
+    __shared__ uint2 s_pat[pat_entries<K>()];  // pattern table (k != 7)
+    if (K != kBloomFastK) fill_patterns(s_pat, pat_k);  // synchronised by the group loop's first barrier
+    unsigned long long* errors = &gwords[kGErrors];
     const int64_t total = bloom_prefix[nj];
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         const int j = find_owner(bloom_prefix, nj, g);
@@ -1071,49 +1206,36 @@ k_bloom_build(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict_
         const int64_t nfine = (int64_t)d.pf.P1 * d.pf.P2;
         const int64_t f0 = (g - bloom_prefix[j]) * d.bloom_group;
         const int64_t f1 = min_i64(f0 + d.bloom_group, nfine);
-        const uint2* buf = final_buf(d, 0);
         const int64_t begin = R.bounds[f0], end = R.bounds[f1];
+        const uint2* __restrict__ buf = final_buf(d, 0) + begin;
         const uint32_t nw = d.seg_blocks * 8;
         const int64_t words = (f1 - f0) * (int64_t)nw;
         uint32_t* gseg = d.bloom + f0 * (int64_t)nw;
         // descriptor fields in registers: the atomics below may write global memory (segments too
         // large for shared memory), so fields read through `d` would be reloaded after each one
-        const int k = d.bloom_k;
         const PartFn pf = d.pf;
         const uint32_t seg_blocks = d.seg_blocks;
+        const uint32_t nf = (uint32_t)(f1 - f0);
+        const int32_t n = (int32_t)(end - begin);  // the group's R tuples
         const bool in_smem = words <= smem_words;
         uint32_t* dst = in_smem ? seg : gseg;
         for (int64_t w = threadIdx.x; w < words; w += kThreads) dst[w] = 0;
         __syncthreads();
-        constexpr int64_t kStep = kProbeILP * kThreads;
-        if (threadIdx.x == 0) prefetch_l2_range(buf + begin, buf + min_i64(end, begin + 2 * kStep));
-        for (int64_t i0 = begin; i0 < end; i0 += kStep) {
-            if (threadIdx.x == 0 && i0 + 2 * kStep < end)
-                prefetch_l2_range(buf + i0 + 2 * kStep, buf + min_i64(end, i0 + 3 * kStep));
-            uint32_t kk[kProbeILP];
-#pragma unroll
-            for (int u = 0; u < kProbeILP; ++u) {
-                const int64_t i = i0 + u * kThreads + threadIdx.x;
-                kk[u] = i < end ? __ldcs(&buf[i].x) : 0u;
+        constexpr int32_t kStep = kProbeILP * kThreads;
+        const int32_t full = n - n % kStep;
+        if (threadIdx.x == 0) prefetch_l2_range(buf, buf + min_i64(n, 2 * kStep));
+        int32_t i0 = 0;
+        if (in_smem) {
+            for (; i0 < full; i0 += kStep) {
+                if (threadIdx.x == 0 && i0 + 2 * kStep < n)
+                    prefetch_l2_range(buf + i0 + 2 * kStep, buf + min_i64(n, (int64_t)i0 + 3 * kStep));
+                bloom_build_group<M, K, false>(buf, i0, n, seg, (uint32_t)f0, nf, pf, seg_blocks, s_pat, errors);
             }
-#pragma unroll
-            for (int u = 0; u < kProbeILP; ++u) {
-                const int64_t i = i0 + u * kThreads + threadIdx.x;
-                if (i >= end) continue;
-                const int64_t local = (int64_t)part_fine_m<M>(pf, kk[u]) - f0;
-                if (local < 0 || local >= f1 - f0) {
-                    atomicAdd(&gwords[kGErrors], 1ull);
-                    continue;
-                }
-                const uint64_t g = bloom_hash(kk[u]);
-                BloomKey bkey;
-                bloom_place(g, seg_blocks, bkey);
-                uint32_t ma, mb;
-                key_masks<K>(s_pat, g, k, ma, mb);
-                uint32_t* blk = dst + local * nw + (int64_t)bkey.block * 8;
-                atomicOr(blk + bkey.wa, ma);
-                if (mb) atomicOr(blk + bkey.wb, mb);
-            }
+            if (i0 < n)
+                bloom_build_group<M, K, true>(buf, i0, n, seg, (uint32_t)f0, nf, pf, seg_blocks, s_pat, errors);
+        } else {
+            for (; i0 < n; i0 += kStep)
+                bloom_build_group<M, K, true>(buf, i0, n, gseg, (uint32_t)f0, nf, pf, seg_blocks, s_pat, errors);
         }
         __syncthreads();
         if (in_smem) {
@@ -1779,7 +1901,7 @@ size_t probe_smem_bytes(int table_cap, int emit_key) {
 // (bulk_carve) or the write-pass layout (scatter_carve).
 static size_t scatter_smem(int max_bins, bool bulk) {
     if (bulk) return 2 * bulk_tile_buf(max_bins) + (size_t)max_bins * (8 + 4 + 4);
-    return 2 * kTileBuf + (size_t)max_bins * (8 + 8 + 4) + (size_t)kSTile * 2;
+    return 2 * kTileBufW + (size_t)max_bins * (8 + 8 + 4) + (size_t)kSTileW * 2;
 }
 
 static cudaError_t set_smem_attr(const void* fn, size_t bytes) {
@@ -1787,7 +1909,7 @@ static cudaError_t set_smem_attr(const void* fn, size_t bytes) {
 }
 
 // Calls f(std::integral_constant<int, M>, std::integral_constant<int, K>) for every partition mode
-// M and Bloom k class K present in the batch.
+// M and Bloom mask class K present in the batch.
 template <class F>
 static void for_mode_k(int modes, int kclasses, F&& f) {
     if ((modes & 1) && (kclasses & 1)) f(std::integral_constant<int, 0>{}, std::integral_constant<int, 0>{});
@@ -1923,20 +2045,21 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 return err;
             uint32_t* h2 = a.hist2 + a.h2_begin[rel];
             if ((err = cudaMemsetAsync(h2, 0, (size_t)a.h2_len[rel] * 4, st)) != cudaSuccess) return err;
-            for_modes(a.modes, [&](auto mt) {
-                constexpr int M = decltype(mt)::value;
-                const dim3 grid(grid_for(a.l2_slice_cap[rel], sms, 4));
-                k_l2_hist<false, M, 0><<<grid, kThreads, (size_t)a.max_p2 * 4, st>>>(
-                    a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2,
-                    a.gwords, 0);
-                ++launches;
-            });
+            if (!(rel == 1 && a.all_bloom_l2)) {
+                for_modes(a.modes, [&](auto mt) {
+                    constexpr int M = decltype(mt)::value;
+                    const dim3 grid(grid_for(a.l2_slice_cap[rel], sms, 4));
+                    k_l2_hist<M><<<grid, kThreads, (size_t)a.max_p2 * 4, st>>>(
+                        a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.gwords);
+                    ++launches;
+                });
+            }
             if (rel == 1 && a.any_bloom_l2) {
                 for_mode_k(a.modes, a.kclasses, [&](auto mt, auto kt) {
                     constexpr int M = decltype(mt)::value, K = decltype(kt)::value;
-                    k_l2_hist<true, M, K><<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4,
-                                            st>>>(a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs,
-                                                  a.hist2, a.slice_cnt2, a.gwords, a.pat_k);
+                    k_l2_bloom<M, K><<<grid_for(a.l2_slice_cap[rel], sms, 4), kThreads, (size_t)a.max_p2 * 4, st>>>(
+                        a.J, a.nj, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2, a.slice_cnt2, a.gwords,
+                        a.pat_k);
                     ++launches;
                 });
             }

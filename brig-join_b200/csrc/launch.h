@@ -40,10 +40,11 @@ struct PipelineArgs {
     int any_bloom;
     int any_bloom_l1;                 // some join probes its filter in S's first pass
     int any_bloom_l2;                 // some join probes its filter in S's second pass
+    int all_bloom_l2;                 // every two-level join probes its filter in S's second pass
     int modes;                        // partition modes present: bit 0 hash, bit 1 modulo
-    int kclasses;                     // Bloom mask classes present: bit 0 bit arithmetic (or no filter),
-                                      // bit 1 pattern tables
-    int pat_k;                        // k the Bloom kernels fill their pattern tables for
+    int kclasses;                     // Bloom mask classes present: bit 0 pattern table (or no filter),
+                                      // bit 1 compile-time k = 7
+    int pat_k;                        // k the Bloom kernels fill their pattern tables for (0: none)
     int num_sms;
     cudaEvent_t* stage_events;        // [kNumStages + 1] or nullptr
     cudaEvent_t s_ready;              // when set, S's passes wait for it (its inputs are still arriving)
