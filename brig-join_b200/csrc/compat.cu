@@ -8,6 +8,7 @@
 // runs the engine's task builder and probe kernel. gpu_main is the whole local join over files.
 // Every helper here synchronises with the host where the reference does (its entry points are
 // blocking); failures print to stderr and leave outputs untouched instead of exiting.
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -409,4 +410,188 @@ void gpu_main(std::vector<int>*, std::vector<int>*, const std::string& r_inputPa
         printf("[PE0] Total (H2D + join) %.4f sec, split tasks %lld\n", sec, overflow_tasks);
     }
     brig_join_destroy(h);
+}
+
+// ---- BloomFilter (src/bloom.cuh:8-36) ------------------------------------------------------------
+namespace brig {
+namespace {
+
+// The reference's Bloom hash (src/bloom.cu:24-31): the seed xor the key, then the two multiply /
+// xor-shift rounds of the MurmurHash3 finaliser.
+__host__ __device__ __forceinline__ uint32_t ref_bloom_hash(int32_t v, uint32_t seed) {
+    uint32_t h = seed ^ (uint32_t)v;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// The eight words a key sets in its 256-bit block (bit hash(v, j + 1) % 256 for j < k).
+__device__ __forceinline__ void ref_bloom_bits(int32_t v, int k, uint32_t (&w)[8]) {
+#pragma unroll
+    for (int x = 0; x < 8; ++x) w[x] = 0u;
+    for (int j = 0; j < k; ++j) {
+        const uint32_t pos = ref_bloom_hash(v, (uint32_t)j + 1u) & 255u;
+        const uint32_t bit = 1u << (pos & 31u), word = pos >> 5;
+#pragma unroll
+        for (int x = 0; x < 8; ++x) w[x] |= word == (uint32_t)x ? bit : 0u;
+    }
+}
+
+// One thread per key: the key's bits are gathered per word, then one atomicOr per touched word.
+__global__ void k_refbf_insert(uint32_t* __restrict__ f, const int* __restrict__ data, int64_t n, int k,
+                               uint64_t nblocks) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int v = data[i];
+        uint32_t w[8];
+        ref_bloom_bits(v, k, w);
+        uint32_t* b = f + (ref_bloom_hash(v, 1u) % nblocks) * 8;
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+            if (w[x]) atomicOr(b + x, w[x]);
+    }
+}
+
+// One thread per key: the key's block is read as two 16-byte loads; a key passes when every one
+// of its bits is set. Passing keys are counted with one atomic per warp.
+__global__ void k_refbf_query(const uint32_t* __restrict__ f, const int* __restrict__ data, int64_t n, int k,
+                              uint64_t nblocks, unsigned char* __restrict__ results,
+                              unsigned long long* __restrict__ passed) {
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        bool ok = false;
+        if (i < n) {
+            const int v = data[i];
+            uint32_t w[8];
+            ref_bloom_bits(v, k, w);
+            const uint4* b = reinterpret_cast<const uint4*>(f + (ref_bloom_hash(v, 1u) % nblocks) * 8);
+            const uint4 a = __ldg(b), c = __ldg(b + 1);
+            ok = ((a.x & w[0]) == w[0]) && ((a.y & w[1]) == w[1]) && ((a.z & w[2]) == w[2]) && ((a.w & w[3]) == w[3]) &&
+                 ((c.x & w[4]) == w[4]) && ((c.y & w[5]) == w[5]) && ((c.z & w[6]) == w[6]) && ((c.w & w[7]) == w[7]);
+            if (results) results[i] = ok ? 1 : 0;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, ok);
+        if ((threadIdx.x & 31) == 0 && m) atomicAdd(passed, (unsigned long long)__popc(m));
+    }
+}
+
+std::vector<int> read_int_file(const char* path) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f.is_open()) fail(BRIG_E_INVALID, std::string("cannot open ") + path);
+    const std::streamsize bytes = f.tellg();
+    std::vector<int> v((size_t)(bytes / 4));
+    f.seekg(0);
+    f.read(reinterpret_cast<char*>(v.data()), (std::streamsize)(v.size() * 4));
+    return v;
+}
+
+}  // namespace
+}  // namespace brig
+
+BloomFilter::BloomFilter(size_t bits, int hashes) : d_filter(nullptr), h_filter(nullptr), num_bits(bits),
+                                                    num_words(0), num_hashes(hashes) {
+    num_bits = (num_bits + 255) / 256 * 256;  // whole 256-bit blocks (src/bloom.cu:428-431)
+    if (num_bits == 0) num_bits = 256;
+    num_words = num_bits / 32;
+    h_filter = new uint32_t[num_words]();
+    if (cudaMalloc(&d_filter, num_words * 4) != cudaSuccess || cudaMemset(d_filter, 0, num_words * 4) != cudaSuccess) {
+        fprintf(stderr, "[brig compat] BloomFilter: device allocation of %zu bytes failed\n", num_words * 4);
+        d_filter = nullptr;
+    }
+}
+
+BloomFilter::~BloomFilter() {
+    delete[] h_filter;
+    if (d_filter) cudaFree(d_filter);
+}
+
+void BloomFilter::buildFromTable(int* gpu_data, size_t num_elements) {
+    if (!d_filter || num_elements == 0) return;
+    brig::k_refbf_insert<<<1184, 256>>>(d_filter, gpu_data, (int64_t)num_elements, num_hashes, num_bits / 256);
+    brig::note_launches(1);
+    const cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) fprintf(stderr, "[brig compat] BloomFilter::buildFromTable: %s\n", cudaGetErrorString(e));
+}
+
+long long BloomFilter::query(const int* gpu_data, size_t num_elements, unsigned char* results) {
+    if (!d_filter || num_elements == 0) return 0;
+    unsigned long long* d_passed = nullptr;
+    if (cudaMalloc(&d_passed, 8) != cudaSuccess) return -1;
+    cudaMemset(d_passed, 0, 8);
+    brig::k_refbf_query<<<1184, 256>>>(d_filter, gpu_data, (int64_t)num_elements, num_hashes, num_bits / 256, results,
+                                        d_passed);
+    brig::note_launches(1);
+    unsigned long long passed = 0;
+    const cudaError_t e = cudaMemcpy(&passed, d_passed, 8, cudaMemcpyDeviceToHost);
+    cudaFree(d_passed);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "[brig compat] BloomFilter::query: %s\n", cudaGetErrorString(e));
+        return -1;
+    }
+    return (long long)passed;
+}
+
+void BloomFilter::queryFromTable(int* gpu_data, size_t num_elements) {
+    const long long passed = query(gpu_data, num_elements, nullptr);
+    printf("[BloomFilter] %lld of %zu keys pass\n", passed, num_elements);
+}
+
+void BloomFilter::printStats() {
+    if (!d_filter) return;
+    if (cudaMemcpy(h_filter, d_filter, num_words * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    size_t set = 0;
+    for (size_t i = 0; i < num_words; ++i) set += (size_t)__builtin_popcount(h_filter[i]);
+    printf("[BloomFilter] bits: %zu, hash functions: %d, memory: %.2f MB, bits set: %.4f\n", num_bits, num_hashes,
+           (double)num_words * 4 / (1024.0 * 1024.0), (double)set / (double)num_bits);
+}
+
+void BloomFilter::verifyNoFalseNegatives(const char* build_file, const char* query_file) {
+    try {
+        const std::vector<int> b = brig::read_int_file(build_file), q = brig::read_int_file(query_file);
+        int* d_q = nullptr;
+        unsigned char* d_res = nullptr;
+        brig::cuda_check(cudaMalloc(&d_q, std::max<size_t>(q.size(), 1) * 4), "cudaMalloc");
+        brig::cuda_check(cudaMalloc(&d_res, std::max<size_t>(q.size(), 1)), "cudaMalloc");
+        brig::cuda_check(cudaMemcpy(d_q, q.data(), q.size() * 4, cudaMemcpyHostToDevice), "H2D");
+        query(d_q, q.size(), d_res);
+        std::vector<unsigned char> res(q.size());
+        brig::cuda_check(cudaMemcpy(res.data(), d_res, res.size(), cudaMemcpyDeviceToHost), "D2H");
+        cudaFree(d_q);
+        cudaFree(d_res);
+        std::vector<int> sorted(b);
+        std::sort(sorted.begin(), sorted.end());
+        long long members = 0, false_neg = 0, passed = 0;
+        for (size_t i = 0; i < q.size(); ++i) {
+            const bool in = std::binary_search(sorted.begin(), sorted.end(), q[i]);
+            members += in;
+            passed += res[i];
+            false_neg += in && !res[i];
+        }
+        printf("[BloomFilter] verify: %zu queries, %lld members, %lld pass, %lld false negatives\n", q.size(), members,
+               passed, false_neg);
+    } catch (const brig::Error& e) {
+        brig::report(e, "BloomFilter::verifyNoFalseNegatives");
+    }
+}
+
+// ---- join_execute_host (src/join_executor.h:87-88) -------------------------------------------------
+void join_execute_host(JoinChunkContext& ctx, int* effective_s_ptr, int* effective_s_val, long long) {
+    if (ctx.device_num > 1 || ctx.kernel_fusion == 2)
+        fprintf(stderr, "[brig compat] join_execute_host: one GPU: the cross-GPU transfer and probe have no effect\n");
+    const auto t0 = std::chrono::steady_clock::now();
+    int n = 0;
+    partial_jointable_gpu_run_only_s(ctx.GPUA_split, effective_s_ptr, ctx.GPUA_val_split, effective_s_val,
+                                     ctx.GPU_block_index_split_R,
+                                     ctx.GPU_block_index_split_S ? ctx.GPU_block_index_split_S[ctx.me] : nullptr,
+                                     ctx.GPU_second_index_split_R,
+                                     ctx.GPU_second_index_split_S ? ctx.GPU_second_index_split_S[ctx.me] : nullptr,
+                                     ctx.GPU_answer, ctx.GPU_answer_val, ctx.GPU_answer_s_val, ctx.GPU_answer_num,
+                                     ctx.max_int_number_for_shared_memory, &n, ctx.gpu_stream, ctx.gpu_event,
+                                     ctx.GPU_answer_write_idx);
+    if (ctx.first_pass_probe_sec)
+        *ctx.first_pass_probe_sec += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (ctx.answer_num_host) ctx.answer_num_host[0] = n;
+    if (ctx.total_answer_num) *ctx.total_answer_num += n;
+    // the engine probes oversized partitions exactly: no overflow blocks to report
 }

@@ -14,6 +14,8 @@
 #ifndef BRIG_JOIN_COMPAT_H_
 #define BRIG_JOIN_COMPAT_H_
 
+#include <cstddef>
+#include <cstdint>
 #include <cuda_runtime.h>
 #include <string>
 #include <vector>
@@ -103,5 +105,141 @@ void partial_jointable_gpu_run_only_s(const int* const d_adata, const int* const
 
 /* Pair capacity used by partial_jointable_gpu_run_only_s (total over appended calls). */
 void brig_compat_set_answer_capacity(long long capacity);
+
+/* ---- Bloom filter object (src/bloom.cuh:8-36) ------------------------------------------------
+ * The reference's global filter with its members and bit layout, so a filter built here can be
+ * queried by code written against the reference and the other way round: the bit count is rounded
+ * up to a multiple of 256; a key v lives in block hash(v, 1) % (bits / 256) of eight 32-bit words
+ * and sets bit hash(v, i + 1) % 256 of that block for i < num_hashes, with hash the reference's
+ * seeded MurmurHash3-style finaliser (src/bloom.cu:24-31). The device buffer comes from cudaMalloc
+ * instead of nvshmem_malloc (one GPU). The engine's own join uses its partitioned filter instead;
+ * this object serves callers of the reference's interface. */
+class BloomFilter {
+private:
+    uint32_t* d_filter;
+    uint32_t* h_filter;
+    size_t num_bits;
+    size_t num_words;
+    int num_hashes;
+
+public:
+    BloomFilter(size_t bits, int hashes);
+    ~BloomFilter();
+    BloomFilter(const BloomFilter&) = delete;
+    BloomFilter& operator=(const BloomFilter&) = delete;
+
+    /* Inserts every key of a device array (src/bloom.cu:460-492). */
+    void buildFromTable(int* gpu_data, size_t num_elements);
+    /* Queries every key of a device array and prints how many pass (declared at
+     * src/bloom.cuh:21). */
+    void queryFromTable(int* gpu_data, size_t num_elements);
+    /* Prints the size, the number of hashes and the fraction of set bits (src/bloom.cuh:22). */
+    void printStats();
+    /* Builds nothing: reads the int32 keys of both files, queries the query file's keys and
+     * reports the keys of the build file among them that the filter rejects (must be none;
+     * src/bloom.cuh:23). */
+    void verifyNoFalseNegatives(const char* build_file, const char* query_file);
+
+    uint32_t* getDeviceFilter() const { return d_filter; }
+    size_t getNumWords() const { return num_words; }
+    size_t getNumBits() const { return num_bits; }
+    int getNumHashes() const { return num_hashes; }
+
+    /* Device query: writes 1 or 0 per key into results (device bytes) and returns the number of
+     * keys that pass. Not in the reference's header; the engine's tests use it. */
+    long long query(const int* gpu_data, size_t num_elements, unsigned char* results);
+};
+
+/* ---- Probe executor (src/join_executor.h:10-88) -----------------------------------------------
+ * The reference's per-chunk context, field for field. At one PE join_execute_host reads R's
+ * partitioned arrays and indexes (GPUA_split, GPUA_val_split, GPU_block_index_split_R,
+ * GPU_second_index_split_R), S's indexes for this PE (GPU_block_index_split_S[me],
+ * GPU_second_index_split_S[me]) with S's partitioned arrays passed as effective_s_ptr /
+ * effective_s_val, the pair buffers and counters (GPU_answer*, answer_num_host), gpu_stream and the
+ * accumulators total_answer_num, total_overflow_count and first_pass_probe_sec. The transfer and
+ * timing fields of the multi-GPU modes are accepted and left alone. */
+struct JoinChunkContext {
+    int me;
+    int device_num;
+
+    int  use_bf;
+    bool use_nvlink;
+    int  kernel_fusion;
+    bool fused_probe_breakdown;
+
+    int*   GPUA_split;
+    int*   GPUB_send_buffer;
+    int*   GPU_buffer;
+    int*   h_pcie_stage;
+    int*   GPUA_val_split;
+    int*   GPUB_send_buffer_val;
+    int*   GPU_buffer_val;
+    int*   h_pcie_stage_val;
+    int2*  GPUB_send_buffer_kv;
+
+    int*       GPU_OB_split;
+    int*       GPU_OB_val_split;
+    long long* GPU_B_prefix_split;
+    long long* GPU_B_offset;
+
+    long long*  GPU_block_index_split_R;
+    long long** GPU_block_index_split_S;
+    long long*  GPU_second_index_split_R;
+    long long** GPU_second_index_split_S;
+
+    int* GPU_answer;
+    int* GPU_answer_val;
+    int* GPU_answer_s_val;
+    int* GPU_answer_num;
+    int* GPU_answer_write_idx;
+    int* answer_num_host;
+
+    std::vector<BloomFilter>* bf;
+    size_t    bf_words;
+    uint32_t* d_bf_global;
+
+    cudaStream_t gpu_stream;
+    cudaEvent_t  gpu_event;
+    cudaStream_t send_stream;
+
+    int max_int_number_for_shared_memory;
+
+    double* first_pass_probe_sec;
+    double* cumulative_bf_exchange_sec;
+    double* cumulative_bf_pipeline_sec;
+    double* cumulative_pre_send_barrier_sec;
+    double* cumulative_inner_barrier_sec;
+    double* cumulative_transfer_sec;
+    double* cumulative_second_pass_sec;
+    double* cumulative_fused_ht_sec;
+    double* cumulative_fused_local_sec;
+    double* cumulative_fused_get_sec;
+    double* cumulative_fused_remote_probe_sec;
+    double* cumulative_fused_wall_sec;
+    double* cumulative_fused_setup_sec;
+
+    double* cumulative_fp_preamble_sec;
+    double* cumulative_fp_memset_sec;
+    double* cumulative_fp_initbar_sec;
+    double* cumulative_fp_build_sec;
+    double* cumulative_fp_local_sec;
+    double* cumulative_fp_reduce_sec;
+
+    long long** d_s_block_ptrs;
+    long long** d_s_second_ptrs;
+    long long*  d_phase_timers;
+    long long   d_phase_timers_slots;
+
+    int*    total_answer_num;
+    int*    total_overflow_count;
+};
+
+/* The local probe of one S chunk (src/join_executor.h:87-88): the engine's task builder and
+ * persistent probe over the caller's partitioned R and S, pairs appended at *GPU_answer_write_idx
+ * up to the capacity of brig_compat_set_answer_capacity, the chunk's count into GPU_answer_num,
+ * answer_num_host[0] and added to *total_answer_num. Synchronous, as the reference. The engine has
+ * no overflow blocks (oversized partitions are probed exactly), so *total_overflow_count gains 0;
+ * actual_b_size is the chunk's S size (informational: the indexes carry it). */
+void join_execute_host(JoinChunkContext& ctx, int* effective_s_ptr, int* effective_s_val, long long actual_b_size);
 
 #endif /* BRIG_JOIN_COMPAT_H_ */

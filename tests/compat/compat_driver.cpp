@@ -3,6 +3,11 @@
 //   compat_driver gpu_main R.bin S.bin R S use_bf            -> prints the reference's total line
 //   compat_driver parts    R.bin S.bin R S P1 P2 pairs.bin    -> partition R and S, check the
 //                                                                reference layout, probe, dump pairs
+//   compat_driver exec     R.bin S.bin R S P1 P2 pairs.bin    -> the same probe through
+//                                                                join_execute_host and a JoinChunkContext
+//   compat_driver bloom    R.bin S.bin R S bits hashes        -> BloomFilter built from R's keys:
+//                                                                every bit where the reference puts it
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -50,6 +55,51 @@ static bool check_layout(const std::vector<int>& keys, const std::vector<long lo
     return start == (long long)keys.size();
 }
 
+// The reference's Bloom hash and bit placement (src/bloom.cu:24-31,153-190), restated on the host:
+// block hash(v, 1) % blocks, bit hash(v, i + 1) % 256 of the block for i < k.
+static uint32_t ref_hash(int v, uint32_t seed) {
+    uint32_t h = seed ^ (uint32_t)v;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// Builds a BloomFilter from R's keys on the device and checks its words against the host
+// restatement bit for bit, then that every R key passes and the S keys that pass on the device are
+// exactly those that pass on the host.
+static int bloom_check(const char* rf, const char* sf, long long R, long long S, long long bits, int k) {
+    std::vector<int> rk = read_keys(rf, R), sk = read_keys(sf, S);
+    int *dr = dev(rk), *ds = dev(sk);
+    BloomFilter bf((size_t)bits, k);
+    bf.buildFromTable(dr, (size_t)R);
+    const size_t words = bf.getNumWords(), blocks = bf.getNumBits() / 256;
+    std::vector<uint32_t> got = host(bf.getDeviceFilter(), words), want(words, 0u);
+    for (long long i = 0; i < R; ++i) {
+        const size_t b = ref_hash(rk[i], 1u) % blocks;
+        for (int j = 0; j < k; ++j) {
+            const uint32_t pos = ref_hash(rk[i], (uint32_t)j + 1u) % 256u;
+            want[b * 8 + pos / 32] |= 1u << (pos % 32);
+        }
+    }
+    const bool same = got == want;
+    long long host_pass = 0;
+    for (long long i = 0; i < S; ++i) {
+        const size_t b = ref_hash(sk[i], 1u) % blocks;
+        bool ok = true;
+        for (int j = 0; j < k; ++j) {
+            const uint32_t pos = ref_hash(sk[i], (uint32_t)j + 1u) % 256u;
+            ok = ok && (want[b * 8 + pos / 32] >> (pos % 32) & 1u);
+        }
+        host_pass += ok;
+    }
+    const long long r_pass = bf.query(dr, (size_t)R, nullptr), s_pass = bf.query(ds, (size_t)S, nullptr);
+    printf("BLOOM words %zu same %d r_pass %lld s_pass %lld host_s_pass %lld\n", words, same ? 1 : 0, r_pass, s_pass,
+           host_pass);
+    return (same && r_pass == R && s_pass == host_pass) ? 0 : 1;
+}
+
 int main(int argc, char** argv) {
     if (argc < 6) return 2;
     const std::string mode = argv[1];
@@ -58,6 +108,7 @@ int main(int argc, char** argv) {
         gpu_main(nullptr, nullptr, argv[2], argv[3], R, S, atoi(argv[6]), false, false, 0.1, 2);
         return 0;
     }
+    if (mode == "bloom") return bloom_check(argv[2], argv[3], R, S, atoll(argv[6]), atoi(argv[7]));
     const int P1 = atoi(argv[6]), P2 = atoi(argv[7]);
     partition_size = P1;
     second_partition_size = P2;
@@ -83,8 +134,42 @@ int main(int argc, char** argv) {
     int *ans = dev(std::vector<int>(cap)), *ansv = dev(std::vector<int>(cap)), *anss = dev(std::vector<int>(cap));
     brig_compat_set_answer_capacity(cap);
     int count = -1;
-    partial_jointable_gpu_run_only_s(da, db, dav, dbv, br, bs, sr, ss, ans, ansv, anss, dnum, 10008, &count, 0, nullptr,
-                                     widx);
+    if (mode == "exec") {
+        // one PE: R and S partitioned in place above, their indexes in the context
+        JoinChunkContext ctx;
+        std::memset(&ctx, 0, sizeof(ctx));
+        long long* s_block[1] = {bs};
+        long long* s_second[1] = {ss};
+        int host_num = 0, total = 0, overflow = 0;
+        double probe_sec = 0.0;
+        ctx.me = 0;
+        ctx.device_num = 1;
+        ctx.use_bf = 10;
+        ctx.kernel_fusion = 1;
+        ctx.GPUA_split = da;
+        ctx.GPUA_val_split = dav;
+        ctx.GPU_block_index_split_R = br;
+        ctx.GPU_block_index_split_S = s_block;
+        ctx.GPU_second_index_split_R = sr;
+        ctx.GPU_second_index_split_S = s_second;
+        ctx.GPU_answer = ans;
+        ctx.GPU_answer_val = ansv;
+        ctx.GPU_answer_s_val = anss;
+        ctx.GPU_answer_num = dnum;
+        ctx.GPU_answer_write_idx = widx;
+        ctx.answer_num_host = &host_num;
+        ctx.max_int_number_for_shared_memory = 10008;
+        ctx.first_pass_probe_sec = &probe_sec;
+        ctx.total_answer_num = &total;
+        ctx.total_overflow_count = &overflow;
+        join_execute_host(ctx, db, dbv, S);
+        count = total;
+        printf("EXEC host_num %d overflow %d\n", host_num, overflow);
+        if (host_num != total || overflow != 0) return 1;
+    } else {
+        partial_jointable_gpu_run_only_s(da, db, dav, dbv, br, bs, sr, ss, ans, ansv, anss, dnum, 10008, &count, 0,
+                                         nullptr, widx);
+    }
     printf("COUNT %d\n", count);
     std::vector<int> a = host(ansv, count > 0 ? count : 0), b = host(anss, count > 0 ? count : 0);
     FILE* f = fopen(argv[8], "wb");
