@@ -245,13 +245,14 @@ def batch_shapes(n_joins, seed, lo=4096, hi=1 << 24):
     return [(int(r), int(4 * r)) for r in nr]
 
 
-def run_batch_workload(args):
+def batch_measure(joins, steps, warmup):
     """256 independent joins, S = 10% Zipf(1.0) matches over R's row order: one batched pipeline
-    (autotuned, CUDA-graph replayed) against 256 sequential single-join calls."""
+    (autotuned, CUDA-graph replayed) against one single-join call per join. Returns the result dict;
+    the batched and sequential pairs of every join are compared as sorted multisets."""
     import torch
     import brig_join as bj
     torch.cuda.set_device(0)
-    shapes = batch_shapes(args.joins, 7)
+    shapes = batch_shapes(joins, 7)
     tot_r = sum(r for r, _ in shapes)
     tot_s = sum(s for _, s in shapes)
     i32 = torch.int32
@@ -262,40 +263,66 @@ def run_batch_workload(args):
     out_s = torch.empty(sum(caps), dtype=i32, device="cuda")
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
-    items, ro, so, oo = [], 0, 0, 0
+    items, ro, so, oo, offs = [], 0, 0, 0, []
     for j, (nr, ns) in enumerate(shapes):
         v = [big[0][ro:ro + nr], big[1][ro:ro + nr], big[2][so:so + ns], big[3][so:so + ns]]
         bj.gen_device(1000 + j, nr, ns, 0.1, 1.0, *v, stream=sp)
         items.append(dict(r_key=v[0], r_val=v[1], n_r=nr, s_key=v[2], s_val=v[3], n_s=ns,
                           out_r=out_r[oo:oo + caps[j]], out_s=out_s[oo:oo + caps[j]], capacity=caps[j]))
+        offs.append(oo)
         ro += nr; so += ns; oo += caps[j]
     torch.cuda.synchronize()
     tuples = tot_r + tot_s
 
-    def timed(fn, steps):
+    def timed(fn, n):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
-        for _ in range(steps):
+        for _ in range(n):
             fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
+        return e0.elapsed_time(e1) / n
+
+    def sorted_pairs(counts):
+        # every join's (r_val, s_val) pairs as one sorted int64 tensor per join
+        res = []
+        for j, c in enumerate(counts):
+            a = out_r[offs[j]:offs[j] + int(c)].to(torch.int64) & 0xffffffff
+            b = out_s[offs[j]:offs[j] + int(c)].to(torch.int64) & 0xffffffff
+            res.append(torch.sort((a << 32) | b).values)
+        return res
 
     # batched: autotune once (outside the timed region), then graph replays
     jb = bj.Join(use_cuda_graph=1)
+    t0 = time.time()
     tuned = jb.autotune(items, stream=sp)
-    for _ in range(args.warmup):
+    tune_s = time.time() - t0
+    for _ in range(max(warmup, 1)):
         jb.run_batch(items, stream=sp)
     counts = jb.batch_counts(len(items))
     assert list(counts) == ms, "batched counts differ from the constructed match counts"
+    batched_pairs = sorted_pairs(counts)
     launches0 = bj.kernel_launches()
     with ClockSampler(0) as clk:
-        ms_batch = timed(lambda: jb.run_batch(items, stream=sp), args.steps)
+        ms_batch = timed(lambda: jb.run_batch(items, stream=sp), steps)
     launches = bj.kernel_launches() - launches0
     jb.batch_counts(len(items))
+    # per-stage device times of the tuned configuration (a profiled handle launches directly)
+    cfg = dict(tuned)
+    cfg = {k: v for k, v in cfg.items() if k in dict(bj.Config._fields_)}
+    with bj.Join(profile_stages=1, **cfg) as jp:
+        jp.run_batch(items, stream=sp)
+        jp.run_batch(items, stream=sp)
+        jp.batch_counts(len(items))
+        jp.stage_times()
+        jp.run_batch(items, stream=sp)
+        jp.batch_counts(len(items))
+        stages = jp.stage_times()
+    jb.close()
     # sequential: the same joins, one plain join call each
     js = bj.Join()
+
     def seq():
         for it in items:
             js.run(it["r_key"], it["r_val"], it["n_r"], it["s_key"], it["s_val"], it["n_s"], it["out_r"], it["out_s"],
@@ -307,18 +334,29 @@ def run_batch_workload(args):
                it["capacity"], stream=sp)
         seq_counts.append(js.stats().count)
     assert seq_counts == ms, "sequential counts differ"
-    ms_seq = timed(seq, max(1, args.steps // 4))
-    line = {
-        "metric": "batched join tuples/s (sum |R|+|S| over 256 joins / t)", "value": tuples / (ms_batch / 1e3),
-        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch,
+    seq_pairs = sorted_pairs(seq_counts)
+    identical = all(torch.equal(a, b) for a, b in zip(batched_pairs, seq_pairs))
+    del batched_pairs, seq_pairs
+    ms_seq = timed(seq, max(1, steps // 4))
+    js.close()
+    return {
+        "metric": "batched join tuples/s (sum |R|+|S| over %d joins / t)" % joins, "value": tuples / (ms_batch / 1e3),
+        "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": warmup, "ms_per_step": ms_batch,
         "higher_is_better": True, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"{args.joins} joins, |R| log-uniform [4K, 16M], |S| = 4|R|, 10% Zipf(1.0) matches",
-                   "total_r": tot_r, "total_s": tot_s, "autotuned": tuned, "graph": True},
+        "config": {"workload": f"{joins} joins, |R| log-uniform [4K, 16M], |S| = 4|R|, 10% Zipf(1.0) matches",
+                   "total_r": tot_r, "total_s": tot_s, "autotuned": tuned, "autotune_s": round(tune_s, 2),
+                   "graph": True},
+        "stage_ms": {k: round(v, 3) for k, v in stages.items()},
         "sequential": {"ms_per_batch": ms_seq, "value": tuples / (ms_seq / 1e3)},
         "speedup_vs_sequential": ms_seq / ms_batch, "gpu_launches": launches, "clocks": clk.summary(),
-        "identical_results": True,
+        "identical_results": identical,
+        "identical_results_check": "per join, the sorted (r_val, s_val) multisets of the batched and the "
+                                   "sequential runs compared on the device",
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_batch_workload(args):
+    print(json.dumps(batch_measure(args.joins, args.steps, args.warmup)), flush=True)
     return 0
 
 
@@ -371,9 +409,10 @@ def run_sweep_workload(args):
 
 
 # ---- served joins ---------------------------------------------------------------------------------
-def run_serve_workload(args):
+def serve_measure(pool_n, requests, rates, streams):
     """Poisson stream of join requests against a 120 GB budget: p50/p99 latency and aggregate
-    tuples/s per offered load, against one request at a time."""
+    tuples/s per offered load, continuous batching against one request at a time. Returns the
+    result dict; every request's count is checked against its constructed match count."""
     import numpy as np
     import threading
     import torch
@@ -381,7 +420,7 @@ def run_serve_workload(args):
     torch.cuda.set_device(0)
     rng = np.random.default_rng(11)
     pool = []
-    for i in range(args.pool):
+    for i in range(pool_n):
         nr = int(math.exp(rng.uniform(math.log(1 << 16), math.log(1 << 26))))
         ratio = int(rng.choice([1, 4, 16]))
         frac = float(rng.choice([0.01, 0.1, 0.5]))
@@ -390,7 +429,7 @@ def run_serve_workload(args):
         bj.gen_device(5000 + i, nr, ns, frac, 0.0, *t)
         pool.append((t, nr, ns, int(math.floor(frac * ns))))
     torch.cuda.synchronize()
-    seq = [int(x) for x in rng.integers(0, len(pool), args.requests)]
+    seq = [int(x) for x in rng.integers(0, len(pool), requests)]
 
     # pinned host outputs: the pairs come back by asynchronous copies, as a client that hands the
     # server page-locked buffers would receive them
@@ -398,7 +437,7 @@ def run_serve_workload(args):
                      for _ in range(2)) for i in range(len(pool))}
 
     def one_load(srv, rate):
-        lat, queue = [], []
+        lat, queue, phases = [], [], []
         gaps = np.random.default_rng(3).exponential(1.0 / rate, len(seq)) if rate > 0 else np.zeros(len(seq))
         tickets = []
         t0 = time.perf_counter()
@@ -423,12 +462,17 @@ def run_serve_workload(args):
             assert res.status == bj.BRIG_OK and res.count == pool[i][3]
             lat.append(res.submit_to_done_ms)
             queue.append(res.queue_ms)
+            phases.append((res.setup_ms, res.join_ms, res.wave))
             done += 1
         th.join()
         wall = time.perf_counter() - t0
         tuples = sum(pool[i][1] + pool[i][2] for i in seq)
+        worst = sorted(range(len(seq)), key=lambda k: -lat[k])[:3]
         return {"offered_req_per_s": rate, "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                "mean_queue_ms": float(np.mean(queue)), "tuples_per_s": tuples / wall, "wall_s": wall}
+                "mean_queue_ms": float(np.mean(queue)), "tuples_per_s": tuples / wall, "wall_s": wall,
+                "slowest": [{"ms": round(lat[k], 2), "queue_ms": round(queue[k], 2),
+                             "setup_ms": round(phases[k][0], 2), "join_ms": round(phases[k][1], 2),
+                             "wave": phases[k][2], "tuples": pool[seq[k]][1] + pool[seq[k]][2]} for k in worst]}
 
     def run_mode(streams, max_wave):
         # One long-running server per mode. A warm-up pass over the whole pool sizes every slot's
@@ -442,18 +486,21 @@ def run_serve_workload(args):
                     srv.poll(x)
             return [one_load(srv, r) for r in rates]
 
-    rates = [float(x) for x in args.rates.split(",")]
-    sweep = run_mode(args.streams, 16)
+    sweep = run_mode(streams, 16)
     base = run_mode(1, 1)
-    line = {
+    return {
         "metric": "served join tuples/s and p50/p99 latency", "value": max(x["tuples_per_s"] for x in sweep),
         "unit": UNIT, "n_gpus": 1, "dtype": "u32", "data": "synthetic", "higher_is_better": True,
-        "config": {"workload": f"{args.requests} Poisson requests from a pool of {len(pool)}: |R| log-uniform "
+        "config": {"workload": f"{requests} Poisson requests from a pool of {len(pool)}: |R| log-uniform "
                                "[64K, 64M], |S|/|R| in {1,4,16}, match in {1%,10%,50%}, budget 120 GB",
-                   "streams": args.streams, "max_wave": 16},
+                   "streams": streams, "max_wave": 16},
         "continuous_batching": sweep, "one_at_a_time": base,
     }
-    print(json.dumps(line), flush=True)
+
+
+def run_serve_workload(args):
+    rates = [float(x) for x in args.rates.split(",")]
+    print(json.dumps(serve_measure(args.pool, args.requests, rates, args.streams)), flush=True)
     return 0
 
 
@@ -471,6 +518,8 @@ def main():
     ap.add_argument("--streams", type=int, default=3, help="serve workload: concurrent waves")
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and served measurements that follow the join's")
     ap.add_argument("--bloom", type=int, default=None, help="override Bloom on/off")
     ap.add_argument("--bloom-level", type=int, default=0,
                     help="S pass that probes the filter (1 first, 2 second, 0 planner's choice)")
@@ -643,6 +692,33 @@ def main():
                          f"(count only) on {cores} host threads"}
         del hr, hs
 
+    # the batched and served forms on the same GPU, after the join's buffers are released
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        if e2e is not None:
+            del hk, ho_r, ho_s
+            if jh is not j:
+                jh.close()
+        j.close()
+        del rk, rv, sk, sv, out_r, out_s
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        b = batch_measure(args.joins, 10, 3)
+        extras["batch"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "speedup_vs_sequential",
+                                            "identical_results", "gpu_launches", "stage_ms")}
+        extras["batch"]["sequential_ms"] = b["sequential"]["ms_per_batch"]
+        extras["batch"]["workload"] = b["config"]["workload"]
+        extras["batch"]["autotuned"] = b["config"]["autotuned"]
+        torch.cuda.empty_cache()
+        sv_ = serve_measure(16, 48, [20.0, 640.0], 3)
+        extras["serve"] = {"workload": sv_["config"]["workload"],
+                           "continuous_batching": [{k: x[k] for k in ("offered_req_per_s", "p50_ms", "p99_ms",
+                                                                      "tuples_per_s")}
+                                                   for x in sv_["continuous_batching"]],
+                           "one_at_a_time": [{k: x[k] for k in ("offered_req_per_s", "p50_ms", "p99_ms",
+                                                                "tuples_per_s")}
+                                             for x in sv_["one_at_a_time"]]}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -663,6 +739,7 @@ def main():
             "matches": st.count, "s_survivors": st.s_survivors,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     j.close()
     if dist:

@@ -69,7 +69,8 @@ class Config(C.Structure):
         ("max_level1_bits", C.c_int32),
         ("s_chunks", C.c_int32),
         ("wait_poll_limit", C.c_int32),
-        ("reserved", C.c_int32 * 2),
+        ("partition_fill", C.c_int32),
+        ("slices_per_sm", C.c_int32),
     ]
 
 
@@ -114,7 +115,8 @@ class ServeConfig(C.Structure):
         ("streams", C.c_int32),
         ("max_queue", C.c_int32),
         ("max_wave_mtuples", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("large_mtuples", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -137,6 +139,8 @@ class ServeResult(C.Structure):
         ("count", C.c_int64),
         ("submit_to_done_ms", C.c_double),
         ("queue_ms", C.c_double),
+        ("setup_ms", C.c_double),
+        ("join_ms", C.c_double),
     ]
 
 
@@ -172,6 +176,7 @@ def lib() -> C.CDLL:
     L.brig_join_run_batch.argtypes = [vp, C.POINTER(BatchItem), C.c_int32, vp]
     L.brig_join_batch_counts.argtypes = [vp, _i64p, C.c_int32]
     L.brig_join_autotune.argtypes = [vp, C.POINTER(BatchItem), C.c_int32, vp, C.POINTER(Config)]
+    L.brig_join_autotune_candidates.argtypes = [C.POINTER(Config), C.POINTER(Config), C.c_int32, C.POINTER(C.c_int32)]
     L.brig_gen_device.argtypes = [C.c_uint64, C.c_int64, C.c_int64, C.c_double, C.c_double,
                                   vp, vp, vp, vp, vp]
     L.brig_gen_host.argtypes = [C.c_uint64, C.c_int64, C.c_int64, C.c_double, C.c_double,
@@ -223,6 +228,21 @@ def make_config(**kw) -> Config:
             raise KeyError(k)
         setattr(cfg, k, v)
     return cfg
+
+
+def autotune_candidates(**kw) -> list:
+    """The configurations brig_join_autotune may try from the configuration kw."""
+    base = make_config(**kw)
+    n = C.c_int32()
+    check(lib().brig_join_autotune_candidates(C.byref(base), None, 0, C.byref(n)), "autotune_candidates")
+    out = (Config * n.value)()
+    check(lib().brig_join_autotune_candidates(C.byref(base), out, n.value, C.byref(n)), "autotune_candidates")
+    return list(out)
+
+
+def config_dict(c: Config) -> dict:
+    """The fields of a Config as a dict (keyword arguments of make_config / Join)."""
+    return {name: getattr(c, name) for name, _ in Config._fields_ if name != "abi_version"}
 
 
 def plan(n_r: int, n_s: int, **kw):
@@ -332,7 +352,9 @@ class Join:
         return {"table_capacity": chosen.table_capacity, "max_level1_bits": chosen.max_level1_bits,
                 "use_bloom": chosen.use_bloom,
                 "bloom_bits_per_key": chosen.bloom_bits_per_key if chosen.use_bloom else 0.0,
-                "bloom_num_hashes": chosen.bloom_num_hashes if chosen.use_bloom else 0}
+                "bloom_num_hashes": chosen.bloom_num_hashes if chosen.use_bloom else 0,
+                "bloom_probe_level": chosen.bloom_probe_level if chosen.use_bloom else 0,
+                "partition_fill": chosen.partition_fill, "slices_per_sm": chosen.slices_per_sm}
 
     def batch_counts(self, n: int, allow_overflow=False) -> np.ndarray:
         c = np.zeros(n, np.int64)
@@ -344,9 +366,10 @@ class Join:
 class Server:
     """Served joins (brig_serve_*): submit host-array requests, poll tickets."""
 
-    def __init__(self, hbm_budget_bytes=0, max_wave=0, streams=0, max_queue=0, max_wave_mtuples=0, **join_cfg):
+    def __init__(self, hbm_budget_bytes=0, max_wave=0, streams=0, max_queue=0, max_wave_mtuples=0,
+                 large_mtuples=0, **join_cfg):
         self.cfg = make_config(**join_cfg)
-        self.scfg = ServeConfig(hbm_budget_bytes, max_wave, streams, max_queue, max_wave_mtuples)
+        self.scfg = ServeConfig(hbm_budget_bytes, max_wave, streams, max_queue, max_wave_mtuples, large_mtuples)
         h = C.c_void_p()
         check(lib().brig_serve_create(C.byref(self.cfg), C.byref(self.scfg), C.byref(h)), "brig_serve_create")
         self.h = h

@@ -288,6 +288,16 @@ int brig_join_autotune(brig_join_t* h, const brig_join_batch_item* items, int32_
     });
 }
 
+int brig_join_autotune_candidates(const brig_join_config* base, brig_join_config* out, int32_t max, int32_t* n) {
+    return guarded([&] {
+        if (!base || !n || (max > 0 && !out)) fail(BRIG_E_INVALID, "null argument");
+        const std::vector<brig_join_config> c = brig::autotune_candidates(*base);
+        for (int32_t i = 0; i < max && i < (int32_t)c.size(); ++i) out[i] = c[i];
+        *n = (int32_t)c.size();
+        return (int)BRIG_OK;
+    });
+}
+
 int brig_join_batch_counts(brig_join_t* h, int64_t* counts, int32_t n_items) {
     return guarded([&] {
         if (!h || !counts) fail(BRIG_E_INVALID, "null argument");

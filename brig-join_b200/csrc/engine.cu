@@ -40,7 +40,9 @@ JoinPlan plan_join(const brig_join_config& cfg, int64_t nr, int64_t ns) {
     p.nr = nr;
     p.ns = ns;
     const int T = cfg.table_capacity > 0 ? cfg.table_capacity : kDefaultTable;
-    const int64_t target = std::max<int64_t>(1, (int64_t)T * 3 / 4);  // R tuples per finest partition
+    if (cfg.partition_fill < 0 || cfg.partition_fill > 100) fail(BRIG_E_INVALID, "partition_fill must be in [0, 100]");
+    const int fill = cfg.partition_fill > 0 ? cfg.partition_fill : 75;
+    const int64_t target = std::max<int64_t>(1, (int64_t)T * fill / 100);  // R tuples per finest partition
     PartFn& f = p.pf;
     f.mode = cfg.partition_mode;
     if (f.mode == BRIG_PART_HASH) {
@@ -176,7 +178,9 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
     auto slice_class = [](const JoinPlan& p, int r) { return r == 0 ? 0 : (p.bloom && p.bloom_level == 1 ? 1 : 2); };
     for (int j = 0; j < nj; ++j)
         for (int r = 0; r < 2; ++r) class_tuples[slice_class(plans[j], r)] += r == 0 ? plans[j].nr : plans[j].ns;
-    const int64_t target = (int64_t)std::max(num_sms, 1) * (nj > 1 ? 16 : 4);
+    if (cfg.slices_per_sm < 0) fail(BRIG_E_INVALID, "slices_per_sm must be >= 0");
+    const int per_sm = cfg.slices_per_sm > 0 ? cfg.slices_per_sm : (nj > 1 ? 16 : 4);
+    const int64_t target = (int64_t)std::max(num_sms, 1) * per_sm;
     int64_t class_sl[3];
     for (int c = 0; c < 3; ++c) {
         int64_t sl = (class_tuples[c] + target - 1) / target;
@@ -734,54 +738,96 @@ void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use
     nj_ = nj;
 }
 
+std::vector<brig_join_config> autotune_candidates(const brig_join_config& base) {
+    std::vector<brig_join_config> out;
+    for (int dim = 0; dim < kTuneDims; ++dim)
+        for (int v = 0; v < tune_values(dim); ++v) out.push_back(tune_apply(base, dim, v));
+    return out;
+}
+
+int tune_values(int dim) {
+    static const int n[kTuneDims] = {4, 3, 4, 3, 3};
+    return (dim >= 0 && dim < kTuneDims) ? n[dim] : 0;
+}
+
+brig_join_config tune_apply(const brig_join_config& base, int dim, int v) {
+    brig_join_config c = base;
+    switch (dim) {
+        case 0: {  // Bloom prefilter: off; 8 bits/key (k = 6); 10 bits/key (k = 7), auto or second pass
+            static const int use[] = {0, 1, 1, 1}, k[] = {0, 6, 7, 7}, lvl[] = {0, 0, 0, 2};
+            static const double bpk[] = {0.0, 8.0, 10.0, 10.0};
+            c.use_bloom = use[v];
+            c.bloom_bits_per_key = use[v] ? bpk[v] : 10.0;
+            c.bloom_num_hashes = k[v];
+            c.bloom_num_bits = 0;
+            c.bloom_probe_level = lvl[v];
+            break;
+        }
+        case 1: {
+            static const int t[] = {1024, 2048, 4096};
+            c.table_capacity = t[v];
+            break;
+        }
+        case 2: {
+            static const int b[] = {7, 8, 9, 10};
+            c.max_level1_bits = b[v];
+            break;
+        }
+        case 3: {
+            static const int f[] = {50, 75, 100};
+            c.partition_fill = f[v];
+            break;
+        }
+        case 4: {
+            static const int w[] = {8, 16, 32};
+            c.slices_per_sm = w[v];
+            break;
+        }
+    }
+    return c;
+}
+
 brig_join_config Engine::autotune(const std::vector<JoinIO>& joins, cudaStream_t stream) {
-    // Candidates: shared-memory table capacity (build-chunk size, which also sets the partition
-    // count through the planner's fill target) x largest level-1 fan-out x Bloom prefilter (off, or
-    // 10 bits/key with 7 hashes; the filter changes only the speed, never the result). A caller's
-    // own Bloom setting is kept as the "on" candidate.
-    const int tables[] = {1024, 2048, 4096};
-    const int l1bits[] = {8, 9, 10};
-    struct BloomChoice {
-        int use;
-        double bpk;
-        int k;
-    };
-    const BloomChoice blooms[] = {
-        {0, 0.0, 0},
-        {1, cfg_.use_bloom && cfg_.bloom_bits_per_key > 0 ? cfg_.bloom_bits_per_key : 10.0,
-         cfg_.use_bloom && cfg_.bloom_num_hashes > 0 ? cfg_.bloom_num_hashes : 7}};
+    // Coordinate search: from the handle's configuration, each dimension in turn takes the value
+    // whose median time over three runs (after a warm-up run that also sizes the workspace) is
+    // lowest, the others held; passes repeat while one improves the time by more than 2%. No
+    // candidate changes a join's result, only its speed.
     const brig_join_config base = cfg_;
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
     cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
-    float best = -1.f;
+    auto time_cfg = [&](const brig_join_config& c) {
+        cfg_ = c;
+        cfg_.profile_stages = 0;
+        run(joins, stream, false);  // warm-up (sizes the workspace)
+        float t[3];
+        for (float& x : t) {
+            cuda_check(cudaEventRecord(e0, stream), "cudaEventRecord");
+            run(joins, stream, false);
+            cuda_check(cudaEventRecord(e1, stream), "cudaEventRecord");
+            cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
+            cuda_check(cudaEventElapsedTime(&x, e0, e1), "cudaEventElapsedTime");
+        }
+        std::sort(t, t + 3);
+        return t[1];
+    };
     brig_join_config best_cfg = base;
     try {
-        for (const BloomChoice& bc : blooms)
-        for (int t : tables) {
-            for (int b : l1bits) {
-                cfg_ = base;
-                cfg_.table_capacity = t;
-                cfg_.max_level1_bits = b;
-                cfg_.profile_stages = 0;
-                cfg_.use_bloom = bc.use;
-                if (bc.use) {
-                    cfg_.bloom_bits_per_key = bc.bpk;
-                    cfg_.bloom_num_hashes = bc.k;
-                    cfg_.bloom_num_bits = 0;
-                }
-                run(joins, stream, false);  // warm-up (sizes the workspace)
-                cuda_check(cudaEventRecord(e0, stream), "cudaEventRecord");
-                run(joins, stream, false);
-                cuda_check(cudaEventRecord(e1, stream), "cudaEventRecord");
-                cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
-                float ms = 0.f;
-                cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-                if (best < 0.f || ms < best) {
-                    best = ms;
-                    best_cfg = cfg_;
+        float best = time_cfg(best_cfg);
+        for (int pass = 0; pass < 3; ++pass) {
+            const float start = best;
+            for (int dim = 0; dim < kTuneDims; ++dim) {
+                for (int v = 0; v < tune_values(dim); ++v) {
+                    const brig_join_config c = tune_apply(best_cfg, dim, v);
+                    if (std::memcmp(&c, &best_cfg, sizeof(c)) == 0) continue;
+                    const float ms = time_cfg(c);
+                    if (ms < best) {
+                        best = ms;
+                        best_cfg = c;
+                    }
                 }
             }
+            if (best > start * 0.98f) break;
         }
     } catch (...) {
         cfg_ = base;

@@ -95,6 +95,13 @@ void layout_for(const brig_join_config& cfg, const JoinPlan* plans, int nj, int 
 void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const JoinIO* joins, int nj,
                    const Shape& sh, char* ws, char* meta_host, int num_sms, PipelineArgs& a);
 
+// The autotuner's search space (Engine::autotune): kTuneDims dimensions, each with tune_values(dim)
+// values; tune_apply(base, dim, v) is base with dimension dim set to its v-th value.
+constexpr int kTuneDims = 5;
+int tune_values(int dim);
+brig_join_config tune_apply(const brig_join_config& base, int dim, int v);
+std::vector<brig_join_config> autotune_candidates(const brig_join_config& base);
+
 class Engine {
 public:
     explicit Engine(const brig_join_config& cfg);

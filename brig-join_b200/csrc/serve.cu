@@ -9,7 +9,10 @@
 //      requests (up to max_wave) are admitted into one wave and launched on that slot: host inputs
 //      are copied in, the wave runs as one batched pipeline, results follow in step 1.
 // A request that arrives while other waves are on the GPU is admitted as soon as a slot and memory
-// are free, so its work overlaps the waves already running. Submit and poll are thread-safe.
+// are free, so its work overlaps the waves already running; large requests (above large_mtuples
+// tuples) run one at a time on slot 0 and small ones may pass them. Submit and poll are
+// thread-safe.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -30,7 +33,7 @@ struct Req {
     brig_serve_request in{};
     int64_t cap = 0;
     int64_t footprint = 0;
-    Clock::time_point t_submit, t_start;
+    Clock::time_point t_submit, t_start, t_enqueued, t_joined;
     // device buffers owned by the request (host-input copies and outputs)
     uint32_t *rk = nullptr, *rv = nullptr, *sk = nullptr, *sv = nullptr, *outr = nullptr, *outs = nullptr;
     int state = 0;  // 0 pending, 1 running, 2 done
@@ -125,12 +128,16 @@ struct Server {
         s.eng->reserve_workspace((size_t)s.ws_target, s.stream);
         s.eng->run(io, s.stream, false);
         cuda_check(cudaEventRecord(s.ev, s.stream), "cudaEventRecord");
+        const auto now = Clock::now();
+        for (Req* q : s.wave) q->t_enqueued = now;
         s.phase = 1;
     }
 
     // Slot s finished its join: copy pairs back (phase 1 -> 2) or finish requests (phase 2 -> 0).
     void advance(Slot& s) {
         if (s.phase == 1) {
+            const auto joined = Clock::now();
+            for (Req* q : s.wave) q->t_joined = joined;
             std::vector<int64_t> c;
             int64_t errors = 0;
             s.eng->sync_counters(c, errors);
@@ -156,6 +163,8 @@ struct Server {
             used -= io_bytes(q->in, q->cap);
             q->res.submit_to_done_ms = std::chrono::duration<double, std::milli>(now - q->t_submit).count();
             q->res.queue_ms = std::chrono::duration<double, std::milli>(q->t_start - q->t_submit).count();
+            q->res.setup_ms = std::chrono::duration<double, std::milli>(q->t_enqueued - q->t_start).count();
+            q->res.join_ms = std::chrono::duration<double, std::milli>(q->t_joined - q->t_enqueued).count();
             q->state = 2;
         }
         s.wave.clear();
@@ -181,52 +190,112 @@ struct Server {
                     fail_wave(s, BRIG_E_CUDA, cudaGetErrorString(q));
                 }
             }
-            // admission
-            for (auto& s : slots) {
+            // admission. A request above large_mtuples tuples is large: large requests run one at a
+            // time, each as a wave of its own, on slot 0, so two of them never share the GPU (which
+            // would slow both and set the tail latency); the other slots batch and overlap the
+            // small requests, which may pass a large one waiting for slot 0 instead of queueing
+            // behind it. Slot 0 also takes small waves while no large request waits. So slot 0's
+            // workspace grows to the largest request once (the warm-up), the others stay small,
+            // and no slot has to map fresh device memory for a request later.
+            for (size_t si = 0; si < slots.size(); ++si) {
+                Slot& s = slots[(si + 1) % slots.size()];  // small-request slots first, then slot 0
+                const bool large_slot = &s == &slots[0];
                 if (s.phase != 0) continue;
                 std::vector<Req*> wave;
+                bool more = false;  // requests still pending after this slot's turn
                 {
                     // Grow the wave while the budget holds: bytes in use (live request buffers and
                     // every slot's workspace) + this wave's request buffers + the growth of this
-                    // slot's workspace.
-                    // A wave also stops at max_wave_mtuples million tuples, so small requests
-                    // batch together while a large one runs alone and does not hold them back.
+                    // slot's workspace. A wave of small requests also stops at max_wave_mtuples
+                    // million tuples.
                     std::lock_guard<std::mutex> lk(mu);
                     const int64_t ws_have = s.eng->workspace_bytes();
                     const int64_t max_tuples = (int64_t)scfg.max_wave_mtuples * 1000000;
+                    const int64_t large_tuples = (int64_t)scfg.large_mtuples * 1000000;
+                    auto is_large = [&](const Req* q) { return q->in.n_r + q->in.n_s > large_tuples; };
                     int64_t io = 0, ws_new = ws_have, tuples = 0;
-                    while (!pending.empty() && (int)wave.size() < scfg.max_wave) {
-                        Req* q = pending.front();
-                        const int64_t t2 = tuples + q->in.n_r + q->in.n_s;
-                        if (!wave.empty() && t2 > max_tuples) break;
-                        wave.push_back(q);
-                        const int64_t io2 = io + io_bytes(q->in, q->cap);
-                        const int64_t ws2 = std::max(ws_have, wave_workspace(wave));
-                        if (used + io2 + (ws2 - ws_have) > scfg.hbm_budget_bytes) {
-                            wave.pop_back();
+                    auto fits = [&](const std::vector<Req*>& w, int64_t io2, int64_t& ws2) {
+                        ws2 = std::max(ws_have, wave_workspace(w));
+                        return used + io2 + (ws2 - ws_have) <= scfg.hbm_budget_bytes;
+                    };
+                    // slot 0: the oldest large request, alone
+                    if (large_slot) {
+                        for (auto it = pending.begin(); it != pending.end(); ++it) {
+                            if (!is_large(*it)) continue;
+                            wave.push_back(*it);
+                            int64_t ws2 = 0;
+                            const int64_t io2 = io_bytes((*it)->in, (*it)->cap);
+                            if (fits(wave, io2, ws2)) {
+                                io = io2;
+                                ws_new = ws2;
+                                tuples = (*it)->in.n_r + (*it)->in.n_s;
+                                pending.erase(it);
+                            } else {
+                                wave.clear();
+                            }
                             break;
                         }
-                        io = io2;
-                        ws_new = ws2;
-                        tuples = t2;
-                        pending.pop_front();
+                    }
+                    // otherwise small requests in arrival order, passing any large one
+                    const bool large_waiting =
+                        std::any_of(pending.begin(), pending.end(), [&](const Req* q) { return is_large(q); });
+                    if (wave.empty() && !(large_slot && large_waiting)) {
+                        for (auto it = pending.begin(); it != pending.end() && (int)wave.size() < scfg.max_wave;) {
+                            Req* q = *it;
+                            if (is_large(q)) {
+                                ++it;
+                                continue;
+                            }
+                            const int64_t t2 = tuples + q->in.n_r + q->in.n_s;
+                            if (!wave.empty() && t2 > max_tuples) break;
+                            wave.push_back(q);
+                            int64_t ws2 = 0;
+                            const int64_t io2 = io + io_bytes(q->in, q->cap);
+                            if (!fits(wave, io2, ws2)) {
+                                wave.pop_back();
+                                break;
+                            }
+                            io = io2;
+                            ws_new = ws2;
+                            tuples = t2;
+                            it = pending.erase(it);
+                        }
+                    }
+                    for (Req* q : wave) {
                         q->state = 1;
                         q->t_start = Clock::now();
                         q->res.wave = next_wave;
                     }
-                    // A slot that must grow grows to at least the largest workspace of any slot
-                    // (when the budget allows), so after a warm-up no slot grows again: growing
-                    // maps fresh device memory and blocks the scheduler for that long.
-                    if (!wave.empty() && ws_new > ws_have) {
+                    // A small-request slot that must grow grows to at least the largest workspace of
+                    // the small-request slots (when the budget allows), so after a warm-up none
+                    // grows again: growing maps fresh device memory and blocks the scheduler.
+                    if (!wave.empty() && ws_new > ws_have && !large_slot) {
                         int64_t widest = 0;
-                        for (const auto& o : slots) widest = std::max(widest, o.ws_target);
+                        for (size_t o = 1; o < slots.size(); ++o) widest = std::max(widest, slots[o].ws_target);
                         const int64_t room = scfg.hbm_budget_bytes - (used + io + (ws_new - ws_have));
                         if (widest > ws_new) ws_new += std::min(widest - ws_new, std::max<int64_t>(room, 0));
                     }
-                    used += io + (ws_new - ws_have);
-                    if (!wave.empty()) s.ws_target = ws_new;
+                    if (!wave.empty()) {
+                        used += io + (ws_new - ws_have);
+                        s.ws_target = ws_new;
+                        // the idle small-request slots grow with it (budget permitting), so that after
+                        // a warm-up no small-request slot grows for a request later
+                        if (!large_slot && ws_new > ws_have)
+                            for (size_t o = 1; o < slots.size(); ++o) {
+                                Slot& t = slots[o];
+                                if (&t == &s || t.phase != 0 || t.ws_target >= ws_new) continue;
+                                if (used + (ws_new - t.ws_target) > scfg.hbm_budget_bytes) continue;
+                                used += ws_new - t.ws_target;
+                                t.ws_target = ws_new;
+                                t.eng->reserve_workspace((size_t)ws_new, t.stream);
+                            }
+                    }
+                    more = !pending.empty();
                 }
-                if (wave.empty()) break;
+                if (wave.empty()) {
+                    if (!more) break;
+                    continue;  // what is pending waits for another slot (or for memory); try the next
+                }
                 s.wave = wave;
                 s.wave_id = next_wave++;
                 try {
@@ -305,6 +374,7 @@ int brig_serve_create(const brig_join_config* jcfg, const brig_serve_config* scf
         if (s->scfg.streams <= 0) s->scfg.streams = 2;
         if (s->scfg.max_queue <= 0) s->scfg.max_queue = 4096;
         if (s->scfg.max_wave_mtuples <= 0) s->scfg.max_wave_mtuples = 256;
+        if (s->scfg.large_mtuples <= 0) s->scfg.large_mtuples = s->scfg.max_wave_mtuples;
         try {
             if (jcfg->device >= 0) brig::cuda_check(cudaSetDevice(jcfg->device), "cudaSetDevice");
             brig::cuda_check(cudaGetDevice(&s->device), "cudaGetDevice");

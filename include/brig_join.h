@@ -93,7 +93,12 @@ typedef struct brig_join_config {
                                        default), -1 = none, so every such wait reports the error at
                                        once (a test of the error path; the results stay exact). The
                                        reference's waits are unbounded (src/join_executor.cu:49) */
-    int32_t reserved[2];
+    int32_t partition_fill;         /* build-side tuples the planner aims for per finest partition, in
+                                       percent of table_capacity (sets the level-2 fan-out; the
+                                       reference aims at 8000 of its 10007 slots,
+                                       src/hash_kernel.cu:240-284); 0 = 75 */
+    int32_t slices_per_sm;          /* level-1 slices per SM of each launch class (the CTA work unit
+                                       of the partition passes); 0 = 4 for one join, 16 for a batch */
 } brig_join_config;
 
 /* Output of one join. Pairs are written in an unspecified order; the multiset is exact. When the
@@ -205,13 +210,21 @@ int brig_join_run_batch(brig_join_t* h, const brig_join_batch_item* items, int32
  * BRIG_E_OVERFLOW if any join exceeded its capacity. */
 int brig_join_batch_counts(brig_join_t* h, int64_t* counts, int32_t n_items);
 
-/* Times candidate configurations (shared-memory table capacity x level-1 fan-out x Bloom
- * prefilter off or on) on the given batch and keeps the fastest in the handle; the chosen
- * configuration is copied to *chosen when not NULL. Runs the batch 2 x 18 times; results of those
- * runs are discarded (outputs are overwritten). The reference has no autotuner; its sizing is fixed heuristics
- * (src/hash_kernel.cu:198-284). */
+/* Tunes the handle's configuration on the given batch and keeps the fastest: a coordinate search,
+ * one dimension at a time from the handle's configuration, over the Bloom prefilter (off; 8 bits/key,
+ * k = 6; 10 bits/key, k = 7, probe level chosen by the planner or in S's second pass), the
+ * shared-memory table capacity, the largest level-1 radix bits, partition_fill (the level-2 fan-out)
+ * and slices_per_sm, each candidate timed as the median of three runs after a warm-up, repeated while
+ * a pass improves the time by more than 2% (at most three passes). The chosen configuration is copied
+ * to *chosen when not NULL. Results of the timing runs are discarded (outputs are overwritten); no
+ * candidate changes the result of a join, only its speed. The reference has no autotuner; its
+ * sizing is fixed heuristics (src/hash_kernel.cu:198-284). */
 int brig_join_autotune(brig_join_t* h, const brig_join_batch_item* items, int32_t n_items, void* stream,
                        brig_join_config* chosen);
+
+/* The configurations the autotuner may try from `base` (each dimension's values with the others at
+ * base): writes up to `max` of them to out and their number to *n. */
+int brig_join_autotune_candidates(const brig_join_config* base, brig_join_config* out, int32_t max, int32_t* n);
 
 /* ---- Served joins: continuous batching under an HBM budget ------------------------------------
  * No reference counterpart. Requests are admitted while their device footprint fits the budget;
@@ -224,7 +237,10 @@ typedef struct brig_serve_config {
     int32_t max_queue;         /* pending requests before submit rejects; 0 = 4096 */
     int32_t max_wave_mtuples;  /* a wave stops growing at this many million tuples (|R|+|S| summed);
                                   a larger request runs as a wave of its own; 0 = 256 */
-    int32_t reserved[4];
+    int32_t large_mtuples;     /* requests above this many million tuples are large: they run one at
+                                  a time (never two on the GPU together) on the first stream, and
+                                  smaller requests may pass one that waits; 0 = max_wave_mtuples */
+    int32_t reserved[3];
 } brig_serve_config;
 
 /* One request. Inputs are HOST arrays (copied in by the server) or device arrays when
@@ -246,6 +262,8 @@ typedef struct brig_serve_result {
     int64_t count;         /* exact match count */
     double  submit_to_done_ms;  /* latency: submit -> results available */
     double  queue_ms;           /* submit -> start of its wave */
+    double  setup_ms;           /* start of its wave -> the wave's work enqueued (buffers, workspace) */
+    double  join_ms;            /* work enqueued -> the join finished on the device */
 } brig_serve_result;
 
 typedef struct brig_serve_t brig_serve_t;

@@ -84,3 +84,52 @@ def test_batch_graph_replay_new_inputs(bj, oracle, torch_cuda):
                 assert c == len(er)
                 assert_same_pairs(oracle, o_r[:c].cpu().numpy().view(np.uint32),
                                   o_s[:c].cpu().numpy().view(np.uint32), er, es)
+
+
+def _skewed_cases(bj, oracle, n, seed):
+    rng = np.random.default_rng(seed)
+    cases, exps = [], []
+    for i in range(n):
+        nr = int(rng.integers(1000, 120_000))
+        ns = 4 * nr
+        rk, rv, sk, sv = bj.gen_host(seed * 100 + i, nr, ns, 0.1, zipf_s=1.0 if i % 2 else 0.0)
+        e = oracle.pairs(rk, rv, sk, sv)
+        exps.append(e)
+        cases.append((rk, rv, sk, sv, len(e[0])))
+    return cases, exps
+
+
+def test_every_autotune_candidate_gives_the_oracle_pairs(bj, oracle, torch_cuda):
+    """Each configuration the autotuner may pick (Bloom choice, table capacity, level-1 bits,
+    partition fill, slices per SM) joins an uneven, partly Zipf-skewed batch to exactly the oracle's
+    pairs: tuning changes the speed only."""
+    cases, exps = _skewed_cases(bj, oracle, 6, 3)
+    cands = bj.autotune_candidates(use_cuda_graph=1)
+    assert len(cands) == 17
+    for c in cands:
+        outs = _batch(bj, torch_cuda, cases, **bj.config_dict(c))
+        for (cnt, r, s), (er, es) in zip(outs, exps):
+            assert cnt == len(er)
+            assert_same_pairs(oracle, r, s, er, es)
+
+
+def test_autotune_keeps_a_candidate_and_the_batch_stays_exact(bj, oracle, torch_cuda):
+    cases, exps = _skewed_cases(bj, oracle, 8, 4)
+    items, keep = [], []
+    for rk, rv, sk, sv, cap in cases:
+        d = [dev(torch_cuda, a) for a in (rk, rv, sk, sv)]
+        o_r = torch_cuda.empty(max(cap, 1), dtype=torch_cuda.int32, device="cuda")
+        o_s = torch_cuda.empty(max(cap, 1), dtype=torch_cuda.int32, device="cuda")
+        keep.append((o_r, o_s))
+        items.append(dict(r_key=d[0], r_val=d[1], n_r=len(rk), s_key=d[2], s_val=d[3], n_s=len(sk),
+                          out_r=o_r, out_s=o_s, capacity=cap))
+        keep.append(d)
+    with bj.Join(use_cuda_graph=1) as j:
+        chosen = j.autotune(items)
+        # the handle's own defaults (0: automatic) stay when no candidate beats them
+        assert chosen["table_capacity"] in (0, 1024, 2048, 4096) and chosen["slices_per_sm"] in (0, 8, 16, 32)
+        j.run_batch(items)
+        counts = j.batch_counts(len(items))
+    for (o_r, o_s), c, (er, es) in zip(keep[0::2], counts, exps):
+        assert c == len(er)
+        assert_same_pairs(oracle, o_r[:c].cpu().numpy().view(np.uint32), o_s[:c].cpu().numpy().view(np.uint32), er, es)

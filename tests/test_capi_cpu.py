@@ -25,9 +25,12 @@ def test_config_defaults(bj):
     assert cfg.bloom_bits_per_key == 10.0 and cfg.use_bloom == 0 and cfg.device == -1
     assert cfg.s_chunks == 0  # S in one piece
     assert cfg.wait_poll_limit == 0  # default bound of the kernels' waits
-    assert C.sizeof(bj.Config) == 88  # layout of brig_join_config (s_chunks and wait_poll_limit took
-    assert bj.Config.s_chunks.offset == 72  # reserved slots)
-    assert bj.Config.wait_poll_limit.offset == 76 and bj.Config.reserved.offset == 80
+    assert cfg.partition_fill == 0 and cfg.slices_per_sm == 0
+    # layout of brig_join_config: s_chunks, wait_poll_limit, partition_fill and slices_per_sm took
+    # what were reserved slots, so the size is unchanged
+    assert C.sizeof(bj.Config) == 88
+    assert bj.Config.s_chunks.offset == 72 and bj.Config.wait_poll_limit.offset == 76
+    assert bj.Config.partition_fill.offset == 80 and bj.Config.slices_per_sm.offset == 84
 
 
 @pytest.mark.parametrize("n_r,n_s,kw,expect", [
@@ -134,3 +137,30 @@ def test_compat_symbols_exported(bj):
         assert name in out, name
     for g in ["partition_size", "second_partition_size", "thread_no", "block_no", "chunk_size"]:
         assert any(line.split()[-1] == g for line in out.splitlines() if line.strip()), g
+
+
+def test_autotune_candidates_vary_one_dimension_each(bj):
+    """The autotuner's search space: every candidate differs from the base in one tuned field."""
+    base = bj.make_config(use_bloom=1)
+    cands = bj.autotune_candidates(use_bloom=1)
+    assert len(cands) == 4 + 3 + 4 + 3 + 3
+    tuned = {"use_bloom", "bloom_bits_per_key", "bloom_num_hashes", "bloom_num_bits", "bloom_probe_level",
+             "table_capacity", "max_level1_bits", "partition_fill", "slices_per_sm"}
+    for c in cands:
+        for name, _ in bj.Config._fields_:
+            if name not in tuned:
+                assert getattr(c, name) == getattr(base, name), name
+    assert {c.table_capacity for c in cands} >= {1024, 2048, 4096}
+    assert {c.max_level1_bits for c in cands} >= {7, 8, 9, 10}
+    assert {c.partition_fill for c in cands} >= {50, 75, 100}
+    assert {c.slices_per_sm for c in cands} >= {8, 16, 32}
+    assert {(c.use_bloom, c.bloom_num_hashes) for c in cands} >= {(0, 0), (1, 6), (1, 7)}
+
+
+def test_planner_partition_fill_and_slices(bj):
+    """partition_fill sets the level-2 fan-out through the per-partition target."""
+    p_default = bj.plan(1 << 26, 1 << 26)  # 75%: 3072 of 4096 per finest partition -> 2^15 partitions
+    p_full = bj.plan(1 << 26, 1 << 26, partition_fill=100)  # 4096 -> 2^14
+    assert p_full[0] == p_default[0] and 2 * p_full[1] == p_default[1]
+    with pytest.raises(bj.BrigError):
+        bj.plan(1 << 20, 1 << 20, partition_fill=101)

@@ -104,3 +104,29 @@ def test_poll_timeout_and_unknown_ticket(bj, torch_cuda):
         t = srv.submit(*_req(bj, 3, 10_000, 1, 0.1))
         res, _, _ = srv.poll(t, 10_000)
         assert res.status == bj.BRIG_OK
+
+
+def test_large_requests_run_one_at_a_time_and_small_ones_pass_them(bj, oracle, torch_cuda):
+    """Requests above large_mtuples run one at a time on the first stream: no two of them are on the
+    GPU together (each starts after the previous one's join has finished), while the small requests
+    submitted behind them start without waiting for them; every result is exact."""
+    reqs = []
+    for i in range(9):
+        big = i % 3 == 0
+        nr, ns = (400_000, 900_000) if big else (20_000, 30_000)
+        reqs.append((big, bj.gen_host(800 + i, nr, ns, 0.2)))
+    exps = [oracle.pairs(*r) for _, r in reqs]
+    with bj.Server(hbm_budget_bytes=8 << 30, max_wave=4, streams=3, large_mtuples=1) as srv:
+        tickets = [srv.submit(*r, capacity=len(e[0]) + 8) for (_, r), e in zip(reqs, exps)]
+        results = [srv.poll(t) for t in tickets]
+    spans = []
+    for (big, r), (er, es), (res, a, b) in zip(reqs, exps, results):
+        assert res.status == bj.BRIG_OK and res.count == len(er)
+        assert_same_pairs(oracle, a, b, er, es)
+        if big:
+            spans.append((res.queue_ms, res.queue_ms + res.setup_ms + res.join_ms))
+    spans.sort()
+    for (s0, e0), (s1, e1) in zip(spans, spans[1:]):
+        assert s1 >= e0 - 0.05, spans  # the next large request started after the previous one's join
+    smalls = [res.queue_ms for (big, _), (res, _, _) in zip(reqs, results) if not big]
+    assert min(smalls) < spans[-1][0], (smalls, spans)  # some small request did not wait for the last large one
