@@ -245,7 +245,7 @@ def batch_shapes(n_joins, seed, lo=4096, hi=1 << 24):
     return [(int(r), int(4 * r)) for r in nr]
 
 
-def batch_measure(joins, steps, warmup):
+def batch_measure(joins, steps, warmup, fixed_cfg=None):
     """256 independent joins, S = 10% Zipf(1.0) matches over R's row order: one batched pipeline
     (autotuned, CUDA-graph replayed) against one single-join call per join. Returns the result dict;
     the batched and sequential pairs of every join are compared as sorted multisets."""
@@ -294,10 +294,14 @@ def batch_measure(joins, steps, warmup):
         return res
 
     # batched: autotune once (outside the timed region), then graph replays
-    jb = bj.Join(use_cuda_graph=1)
-    t0 = time.time()
-    tuned = jb.autotune(items, stream=sp)
-    tune_s = time.time() - t0
+    if fixed_cfg:
+        jb = bj.Join(use_cuda_graph=1, **fixed_cfg)
+        tuned, tune_s = dict(fixed_cfg), 0.0
+    else:
+        jb = bj.Join(use_cuda_graph=1)
+        t0 = time.time()
+        tuned = jb.autotune(items, stream=sp)
+        tune_s = time.time() - t0
     for _ in range(max(warmup, 1)):
         jb.run_batch(items, stream=sp)
     counts = jb.batch_counts(len(items))
@@ -356,7 +360,8 @@ def batch_measure(joins, steps, warmup):
 
 
 def run_batch_workload(args):
-    print(json.dumps(batch_measure(args.joins, args.steps, args.warmup)), flush=True)
+    fixed = json.loads(args.batch_config) if args.batch_config else None
+    print(json.dumps(batch_measure(args.joins, args.steps, args.warmup, fixed)), flush=True)
     return 0
 
 
@@ -512,6 +517,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["batch", "serve", "sweep"])
     ap.add_argument("--joins", type=int, default=256, help="batch workload: number of joins")
+    ap.add_argument("--batch-config", default="",
+                    help="batch workload: a JSON object of configuration fields to use instead of autotuning")
     ap.add_argument("--pool", type=int, default=24, help="serve workload: distinct requests")
     ap.add_argument("--requests", type=int, default=64, help="serve workload: requests per load point")
     ap.add_argument("--rates", default="20,80,320,1280", help="serve workload: offered loads (requests/s)")

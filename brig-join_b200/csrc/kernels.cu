@@ -1585,48 +1585,55 @@ __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2*
 
 // Streams tuples [0, n) of `src` (shared memory when kShared, else global) through the filter and
 // the warp's candidate queue; full warps of candidates are probed as they form.
+template <bool kShared, int U, bool kGuard>
+__device__ __forceinline__ void probe_step(const JoinDesc& d, const uint2* __restrict__ src, uint32_t base, uint32_t n,
+                                           const uint32_t* bitmap, uint2* q, int& qn, const uint2* table,
+                                           const uint32_t* off, uint32_t mask, bool bs, int emit_key, int lane,
+                                           WarpOut& o) {
+    uint2 e[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const uint32_t i = base + u * kThreads + threadIdx.x;
+        if (kShared) e[u] = (!kGuard || i < n) ? src[i] : make_uint2(0u, 0u);
+        else e[u] = (!kGuard || i < n) ? __ldcs(src + i) : make_uint2(0u, 0u);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const uint32_t i = base + u * kThreads + threadIdx.x;
+        const uint32_t pb = presence_bit(e[u].x);
+        const bool cand = (!kGuard || i < n) && ((bitmap[pb >> 5] >> (pb & 31u)) & 1u);
+        const uint32_t cm = __ballot_sync(0xffffffffu, cand);
+        if (cm) {
+            if (cand) q[qn + __popc(cm & lanemask_lt())] = e[u];
+            qn += __popc(cm);
+            __syncwarp();
+            if (qn >= 32) {
+                probe_candidates(d, q, 32, table, off, mask, bs, emit_key, lane, o);
+                // move the overflow (fewer than 32) to the front of the queue
+                const uint2 rest = lane < qn - 32 ? q[32 + lane] : make_uint2(0u, 0u);
+                __syncwarp();
+                if (lane < qn - 32) q[lane] = rest;
+                qn -= 32;
+                __syncwarp();
+            }
+        }
+    }
+}
+
 template <bool kShared, int U>
 __device__ __forceinline__ void probe_stream(const JoinDesc& d, const uint2* __restrict__ src, uint32_t n,
                                              const uint32_t* bitmap, uint2* q, int& qn, const uint2* table,
                                              const uint32_t* off, uint32_t mask, bool bs, int emit_key, int lane,
                                              WarpOut& o) {
     constexpr uint32_t kStep = (uint32_t)(U * kThreads);
-    for (uint32_t base = 0; base < n; base += kStep) {
+    uint32_t base = 0;
+    for (; base + kStep <= n; base += kStep) {
         // streamed from global memory: keep the range two iterations ahead on its way into L2
         if (!kShared && threadIdx.x == 0 && base + 2 * kStep < n)
             prefetch_l2_range(src + base + 2 * kStep, src + min_i64((int64_t)n, (int64_t)base + 3 * kStep));
-        uint2 e[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t i = base + u * kThreads + threadIdx.x;
-            if (kShared) e[u] = i < n ? src[i] : make_uint2(0u, 0u);
-            else e[u] = i < n ? __ldcs(src + i) : make_uint2(0u, 0u);
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t i = base + u * kThreads + threadIdx.x;
-            bool cand = false;
-            if (i < n) {
-                const uint32_t pb = presence_bit(e[u].x);
-                cand = (bitmap[pb >> 5] >> (pb & 31u)) & 1u;
-            }
-            const uint32_t cm = __ballot_sync(0xffffffffu, cand);
-            if (cm) {
-                if (cand) q[qn + __popc(cm & lanemask_lt())] = e[u];
-                qn += __popc(cm);
-                __syncwarp();
-                if (qn >= 32) {
-                    probe_candidates(d, q, 32, table, off, mask, bs, emit_key, lane, o);
-                    // move the overflow (fewer than 32) to the front of the queue
-                    const uint2 rest = lane < qn - 32 ? q[32 + lane] : make_uint2(0u, 0u);
-                    __syncwarp();
-                    if (lane < qn - 32) q[lane] = rest;
-                    qn -= 32;
-                    __syncwarp();
-                }
-            }
-        }
+        probe_step<kShared, U, false>(d, src, base, n, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
     }
+    if (base < n) probe_step<kShared, U, true>(d, src, base, n, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
 }
 
 // A task of the probe queue with its join's buffers resolved: the build and streamed ranges.
