@@ -19,7 +19,8 @@ namespace brig {
 
 // ---- limits -------------------------------------------------------------------------------------
 constexpr int kMaxP1 = 4096;          // first-level fan-out (the reference caps at PARTITION_MAX=2048,
-                                      // src/kernel_functions.h:15)
+                                      // src/kernel_functions.h:15); at most 12 radix bits, which
+                                      // part1_m relies on
 constexpr int kMaxP2 = 1024;          // second-level fan-out (SECOND_PASS_MAX=4096, :14)
 constexpr int kMaxTable = 4096;       // build-side tuples per shared-memory table (largest allowed)
 constexpr int kDefaultTable = 4096;   // default table capacity
@@ -98,17 +99,33 @@ struct PartFn {
     uint64_t M1, M2;    // fastmod magics (modulo mode)
 };
 
+// mix32 without its last xor-shift, which changes only the low 16 bits: the top 16 bits are those
+// of mix32(key), so the level-1 id (b1 <= 12 bits) takes two fewer instructions from it.
+BRIG_HD uint32_t mix32_hi(uint32_t x) {
+    x ^= x >> 16; x *= 0x85ebca6bu;
+    x ^= x >> 13; x *= 0xc2b2ae35u;
+    return x;
+}
+// The top s bits of x (0 when s == 0): one clamped funnel shift on the device.
+BRIG_HD uint32_t top_bits(uint32_t x, int s) {
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_rc(x, 0u, 32u - (uint32_t)s);
+#else
+    return (uint32_t)(((uint64_t)x << s) >> 32);
+#endif
+}
+
 // Mode-specialised forms, M = 0 (hash) or 1 (modulo). The partition kernels are instantiated per
 // mode and skip the joins of the other mode, so their per-key code carries no mode test. In hash
 // mode p is the top b1 bits of mix32(key) and q the next b2 bits (both 0 when the bit count is 0).
 template <int M>
 BRIG_HD uint32_t part1_m(const PartFn& f, uint32_t key) {
-    if constexpr (M == 0) return (uint32_t)(((uint64_t)mix32(key) << f.b1) >> 32);
+    if constexpr (M == 0) return top_bits(mix32_hi(key), f.b1);  // b1 <= 12: equal to mix32's top bits
     else return fastmod(key, f.M1, f.P1);
 }
 template <int M>
 BRIG_HD uint32_t part2_m(const PartFn& f, uint32_t key) {
-    if constexpr (M == 0) return (uint32_t)(((uint64_t)(mix32(key) << f.b1) << f.b2) >> 32);
+    if constexpr (M == 0) return top_bits(mix32(key) << f.b1, f.b2);
     else return fastmod(key, f.M2, f.P2);
 }
 // Finest partition id p * P2 + q: the probe-task unit and the Bloom segment index.

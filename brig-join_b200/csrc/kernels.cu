@@ -517,10 +517,8 @@ __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, con
         if (x == 0 && t + 1 < ntiles)
             in.issue(t0 + kSTileB, (int)min_i64(kSTileB, end - t0 - kSTileB), inbuf + (b ^ 1) * buf_stride, &bars[b ^ 1]);
         // exclusive scan of the counts, one bin per thread (every warp scans the warp totals itself);
-        // cursor[x] (the next output position of bin x) and spos[x] (staged start | count << 16)
-        // stay in shared memory until the owner stores the run, which keeps registers free for the
-        // tuples held across the scan
-        const uint32_t n = owner ? cnt[x] : 0u;
+        // cursor[x] is the next output position of bin x, spos[x] its staged start this tile
+        const uint32_t n = owner ? cnt[x] : 0u;  // kept by the owner until it stores the run
         if (owner) cnt[x] = 0;  // for the next tile (its ranks may start before this tile's stores)
         uint32_t inc = n;
 #pragma unroll
@@ -538,27 +536,28 @@ __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, con
         }
         const uint32_t wbase = __shfl_sync(0xffffffffu, w, (wid + 31) & 31);
         const uint32_t e0 = inc - n + (wid > 0 ? wbase : 0u);
+        uint32_t sx = 0;  // the owner's staged start, kept until it stores the run
         if (owner) {
-            const uint32_t base = e0 + (uint32_t)x;                              // bin x owns n + 1 slots
-            spos[x] = (base + ((base ^ (uint32_t)cursor[x]) & 1u)) | (n << 16);  // same parity as its output
+            const uint32_t base = e0 + (uint32_t)x;                // bin x owns n + 1 slots
+            sx = base + ((base ^ (uint32_t)cursor[x]) & 1u);       // same parity as its output
+            spos[x] = sx;
         }
         __syncthreads();
         uint2* stage = reinterpret_cast<uint2*>(buf);
         if (full) {
 #pragma unroll
-            for (int k = 0; k < kItems; ++k) stage[(spos[br[k] >> 16] & 0xffffu) + (br[k] & 0xffffu)] = it[k];
+            for (int k = 0; k < kItems; ++k) stage[spos[br[k] >> 16] + (br[k] & 0xffffu)] = it[k];
         } else {
 #pragma unroll
             for (int k = 0; k < kItems; ++k) {
                 const int i = k * kSThreads + x;
-                if (i < tn) stage[(spos[br[k] >> 16] & 0xffffu) + (br[k] & 0xffffu)] = it[k];
+                if (i < tn) stage[spos[br[k] >> 16] + (br[k] & 0xffffu)] = it[k];
             }
         }
         fence_proxy_async();  // the staging stores before the bulk engine reads them
         __syncthreads();
         if (owner) {
-            const uint32_t sp = spos[x];
-            const uint32_t n = sp >> 16, s = sp & 0xffffu;
+            const uint32_t s = sx;
             const int64_t o = cursor[x];
             cursor[x] = o + n;
             if (n == 0) {
@@ -644,7 +643,7 @@ __device__ __forceinline__ bool bloom_pass(uint2 w, uint2 mk) {
 // Finest partition of a key with mix m (hash mode: the top b1 + b2 bits) or key (modulo mode).
 template <int M>
 __device__ __forceinline__ uint32_t fine_of(const PartFn& f, uint32_t key, uint32_t m) {
-    if constexpr (M == 0) return (uint32_t)(((uint64_t)m << (f.b1 + f.b2)) >> 32);
+    if constexpr (M == 0) return top_bits(m, f.b1 + f.b2);
     else return fastmod(key, f.M1, f.P1) * f.P2 + fastmod(key, f.M2, f.P2);
 }
 constexpr int kProbeILP = 6;  // keys per thread with their filter words in flight together
@@ -995,7 +994,7 @@ __device__ __forceinline__ void l2_bloom_group(const uint2* __restrict__ src, in
         const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
         const uint32_t m = mix32(e[u].x);
         uint32_t q;
-        if constexpr (M == 0) q = (uint32_t)(((uint64_t)(m << pf.b1) << pf.b2) >> 32);
+        if constexpr (M == 0) q = top_bits(m << pf.b1, pf.b2);
         else q = fastmod(e[u].x, pf.M2, pf.P2);
         const BloomSlot sl = bloom_slot(m, fine0 + q, seg_blocks);
         wv[u] = make_uint2(0u, 0u);
