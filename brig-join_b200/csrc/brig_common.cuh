@@ -36,7 +36,7 @@ constexpr int kWarpBuf = 128;         // output pairs staged per warp before a g
 // Tuples per level-2 slice: 262144, or 131072 for S when its second pass probes the Bloom filter
 // (the filter segments of the partitions in flight must stay in L2; with the longer slices twice
 // as many partitions are in flight).
-constexpr int64_t kL2Slice = 64 * kTile;
+constexpr int64_t kL2Slice = 21 * kSTile;
 constexpr uint32_t kDefaultWaitPolls = 1u << 22;  // polls of a bounded wait before it gives up
 constexpr int64_t kL2SliceBloom = 32 * kTile;
 
