@@ -30,8 +30,15 @@ constexpr int kMaxBloomK = 16;
 constexpr int kThreads = 512;         // threads per CTA of every partition and probe kernel
 constexpr int kTile = 4096;           // unit of the level-2 slice length
 constexpr int kSThreads = 1024;       // threads per CTA of the scatter kernels (one CTA per SM)
+constexpr int kSThreadsSmall = 512;   // threads per CTA of their small bulk-store form (two per SM)
 constexpr int kSTile = 12288;         // tuples per tile of the bulk-store scatter (slice lengths are
                                       // multiples of it)
+// Forms of a scatter launch: the write pass (any bin count up to the fan-out limits), the
+// bulk-store form (up to kBulkMaxBins bins, 12288-tuple tiles, one 1024-thread CTA per SM) and its
+// small form (up to kBulkSmallMaxBins bins, 6144-tuple tiles, two 512-thread CTAs per SM).
+enum ScatterForm : int { kFormPass = 0, kFormBulk = 1, kFormBulkSmall = 2 };
+constexpr int kBulkMaxBins = 1024;
+constexpr int kBulkSmallMaxBins = 512;
 constexpr int kWarpBuf = 128;         // output pairs staged per warp before a global flush
 // Tuples per level-2 slice: 262144, or 131072 for S when its second pass probes the Bloom filter
 // (the filter segments of the partitions in flight must stay in L2; with the longer slices twice

@@ -628,6 +628,31 @@ void fill_pipeline(const brig_join_config& cfg, const JoinPlan* plans, const Joi
     a.slice_cnt2 = reinterpret_cast<uint32_t*>(ws + sh.slice_cnt2);
     a.l2_slice_cap[0] = sh.l2_slice_cap[0];
     a.l2_slice_cap[1] = sh.l2_slice_cap[1];
+    // Scatter forms. The small bulk-store form (two CTAs per SM, half-size tiles) hides the
+    // per-slice start-up and the per-tile barriers of one CTA behind the other's work, which is what
+    // short slices need; the full-size tiles' longer runs per bin win on long slices over many bins.
+    // Slices are short below 64K tuples, or below 256K when there are at most 128 bins (runs of 48
+    // or more tuples per half tile). S's level-2 input is the filter's survivors when its filter is
+    // probed at level 2: a fraction of slices of 131072 tuples, short in any case. Measured at 640M
+    // x 640M (512 x 512 bins): level-1 slices of 1M tuples, level-2 slices of R of 214K tuples in the
+    // large form; survivors 0.52 ms in the small form against 0.69 in the large one.
+    int64_t rel_n[2] = {0, 0};
+    for (int j = 0; j < nj; ++j) {
+        rel_n[0] += plans[j].nr;
+        rel_n[1] += plans[j].ns;
+    }
+    auto form_for = [](int bins, int64_t avg_slice, bool short_slices) {
+        if (bins > kBulkMaxBins) return (int)kFormPass;
+        if (bins <= kBulkSmallMaxBins &&
+            (short_slices || avg_slice < 65536 || (bins <= 128 && avg_slice < 262144)))
+            return (int)kFormBulkSmall;
+        return (int)kFormBulk;
+    };
+    for (int r = 0; r < 2; ++r) {
+        a.l1_form[r] = form_for(sh.max_p1, rel_n[r] / std::max<int64_t>(1, sh.total_slices[r]), false);
+        a.l2_form[r] = form_for(sh.max_p2, rel_n[r] / std::max<int64_t>(1, sh.l2_slice_cap[r]),
+                                r == 1 && sh.any_bloom_l2);
+    }
 }
 
 void Engine::run(const std::vector<JoinIO>& joins, cudaStream_t stream, bool use_graph, cudaEvent_t s_ready) {

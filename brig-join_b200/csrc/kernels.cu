@@ -352,6 +352,20 @@ constexpr int kSTileW = 8192;    // write-pass form
 constexpr int kSTileB = kSTile;  // bulk-store form
 static_assert(kSTileB % (4 * kSThreads) == 0 && kSTileW % (4 * kSThreads) == 0, "whole 16-byte loads per thread");
 
+// The three scatter forms a launch can take (ScatterForm). kFormBulkSmall is the bulk-store form in CTAs of 512
+// threads with 6144-tuple tiles, two CTAs per SM: each CTA's barriers, scans and slice start-up
+// overlap the other CTA's work, which pays where slices are short (a batch of small joins, the
+// Bloom survivors of a level-2 slice) or bins few (long runs per tile even in half a tile); on long
+// slices over many bins the full-size tile's longer runs win (640M keys, 512 bins: 2.40 ms for the
+// level-1 scatter against 3.61 in the small form).
+__host__ __device__ constexpr int form_threads(int f) { return f == kFormBulkSmall ? kSThreadsSmall : kSThreads; }
+__host__ __device__ constexpr int form_tile(int f) {
+    return f == kFormBulkSmall ? kSTile / 2 : (f == kFormBulk ? kSTileB : kSTileW);
+}
+__host__ __device__ constexpr int form_ctas_per_sm(int f) { return f == kFormBulkSmall ? 2 : 1; }
+static_assert(form_tile(kFormBulkSmall) % (4 * kSThreadsSmall) == 0, "whole 16-byte loads per thread");
+static_assert(kSTile % form_tile(kFormBulkSmall) == 0, "slices are whole small tiles");
+
 // Scatters tuples [begin, end) of `in` into `out`. cursor[b] is the next output position of bin
 // b; it advances as tiles are written. Each tile of kSTileW tuples arrives by bulk copy into one of
 // the two input buffers while the previous tile is processed. Per tile every thread holds its
@@ -459,43 +473,63 @@ __device__ void scatter_tiles(const In& in, int64_t begin, int64_t end, const Bi
 // the staging stores and the bulk engine's reads only. The next tile's load goes into the other
 // buffer once the bulk copies of the tile that used it have finished reading it (checked after
 // step 1, by when they normally have).
-constexpr int kBulkMaxBins = 1024;
-static_assert(kBulkMaxBins <= kSThreads, "one bin per thread");
-// The level-2 scatter takes the bulk path up to the same bin count: with 12288-tuple tiles it beats
-// the write-pass form at 512 bins too (R's level-2 scatter at 640M keys: 3.14 against 3.28 ms).
-constexpr int kBulkMaxBinsL2 = kBulkMaxBins;
-// One tile buffer of the bulk scatter: the tile plus one slot per bin, a multiple of 16 bytes.
-__host__ __device__ constexpr size_t bulk_tile_buf(int max_bins) {
-    return (size_t)((kSTileB + max_bins + 2 + 1) & ~1) * 8;
+static_assert(kBulkMaxBins <= kSThreads && kBulkSmallMaxBins <= kSThreadsSmall, "one bin per thread");
+// A staging buffer of the bulk scatter: a tile of TILE tuples plus one slot per bin, a multiple of
+// 16 bytes. The large form stages each tile in its own input buffer (two such buffers); the small
+// form has one input buffer of a tile (plus the tuple before a misaligned start) and one staging
+// buffer.
+__host__ __device__ constexpr size_t bulk_tile_buf(int max_bins, int tile = kSTileB) {
+    return (size_t)((tile + max_bins + 2 + 1) & ~1) * 8;
 }
+__host__ __device__ constexpr size_t bulk_in_buf(int tile) { return (size_t)(tile + 2) * 8; }
+static_assert(bulk_in_buf(kSTile / 2) % 16 == 0, "the staging buffer after it starts on 16 bytes");
 
-template <class In, class Bin>
+template <int F, class In, class Bin>
 __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, const Bin& bin, int nbins,
                                    uint2* __restrict__ out, int64_t out_limit, int64_t* cursor, uint32_t* cnt,
                                    uint32_t* spos, uint32_t* tmp, unsigned char* inbuf, size_t buf_stride,
                                    uint64_t* bars, uint32_t& ph, unsigned long long* errors, uint32_t polls) {
-    constexpr int kItems = kSTileB / kSThreads;
-    constexpr int kWarps = kSThreads / 32;
-    const int64_t ntiles = (end - begin + kSTileB - 1) / kSTileB;
+    // kSplit: one input buffer and a separate staging buffer at inbuf + buf_stride (small form);
+    // else two input buffers buf_stride apart, each tile staged in its own (large form).
+    constexpr bool kSplit = F == kFormBulkSmall;
+    constexpr int NT = form_threads(F), TILE = form_tile(F);
+    constexpr int kItems = TILE / NT;
+    constexpr int kWarps = NT / 32;
+    const int64_t ntiles = (end - begin + TILE - 1) / TILE;
     if (ntiles <= 0) return;
     const int x = threadIdx.x, lane = x & 31, wid = x >> 5;
     const bool owner = x < nbins;
     if (owner) cnt[x] = 0;
-    if (x == 0) in.issue(begin, (int)min_i64(kSTileB, end - begin), inbuf, &bars[0]);
+    if (x == 0) in.issue(begin, (int)min_i64(TILE, end - begin), inbuf, &bars[0]);
     __syncthreads();  // cnt is zero
     for (int64_t t = 0; t < ntiles; ++t) {
-        const int64_t t0 = begin + t * kSTileB;
-        const int tn = (int)min_i64(kSTileB, end - t0);
-        const int b = (int)(t & 1);
+        const int64_t t0 = begin + t * TILE;
+        const int tn = (int)min_i64(TILE, end - t0);
+        const int b = kSplit ? 0 : (int)(t & 1);
         mbar_wait(&bars[b], (ph >> b) & 1u, errors, polls);
         ph ^= 1u << b;
         unsigned char* buf = inbuf + b * buf_stride;
+        uint2* stage = reinterpret_cast<uint2*>(kSplit ? inbuf + buf_stride : buf);
         const auto lay = in.layout(t0, tn);
-        const bool full = tn == kSTileB && in.fast(lay);  // block-uniform
+        const bool full = tn == TILE && in.fast(lay);  // block-uniform
         uint2 it[kItems];
         uint32_t br[kItems];  // bin << 16 | rank of the tuple within its bin in this tile
         if (full) {
-            in.template load_full<kItems, kSThreads>(buf, lay, it);
+            in.template load_full<kItems, NT>(buf, lay, it);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kItems; ++k) {
+                const int i = k * NT + x;
+                if (i < tn) it[k] = in.item(buf, t0, i, tn, lay);
+            }
+        }
+        if constexpr (kSplit) {
+            // every thread holds its tuples: the input buffer takes the next tile, whose load then
+            // overlaps this tile's ranking, scan, staging and stores
+            __syncthreads();
+            if (x == 0 && t + 1 < ntiles) in.issue(t0 + TILE, (int)min_i64(TILE, end - t0 - TILE), inbuf, &bars[0]);
+        }
+        if (full) {
 #pragma unroll
             for (int k = 0; k < kItems; ++k) {
                 const uint32_t bb = bin(it[k].x);
@@ -504,18 +538,18 @@ __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, con
         } else {
 #pragma unroll
             for (int k = 0; k < kItems; ++k) {
-                const int i = k * kSThreads + x;
-                if (i < tn) {
-                    it[k] = in.item(buf, t0, i, tn, lay);
+                if (k * NT + x < tn) {
                     const uint32_t bb = bin(it[k].x);
                     br[k] = (bb << 16) | atomicAdd(&cnt[bb], 1u);
                 }
             }
         }
-        bulk_wait_read();  // this thread's bulk stores of the previous tile have read buffer b ^ 1
+        // this thread's bulk stores of the previous tile have read their staging slots (the other
+        // input buffer, or the staging buffer)
+        bulk_wait_read();
         __syncthreads();
-        if (x == 0 && t + 1 < ntiles)
-            in.issue(t0 + kSTileB, (int)min_i64(kSTileB, end - t0 - kSTileB), inbuf + (b ^ 1) * buf_stride, &bars[b ^ 1]);
+        if (!kSplit && x == 0 && t + 1 < ntiles)
+            in.issue(t0 + TILE, (int)min_i64(TILE, end - t0 - TILE), inbuf + (b ^ 1) * buf_stride, &bars[b ^ 1]);
         // exclusive scan of the counts, one bin per thread (every warp scans the warp totals itself);
         // cursor[x] is the next output position of bin x, spos[x] its staged start this tile
         const uint32_t n = owner ? cnt[x] : 0u;  // kept by the owner until it stores the run
@@ -543,16 +577,13 @@ __device__ void scatter_tiles_bulk(const In& in, int64_t begin, int64_t end, con
             spos[x] = sx;
         }
         __syncthreads();
-        uint2* stage = reinterpret_cast<uint2*>(buf);
         if (full) {
 #pragma unroll
             for (int k = 0; k < kItems; ++k) stage[spos[br[k] >> 16] + (br[k] & 0xffffu)] = it[k];
         } else {
 #pragma unroll
-            for (int k = 0; k < kItems; ++k) {
-                const int i = k * kSThreads + x;
-                if (i < tn) stage[spos[br[k] >> 16] + (br[k] & 0xffffu)] = it[k];
-            }
+            for (int k = 0; k < kItems; ++k)
+                if (k * NT + x < tn) stage[spos[br[k] >> 16] + (br[k] & 0xffffu)] = it[k];
         }
         fence_proxy_async();  // the staging stores before the bulk engine reads them
         __syncthreads();
@@ -598,10 +629,17 @@ __device__ __forceinline__ void scatter_carve(unsigned char* smem, int max_bins,
 
 // Shared-memory layout of the bulk scatter: two tile buffers of bulk_tile_buf(max_bins) bytes, then
 // the output cursors (int64 per bin), the bin counts and the staged starts (uint32 each).
-__device__ __forceinline__ void bulk_carve(unsigned char* smem, int max_bins, unsigned char*& inbuf,
+__host__ __device__ constexpr size_t bulk_buf_stride(int form, int max_bins) {
+    return form == kFormBulkSmall ? bulk_in_buf(kSTile / 2) : bulk_tile_buf(max_bins);
+}
+__host__ __device__ constexpr size_t bulk_bufs(int form, int max_bins) {
+    return form == kFormBulkSmall ? bulk_in_buf(kSTile / 2) + bulk_tile_buf(max_bins, kSTile / 2)
+                                  : 2 * bulk_tile_buf(max_bins);
+}
+__device__ __forceinline__ void bulk_carve(unsigned char* smem, int form, int max_bins, unsigned char*& inbuf,
                                            int64_t*& cursor, uint32_t*& cnt, uint32_t*& spos) {
     inbuf = smem;
-    cursor = reinterpret_cast<int64_t*>(smem + 2 * bulk_tile_buf(max_bins));
+    cursor = reinterpret_cast<int64_t*>(smem + bulk_bufs(form, max_bins));
     cnt = reinterpret_cast<uint32_t*>(cursor + max_bins);
     spos = cnt + max_bins;
 }
@@ -798,17 +836,18 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 // of this relation, i.e. the partition's start plus the counts of all earlier slices.
 // kPacked selects the slices this launch handles: false = tuples from the caller's key/value arrays,
 // true = S survivors of a level-1 Bloom probe, packed in cmp. One instantiation per input form keeps
-// each kernel within the 64 registers that two CTAs per SM allow.
-template <bool kPacked, int M, bool kBulk>
-__global__ void __launch_bounds__(kSThreads, 1)
+// each kernel within 64 registers a thread. F is the scatter form (ScatterForm).
+template <bool kPacked, int M, int F>
+__global__ void __launch_bounds__(form_threads(F), form_ctas_per_sm(F))
 k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ slice_prefix,
              const int64_t* __restrict__ scan, unsigned long long* gwords, int max_bins) {
+    constexpr bool kBulk = F != kFormPass;
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* inbuf;
     int64_t *cursor, *delta = nullptr;
     uint32_t *cnt, *spos = nullptr;
     uint16_t* sbin = nullptr;
-    if constexpr (kBulk) bulk_carve(smem, max_bins, inbuf, cursor, cnt, spos);  // max_bins <= kBulkMaxBins
+    if constexpr (kBulk) bulk_carve(smem, F, max_bins, inbuf, cursor, cnt, spos);  // max_bins: at most the form's bins
     else scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
     __shared__ uint32_t tmp[kSThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
@@ -828,24 +867,24 @@ k_l1_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const uint32_t P1 = d.pf.P1;
         const int64_t* S = scan + R.hist_base;
         const int64_t s0 = S[0];
-        for (uint32_t p = threadIdx.x; p < P1; p += kSThreads)
+        for (uint32_t p = threadIdx.x; p < P1; p += form_threads(F))
             cursor[p] = S[(int64_t)p * R.nslices + s] - s0;
         __syncthreads();
         const Bin1<M> bin{d.pf};
         if constexpr (kPacked) {
             const PackedTiles in{R.cmp};
             if constexpr (kBulk)
-                scatter_tiles_bulk(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
-                                   bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors], polls);
+                scatter_tiles_bulk<F>(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
+                                      bulk_buf_stride(F, max_bins), bars, ph, &gwords[kGErrors], polls);
             else
                 scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph,
                               &gwords[kGErrors], polls);
         } else {
             const bool al = ((((uintptr_t)R.key) | ((uintptr_t)R.val)) & 3) == 0;
             if constexpr (kBulk) {
-                const KvTiles<kSTileB> in{R.key, R.val, al};
-                scatter_tiles_bulk(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
-                                   bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors], polls);
+                const KvTiles<form_tile(F)> in{R.key, R.val, al};
+                scatter_tiles_bulk<F>(in, b, e, bin, (int)P1, R.l1, R.n, cursor, cnt, spos, tmp, inbuf,
+                                      bulk_buf_stride(F, max_bins), bars, ph, &gwords[kGErrors], polls);
             } else {
                 const KvTiles<kSTileW> in{R.key, R.val, al};
                 scatter_tiles(in, b, e, bin, (int)P1, R.l1, R.n, cursor, delta, cnt, sbin, tmp, inbuf, bars, ph,
@@ -1083,19 +1122,20 @@ k_l2_bloom(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ s
     }
 }
 
-// Level-2 scatter of one slice into its private runs of the level-2 buffer.
-template <int M, bool kBulk>
-__global__ void __launch_bounds__(kSThreads, 1)
+// Level-2 scatter of one slice into its private runs of the level-2 buffer (F: the scatter form).
+template <int M, int F>
+__global__ void __launch_bounds__(form_threads(F), form_ctas_per_sm(F))
 k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __restrict__ seg_prefix,
              const int64_t* __restrict__ seg_off, const uint32_t* __restrict__ seg_ns, int64_t total_segs,
              const int64_t* __restrict__ scan2, const uint32_t* __restrict__ slice_cnt2, unsigned long long* gwords,
              int max_bins) {
+    constexpr bool kBulk = F != kFormPass;
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned char* inbuf;
     int64_t *cursor, *delta = nullptr;
     uint32_t *cnt, *spos = nullptr;
     uint16_t* sbin = nullptr;
-    if constexpr (kBulk) bulk_carve(smem, max_bins, inbuf, cursor, cnt, spos);  // max_bins <= kBulkMaxBins
+    if constexpr (kBulk) bulk_carve(smem, F, max_bins, inbuf, cursor, cnt, spos);  // max_bins: at most the form's bins
     else scatter_carve(smem, max_bins, inbuf, cursor, delta, cnt, sbin);
     __shared__ uint32_t tmp[kSThreads / 32];
     __shared__ __align__(8) uint64_t bars[2];
@@ -1115,12 +1155,12 @@ k_l2_scatter(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __r
         const int64_t* S2 = scan2 + R.h2_base;
         const int64_t s0 = S2[0];
         const int64_t* Sx = S2 + x.local_off * P2;
-        for (uint32_t q = threadIdx.x; q < P2; q += kSThreads) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
+        for (uint32_t q = threadIdx.x; q < P2; q += form_threads(F)) cursor[q] = Sx[(int64_t)q * x.ns + x.sl] - s0;
         __syncthreads();
         const PackedTiles in{bloom ? R.cmp : R.l1};
         if constexpr (kBulk)
-            scatter_tiles_bulk(in, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2, R.n, cursor, cnt, spos, tmp, inbuf,
-                               bulk_tile_buf(max_bins), bars, ph, &gwords[kGErrors], polls);
+            scatter_tiles_bulk<F>(in, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2, R.n, cursor, cnt, spos, tmp, inbuf,
+                                  bulk_buf_stride(F, max_bins), bars, ph, &gwords[kGErrors], polls);
         else
             scatter_tiles(in, begin, end, Bin2<M>{d.pf}, (int)P2, R.l2, R.n, cursor, delta, cnt, sbin, tmp, inbuf,
                           bars, ph, &gwords[kGErrors], polls);
@@ -1905,8 +1945,8 @@ size_t probe_smem_bytes(int table_cap, int emit_key) {
 // cursor and a count per bin.
 // Dynamic shared memory of a scatter kernel over at most max_bins bins: the bulk-store layout
 // (bulk_carve) or the write-pass layout (scatter_carve).
-static size_t scatter_smem(int max_bins, bool bulk) {
-    if (bulk) return 2 * bulk_tile_buf(max_bins) + (size_t)max_bins * (8 + 4 + 4);
+static size_t scatter_smem(int max_bins, int form) {
+    if (form != kFormPass) return bulk_bufs(form, max_bins) + (size_t)max_bins * (8 + 4 + 4);
     return 2 * kTileBufW + (size_t)max_bins * (8 + 8 + 4) + (size_t)kSTileW * 2;
 }
 
@@ -1931,6 +1971,14 @@ static void for_modes(int modes, F&& f) {
     if (modes & 2) f(std::integral_constant<int, 1>{});
 }
 
+// Calls f(std::integral_constant<int, F>) for the scatter form F (ScatterForm).
+template <class Fn>
+static void for_form(int form, Fn&& f) {
+    if (form == kFormBulkSmall) f(std::integral_constant<int, kFormBulkSmall>{});
+    else if (form == kFormBulk) f(std::integral_constant<int, kFormBulk>{});
+    else f(std::integral_constant<int, kFormPass>{});
+}
+
 static int grid_for(int64_t work, int num_sms, int per_sm) {
     int64_t g = std::min<int64_t>(work, (int64_t)num_sms * per_sm);
     return (int)std::max<int64_t>(g, 1);
@@ -1938,18 +1986,29 @@ static int grid_for(int64_t work, int num_sms, int per_sm) {
 
 static cudaError_t set_kernel_attrs() {
     cudaError_t err;
-    const void* l1s[] = {(const void*)k_l1_scatter<false, 0, false>, (const void*)k_l1_scatter<false, 1, false>,
-                         (const void*)k_l1_scatter<true, 0, false>, (const void*)k_l1_scatter<true, 1, false>};
+    const void* l1s[] = {(const void*)k_l1_scatter<false, 0, kFormPass>, (const void*)k_l1_scatter<false, 1, kFormPass>,
+                         (const void*)k_l1_scatter<true, 0, kFormPass>, (const void*)k_l1_scatter<true, 1, kFormPass>};
     for (const void* f : l1s)
-        if ((err = set_smem_attr(f, scatter_smem(kMaxP1, false))) != cudaSuccess) return err;
-    const void* bulks[] = {(const void*)k_l1_scatter<false, 0, true>, (const void*)k_l1_scatter<false, 1, true>,
-                           (const void*)k_l1_scatter<true, 0, true>,  (const void*)k_l1_scatter<true, 1, true>,
-                           (const void*)k_l2_scatter<0, true>,        (const void*)k_l2_scatter<1, true>};
+        if ((err = set_smem_attr(f, scatter_smem(kMaxP1, kFormPass))) != cudaSuccess) return err;
+    const void* bulks[] = {(const void*)k_l1_scatter<false, 0, kFormBulk>, (const void*)k_l1_scatter<false, 1, kFormBulk>,
+                           (const void*)k_l1_scatter<true, 0, kFormBulk>,  (const void*)k_l1_scatter<true, 1, kFormBulk>,
+                           (const void*)k_l2_scatter<0, kFormBulk>,        (const void*)k_l2_scatter<1, kFormBulk>};
     for (const void* f : bulks)
-        if ((err = set_smem_attr(f, scatter_smem(kBulkMaxBins, true))) != cudaSuccess) return err;
-    const void* l2s[] = {(const void*)k_l2_scatter<0, false>, (const void*)k_l2_scatter<1, false>};
+        if ((err = set_smem_attr(f, scatter_smem(kBulkMaxBins, kFormBulk))) != cudaSuccess) return err;
+    // the small form: two CTAs per SM, so shared memory takes the largest carve-out
+    const void* smalls[] = {
+        (const void*)k_l1_scatter<false, 0, kFormBulkSmall>, (const void*)k_l1_scatter<false, 1, kFormBulkSmall>,
+        (const void*)k_l1_scatter<true, 0, kFormBulkSmall>,  (const void*)k_l1_scatter<true, 1, kFormBulkSmall>,
+        (const void*)k_l2_scatter<0, kFormBulkSmall>,        (const void*)k_l2_scatter<1, kFormBulkSmall>};
+    for (const void* f : smalls) {
+        if ((err = set_smem_attr(f, scatter_smem(kBulkSmallMaxBins, kFormBulkSmall))) != cudaSuccess) return err;
+        if ((err = cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+            return err;
+    }
+    const void* l2s[] = {(const void*)k_l2_scatter<0, kFormPass>, (const void*)k_l2_scatter<1, kFormPass>};
     for (const void* f : l2s)
-        if ((err = set_smem_attr(f, scatter_smem(kMaxP2, false))) != cudaSuccess) return err;
+        if ((err = set_smem_attr(f, scatter_smem(kMaxP2, kFormPass))) != cudaSuccess) return err;
     const void* bbs[] = {(const void*)k_bloom_build<0, 0>, (const void*)k_bloom_build<1, 0>,
                          (const void*)k_bloom_build<0, kBloomFastK>, (const void*)k_bloom_build<1, kBloomFastK>};
     for (const void* f : bbs)
@@ -2022,18 +2081,20 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
         if (a.total_slices[rel] > 0) {
             for_modes(a.modes, [&](auto mt) {
                 constexpr int M = decltype(mt)::value;
-                const dim3 grid(grid_for(a.total_slices[rel], sms, 1));
-                const bool bulk = a.max_p1 <= kBulkMaxBins;
-                (bulk ? k_l1_scatter<false, M, true> : k_l1_scatter<false, M, false>)<<<grid, kSThreads,
-                    scatter_smem(a.max_p1, bulk), st>>>(a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords,
-                                                  a.max_p1);
-                ++launches;
-                if (rel == 1 && a.any_bloom_l1) {
-                    (bulk ? k_l1_scatter<true, M, true> : k_l1_scatter<true, M, false>)<<<grid, kSThreads,
-                        scatter_smem(a.max_p1, bulk), st>>>(a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords,
-                                                      a.max_p1);
+                const int form = a.l1_form[rel];
+                for_form(form, [&](auto ft) {
+                    constexpr int F = decltype(ft)::value;
+                    const dim3 grid(grid_for(a.total_slices[rel], sms, form_ctas_per_sm(F)));
+                    const size_t smem = scatter_smem(a.max_p1, F);
+                    k_l1_scatter<false, M, F><<<grid, form_threads(F), smem, st>>>(
+                        a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
                     ++launches;
-                }
+                    if (rel == 1 && a.any_bloom_l1) {
+                        k_l1_scatter<true, M, F><<<grid, form_threads(F), smem, st>>>(
+                            a.J, a.nj, rel, a.slice_prefix[rel], a.hist_scan, a.gwords, a.max_p1);
+                        ++launches;
+                    }
+                });
             });
         }
         mark(m0 + 2);
@@ -2075,12 +2136,14 @@ cudaError_t enqueue_pipeline(const PipelineArgs& a, cudaStream_t st) {
                 return err;
             for_modes(a.modes, [&](auto mt) {
                 constexpr int M = decltype(mt)::value;
-                const bool bulk2 = a.max_p2 <= kBulkMaxBinsL2;
-                (bulk2 ? k_l2_scatter<M, true> : k_l2_scatter<M, false>)<<<grid_for(a.l2_slice_cap[rel], sms, 1),
-                                                                          kSThreads, scatter_smem(a.max_p2, bulk2), st>>>(
-                    a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2_scan, a.slice_cnt2,
-                    a.gwords, a.max_p2);
-                ++launches;
+                for_form(a.l2_form[rel], [&](auto ft) {
+                    constexpr int F = decltype(ft)::value;
+                    k_l2_scatter<M, F><<<grid_for(a.l2_slice_cap[rel], sms, form_ctas_per_sm(F)), form_threads(F),
+                                         scatter_smem(a.max_p2, F), st>>>(
+                        a.J, a.nj, rel, a.seg_prefix, a.seg_off, a.seg_ns, a.total_segs, a.hist2_scan, a.slice_cnt2,
+                        a.gwords, a.max_p2);
+                    ++launches;
+                });
             });
             dim3 grid((unsigned)std::min<int64_t>(((int64_t)a.max_p1 * a.max_p2 + 1 + 255) / 256, 4096),
                       (unsigned)std::min(a.nj, 65535));

@@ -59,6 +59,7 @@ struct PipelineArgs {
     int64_t h2_begin[2], h2_len[2];   // range of each relation in hist2
     uint32_t* slice_cnt2;             // [max slices] survivors per slice (level-2 Bloom probe)
     int64_t l2_slice_cap[2];          // upper bound of level-2 slices per relation
+    int l1_form[2], l2_form[2];       // ScatterForm of each relation's level-1 and level-2 scatters
 };
 
 // Pipeline parts (a full join runs all four; the reference-named entry points run subsets).

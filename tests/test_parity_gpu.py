@@ -26,6 +26,30 @@ def test_uniform_hash(bj, oracle, torch_cuda, n, bloom):
         assert st.count <= st.s_survivors < n
 
 
+# Scatter forms. The engine picks, per scatter launch, the write pass (more than 1024 bins), the
+# bulk-store form (1024-thread CTAs, 12288-tuple tiles) or its small form (two 512-thread CTAs per
+# SM, 6144-tuple tiles) from the bin count and the mean slice length: small below 64K tuples per
+# slice, or below 256K with at most 128 bins; S's level-2 survivors of a level-2 filter always small.
+# Small joins take the small form everywhere; these cases reach the large form at 2^24 tuples with
+# one level-1 slice per SM (slices of 113,664 tuples):
+#   l1_large: 512 level-1 bins -> large level-1 scatters (level 2: 16 bins, short slices -> small);
+#   l2_large: 16 x 512 -> small level-1 scatters, large level-2 scatters (slices of about 204K).
+@pytest.mark.parametrize("case", [
+    dict(partition_size=512),
+    dict(partition_size=512, use_bloom=1, bloom_probe_level=1),
+    dict(partition_mode=1, partition_size=500, second_partition_size=9),
+    dict(partition_size=16, second_partition_size=512),
+    dict(partition_size=16, second_partition_size=512, use_bloom=1, bloom_probe_level=2),
+    dict(partition_mode=1, partition_size=16, second_partition_size=509),
+], ids=["l1_large", "l1_large_bloom1", "l1_large_modulo", "l2_large", "l2_large_bloom2", "l2_large_modulo"])
+def test_large_scatter_form_16M(bj, oracle, torch_cuda, case):
+    n = 1 << 24
+    rk, rv, sk, sv = bj.gen_host(5, n, n, 0.1)
+    st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, slices_per_sm=1, **case)
+    assert st.count == n // 10
+    assert st.partition_size == case["partition_size"]
+
+
 @pytest.mark.parametrize("level", [1, 2])
 @pytest.mark.parametrize("mode,p1,p2", [(0, 16, 16), (0, 64, 64), (1, 100, 7), (1, 512, 67), (0, 4, 64)])
 def test_bloom_probe_levels(bj, oracle, torch_cuda, level, mode, p1, p2):
