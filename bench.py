@@ -215,14 +215,14 @@ def stage_bytes(nr, ns, surv, matches, bloom_bits, bloom_level):
 
 
 # DRAM bytes (read + write) per tuple of each stage's main kernel, from ncu captures of the same
-# kernels on 2^26 x 2^26 (inputs 4x the L2, level-1 fan-out 512 as at 640M) summarised in the
-# profiles directory: (bytes per tuple, which count the stage's launch processes). Used to scale the
+# kernels on 2^26 x 2^26 (inputs 4x the L2, fan-outs 512 x 512 and the filter probed at level 2 as at
+# 640M) summarised in the profiles directory: (bytes per tuple, which count the stage's launch processes). Used to scale the
 # measured traffic to the benchmarked launch; the per-tuple traffic of these streaming kernels does
 # not depend on the relation size once the inputs exceed the L2.
 NCU_TRAFFIC_PER_TUPLE = {
-    "r_hist": (4.07, "nr"), "r_scatter": (16.1, "nr"), "r_l2_hist": (8.06, "nr"), "r_l2_scatter": (16.2, "nr"),
-    "bloom_build": (8.44, "nr"), "s_hist_probe": (4.06, "ns"), "s_scatter": (16.1, "ns"),
-    "s_l2_hist": (10.04, "ns"), "probe": (9.83, "nr"),
+    "r_hist": (4.05, "nr"), "r_scatter": (15.93, "nr"), "r_l2_hist": (8.01, "nr"), "r_l2_scatter": (16.30, "nr"),
+    "bloom_build": (9.01, "nr"), "s_hist_probe": (4.01, "ns"), "s_scatter": (15.94, "ns"),
+    "s_l2_hist": (10.15, "ns"), "probe": (9.93, "nr"),
 }
 
 
@@ -234,6 +234,28 @@ def stage_traffic(stage, nr, ns, bloom_level):
         return None  # captured with the filter probed in the second pass
     per, unit = NCU_TRAFFIC_PER_TUPLE[stage]
     return per * (nr if unit == "nr" else ns)
+
+
+def gather_peak(bj, torch, stream, table_bytes=2 << 20, loads=1 << 30):
+    """Random 8-byte reads per second from an L2-resident table (brig_join_gather_rate): the ceiling of
+    the level-2 Bloom probe, one such read per key. Median of 5 timed launches after 2 warm-ups."""
+    table = torch.randint(0, 1 << 30, (table_bytes // 4,), dtype=torch.int32, device="cuda")
+    sink = torch.zeros(1, dtype=torch.int32, device="cuda")
+    sp = stream.cuda_stream
+    for _ in range(2):
+        bj.gather_rate(table, loads, sink, stream=sp)
+    rates = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        n = bj.gather_rate(table, loads, sink, stream=sp)
+        e1.record(stream)
+        e1.synchronize()
+        rates.append(n / (e0.elapsed_time(e1) / 1e3))
+    rates.sort()
+    return {"peak_reads_per_s": rates[len(rates) // 2], "unit": "reads/s",
+            "peak_kind": f"measured in this run: brig_join_gather_rate, {loads} random 8-byte reads from a "
+                         f"{table_bytes >> 20} MB L2-resident table"}
 
 
 # ---- batched uneven joins -------------------------------------------------------------------------
@@ -647,6 +669,14 @@ def main():
     achieved = sb[dom] / (avg[dom] / 1e3) / 1e9
     join_bytes = 8 * (nr + ns) + 8 * st.count
     join_gbs = join_bytes / (ms_step / 1e3) / 1e9
+    # The level-2 Bloom pass reads one filter word pair per S key from L2 at a hashed position: its
+    # ceiling is the rate of such reads, measured here outside the timed region (2 MB table).
+    gather = None
+    if blvl == 2 and "s_l2_hist" in avg:
+        gather = gather_peak(bj, torch, stream)
+        keys_per_s = ns / (avg["s_l2_hist"] / 1e3)
+        gather.update({"kernel": "s_l2_hist", "achieved_reads_per_s": keys_per_s,
+                       "frac": keys_per_s / gather["peak_reads_per_s"]})
 
     # end to end through the host-array entry point: pinned host inputs in, pairs out
     e2e = None
@@ -742,6 +772,7 @@ def main():
                          "peak_kind": peak_kind},
             "join_roofline": {"algorithmic_bytes": join_bytes, "achieved": join_gbs, "peak": peak,
                               "frac": join_gbs / peak, "unit": "GB/s"},
+            "bloom_read_roofline": gather,
             "stage_ms": {k: round(v, 4) for k, v in avg.items()},
             "matches": st.count, "s_survivors": st.s_survivors,
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),

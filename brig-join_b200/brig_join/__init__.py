@@ -190,6 +190,7 @@ def lib() -> C.CDLL:
     L.brig_join_last_error.restype = C.c_char_p
     L.brig_join_kernel_launches.argtypes = []
     L.brig_join_kernel_launches.restype = C.c_int64
+    L.brig_join_gather_rate.argtypes = [vp, C.c_int64, C.c_int64, vp, _i64p, vp]
     if hasattr(L, "brig_serve_create"):
         L.brig_serve_create.argtypes = [C.POINTER(Config), C.POINTER(ServeConfig), C.POINTER(vp)]
         L.brig_serve_submit.argtypes = [vp, C.POINTER(ServeRequest), _i64p]
@@ -428,3 +429,12 @@ def gen_device(seed: int, n_r: int, n_s: int, match_frac, zipf_s, r_key, r_val, 
 
 def kernel_launches() -> int:
     return int(lib().brig_join_kernel_launches())
+
+
+def gather_rate(table, loads: int, sink, stream=None) -> int:
+    """Enqueues the random-read kernel over the device tensor `table` (a power-of-two byte size);
+    returns the number of 8-byte reads it performs. Time it with events around the call."""
+    issued = C.c_int64()
+    check(lib().brig_join_gather_rate(_ptr(table), table.numel() * table.element_size(), loads, _ptr(sink),
+                                      C.byref(issued), _ptr(stream)), "brig_join_gather_rate")
+    return int(issued.value)

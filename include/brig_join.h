@@ -320,6 +320,17 @@ const char* brig_join_last_error(void);
 /* Number of kernel launches issued by this thread since process start (all handles). */
 int64_t brig_join_kernel_launches(void);
 
+/* Measurement helper, with no counterpart in the reference: enqueues on `stream` one kernel that
+ * performs about `loads` independent 8-byte reads at pseudo-random positions of `table` (a device
+ * array of `table_bytes` bytes, a power of two of at least 256, 8-byte aligned; small enough to stay
+ * in L2, like one level-1 partition's Bloom segments) and nothing else, two 512-thread CTAs per SM.
+ * The reads each touch their own cache line, as the level-2 Bloom probe's filter reads do, so the
+ * kernel's rate (time it with events around the call) is the ceiling of that probe. *loads_issued
+ * receives the exact number of reads enqueued; `sink` (one device word) is written only if the
+ * reads' checksum hits one fixed value. */
+int brig_join_gather_rate(const void* table, int64_t table_bytes, int64_t loads, uint32_t* sink,
+                          int64_t* loads_issued, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -314,3 +314,17 @@ def test_bounded_waits_report_internal_error_and_stay_exact(bj, oracle, torch_cu
                       exp_r, exp_s)
     st = _parity(bj, oracle, torch_cuda, rk, rv, sk, sv, use_bloom=1, partition_size=16, second_partition_size=8)
     assert st.count == n
+
+
+def test_gather_rate_helper(bj, torch_cuda):
+    """brig_join_gather_rate (the benchmark's ceiling for the level-2 Bloom probe's filter reads)
+    enqueues one kernel of the requested size and rejects tables that are not a power of two."""
+    table = torch_cuda.arange(1 << 18, dtype=torch_cuda.int32, device="cuda")
+    sink = torch_cuda.zeros(1, dtype=torch_cuda.int32, device="cuda")
+    n0 = bj.kernel_launches()
+    issued = bj.gather_rate(table, 1 << 24, sink)
+    torch_cuda.cuda.synchronize()
+    assert bj.kernel_launches() - n0 == 1
+    assert (1 << 23) < issued <= (1 << 24)
+    with pytest.raises(bj.BrigError):
+        bj.gather_rate(table[:1000], 1 << 20, sink)
