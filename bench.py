@@ -404,13 +404,15 @@ def run_sweep_workload(args):
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
     rows = []
-    for frac in (0.001, 0.01, 0.1, 1.0):
+    fracs = [float(x) for x in args.fracs.split(",")] if args.fracs else [0.001, 0.01, 0.1, 1.0]
+    bpks = [float(x) for x in args.bpks.split(",")] if args.bpks else [0, 8.0, 10.0, 14.0]
+    for frac in fracs:
         bj.gen_device(7, nr, ns, frac, 0.0, rk, rv, sk, sv, stream=sp)
         m = int(math.floor(frac * ns))
         cap = m + 4096
         out_r = torch.empty(cap, dtype=i32, device="cuda")
         out_s = torch.empty(cap, dtype=i32, device="cuda")
-        for bpk in (0, 8.0, 10.0, 14.0):
+        for bpk in bpks:
             kw = dict(use_bloom=1, bloom_bits_per_key=bpk) if bpk else dict(use_bloom=0)
             with bj.Join(**kw) as j:
                 for _ in range(max(args.warmup, 1)):
@@ -544,6 +546,8 @@ def main():
     ap.add_argument("--pool", type=int, default=24, help="serve workload: distinct requests")
     ap.add_argument("--requests", type=int, default=64, help="serve workload: requests per load point")
     ap.add_argument("--rates", default="20,80,320,1280", help="serve workload: offered loads (requests/s)")
+    ap.add_argument("--fracs", default="", help="sweep workload: match fractions (comma-separated)")
+    ap.add_argument("--bpks", default="", help="sweep workload: Bloom bits per key, 0 = no filter (comma-separated)")
     ap.add_argument("--streams", type=int, default=3, help="serve workload: concurrent waves")
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

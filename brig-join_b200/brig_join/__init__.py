@@ -41,6 +41,7 @@ STATUS_NAMES = {
 }
 PART_HASH = 0
 PART_MODULO = 1
+BLOOM_ADAPTIVE = 2  # use_bloom: the filter, switched off while it lets more than 30% of S through
 ABI_VERSION = 1
 NUM_STAGES = 13
 NOALLOC_MAX_TUPLES = 262144
@@ -191,6 +192,8 @@ def lib() -> C.CDLL:
     L.brig_join_kernel_launches.argtypes = []
     L.brig_join_kernel_launches.restype = C.c_int64
     L.brig_join_gather_rate.argtypes = [vp, C.c_int64, C.c_int64, vp, _i64p, vp]
+    L.brig_join_read_relation.argtypes = [C.c_char_p, C.c_int64, C.c_int32, C.c_uint32, vp, vp]
+    L.brig_join_write_pairs.argtypes = [C.c_char_p, vp, vp, vp, C.c_int64]
     if hasattr(L, "brig_serve_create"):
         L.brig_serve_create.argtypes = [C.POINTER(Config), C.POINTER(ServeConfig), C.POINTER(vp)]
         L.brig_serve_submit.argtypes = [vp, C.POINTER(ServeRequest), _i64p]
@@ -429,6 +432,29 @@ def gen_device(seed: int, n_r: int, n_s: int, match_frac, zipf_s, r_key, r_val, 
 
 def kernel_launches() -> int:
     return int(lib().brig_join_kernel_launches())
+
+
+def read_relation(path: str, n: int, read_val: bool = False, val_base: int = 1):
+    """One relation in the reference's input layout: (keys, values) as uint32 arrays; without a value
+    block the values are val_base + row (the reference uses 1 for R, 100000001 for S)."""
+    import numpy as np
+    k = np.empty(n, np.uint32)
+    v = np.empty(n, np.uint32)
+    check(lib().brig_join_read_relation(os.fsencode(path), n, 1 if read_val else 0, val_base,
+                                        k.ctypes.data, v.ctypes.data), "brig_join_read_relation")
+    return k, v
+
+
+def write_pairs(path: str, r_val, s_val, key=None) -> None:
+    """Writes pairs in the reference's headerless int32 block layout (keys, R values, S values)."""
+    import numpy as np
+    r = np.ascontiguousarray(r_val, np.uint32)
+    s = np.ascontiguousarray(s_val, np.uint32)
+    k = None if key is None else np.ascontiguousarray(key, np.uint32)
+    if len(r) != len(s) or (k is not None and len(k) != len(r)):
+        raise ValueError("pair arrays differ in length")
+    check(lib().brig_join_write_pairs(os.fsencode(path), None if k is None else k.ctypes.data, r.ctypes.data,
+                                      s.ctypes.data, len(r)), "brig_join_write_pairs")
 
 
 def gather_rate(table, loads: int, sink, stream=None) -> int:

@@ -340,25 +340,11 @@ void gpu_main(std::vector<int>*, std::vector<int>*, const std::string& r_inputPa
         return;
     }
     std::vector<int> tk(R), tv(R), sk(S), sv(S);
-    {
-        std::ifstream rf(r_inputPath, std::ios::binary), sf(s_inputPath, std::ios::binary);
-        if (!rf.is_open() || !sf.is_open()) {
-            fprintf(stderr, "[brig compat] gpu_main: failed to open input files\n");
-            return;
-        }
-        rf.read(reinterpret_cast<char*>(tk.data()), (std::streamsize)(4 * R));
-        sf.read(reinterpret_cast<char*>(sk.data()), (std::streamsize)(4 * S));
-        if (read_val) {
-            rf.read(reinterpret_cast<char*>(tv.data()), (std::streamsize)(4 * R));
-            sf.read(reinterpret_cast<char*>(sv.data()), (std::streamsize)(4 * S));
-        } else {
-            for (long long i = 0; i < R; ++i) tv[i] = (int)i + 1;
-            for (long long i = 0; i < S; ++i) sv[i] = (int)i + 100000001;
-        }
-        if (!rf || !sf) {
-            fprintf(stderr, "[brig compat] gpu_main: input shorter than the given sizes\n");
-            return;
-        }
+    auto u32 = [](std::vector<int>& v) { return reinterpret_cast<uint32_t*>(v.data()); };
+    if (brig_join_read_relation(r_inputPath.c_str(), R, read_val ? 1 : 0, 1u, u32(tk), u32(tv)) != BRIG_OK ||
+        brig_join_read_relation(s_inputPath.c_str(), S, read_val ? 1 : 0, 100000001u, u32(sk), u32(sv)) != BRIG_OK) {
+        fprintf(stderr, "[brig compat] gpu_main: %s\n", brig_join_last_error());
+        return;
     }
     if (sanityCheck && run_sanity_check) run_sanity_check(tk.data(), R, sk.data(), S);
     brig_join_config cfg;

@@ -182,6 +182,21 @@ private:
     unsigned long long* d_gwords_ = nullptr;
     int nj_ = 0;
 
+    // The adaptive filter (use_bloom == BRIG_BLOOM_ADAPTIVE, single joins): the survivor count of
+    // the last filtered run comes back into pinned memory behind the run; while the last measured
+    // share of S passing the filter is above the break-even, runs plan without the filter, and every
+    // kBloomRetest-th of them tests it again.
+    int64_t* surv_host_ = nullptr;
+    cudaEvent_t surv_ev_ = nullptr;
+    bool surv_pending_ = false;
+    int64_t surv_ns_ = 0;
+    bool bloom_off_ = false;
+    int runs_off_ = 0;
+    // The configuration the next run of `nj` joins plans with.
+    brig_join_config adapt_config(int nj);
+    // Queues the read-back of a filtered single join's survivor count (adaptive filter only).
+    void note_survivors(const std::vector<JoinPlan>& plans, const int64_t* counters, cudaStream_t stream);
+
     // Stage events of the last kStageRing runs (profile_stages): run i records into set i % ring.
     static constexpr int kStageRing = 64;
     cudaEvent_t stage_ev_[kStageRing][kNumStages + 1] = {};

@@ -49,6 +49,9 @@ enum brig_status {
  *                   (src/kernel_functions.cu:66,121 first level; :187,238 second level). */
 enum brig_partition_mode { BRIG_PART_HASH = 0, BRIG_PART_MODULO = 1 };
 
+/* use_bloom values beyond the reference's on/off (see brig_join_config.use_bloom). */
+#define BRIG_BLOOM_ADAPTIVE 2
+
 /* Join configuration. Fields map onto the reference's gpu_main arguments and CLI flags
  * (src/hash_kernel.h:21-34, src/driver.cpp:66-94); zero means "choose automatically". */
 typedef struct brig_join_config {
@@ -58,7 +61,11 @@ typedef struct brig_join_config {
     int32_t second_partition_size;  /* second-level fan-out P2 (--second_partition_size); 0 = auto,
                                        1 = single level */
     int32_t use_bloom;              /* 0 = no prefilter (use_bf 0); 1 = partitioned Bloom filter on R
-                                       probed in S's first partition pass (use_bf 10/14) */
+                                       probed in S's first partition pass (use_bf 10/14);
+                                       BRIG_BLOOM_ADAPTIVE = as 1, but a handle whose filtered
+                                       single join let more than 30% of S through runs its next joins
+                                       without the filter (there it costs more than it saves),
+                                       testing it again every 16th run */
     int32_t bloom_num_hashes;       /* k (--num_hashes); 0 = round(bits_per_key * ln 2), max 16 */
     double  bloom_bits_per_key;     /* filter size when bloom_num_bits == 0; default 10 */
     int64_t bloom_num_bits;         /* total filter bits (--num_bits); 0 = bits_per_key * |R| */
@@ -313,6 +320,21 @@ int brig_join_run_noalloc(const brig_join_config* cfg,
                           const uint32_t* r_key, const uint32_t* r_val, int64_t n_r,
                           const uint32_t* s_key, const uint32_t* s_val, int64_t n_s,
                           const brig_join_output* out, void* stream);
+
+/* ---- The reference's file formats (host arrays, no device work) -------------------------------
+ * Reads one relation in the reference's input layout: headerless little-endian int32, the n keys
+ * followed, when read_val is 1, by the n values (datagen/gen_dataset.cpp writes the key block;
+ * gpu_main reads both blocks with --read_val 1, src/hash_kernel.cu:300-335). With read_val 0 and
+ * vals not NULL, vals[i] = val_base + i: the reference's synthesised payloads are row + 1 for R
+ * (val_base 1) and row + 100000001 for S. BRIG_E_INVALID when the file is shorter than asked. */
+int brig_join_read_relation(const char* path, int64_t n, int32_t read_val, uint32_t val_base,
+                            uint32_t* keys, uint32_t* vals);
+
+/* Writes n pairs to `path` in the same headerless int32 block layout: the keys (when key is not
+ * NULL), then the R values, then the S values. The reference parses an output path and never
+ * writes it (src/driver.cpp:50,119); this is the writer it lacks. */
+int brig_join_write_pairs(const char* path, const uint32_t* key, const uint32_t* r_val, const uint32_t* s_val,
+                          int64_t n);
 
 /* Message for the last failed call on this thread (empty string if none). */
 const char* brig_join_last_error(void);

@@ -1,6 +1,7 @@
 """C-ABI checks that need no GPU: the library loads and exports every declared function, the
 planner's fan-outs, argument validation, error reporting without a device, and the host generator."""
 import ctypes as C
+import os
 import subprocess
 
 import numpy as np
@@ -164,3 +165,35 @@ def test_planner_partition_fill_and_slices(bj):
     assert p_full[0] == p_default[0] and 2 * p_full[1] == p_default[1]
     with pytest.raises(bj.BrigError):
         bj.plan(1 << 20, 1 << 20, partition_fill=101)
+
+
+def test_reference_file_formats_round_trip(bj, tmp_path):
+    """brig_join_read_relation reads the reference's input layout (key block, then the value block
+    with --read_val 1; synthesised row + base values without it) and brig_join_write_pairs writes the
+    pairs in the same headerless int32 block layout; host code only, no GPU."""
+    rng = np.random.default_rng(3)
+    keys = rng.integers(0, 2**32, 1000, dtype=np.uint64).astype(np.uint32)
+    vals = rng.integers(0, 2**32, 1000, dtype=np.uint64).astype(np.uint32)
+    f = str(tmp_path / "R.bin")
+    np.concatenate([keys, vals]).tofile(f)
+    k, v = bj.read_relation(f, 1000, read_val=True)
+    assert np.array_equal(k, keys) and np.array_equal(v, vals)
+    k, v = bj.read_relation(f, 1000, read_val=False, val_base=100000001)
+    assert np.array_equal(k, keys) and np.array_equal(v, np.arange(1000, dtype=np.uint32) + 100000001)
+    with pytest.raises(bj.BrigError):
+        bj.read_relation(f, 1500, read_val=True)  # 3000 words asked of a 2000-word file
+    out = str(tmp_path / "pairs.bin")
+    bj.write_pairs(out, vals[:10], keys[:10], key=keys[5:15])
+    assert np.array_equal(np.fromfile(out, np.uint32), np.concatenate([keys[5:15], vals[:10], keys[:10]]))
+    bj.write_pairs(out, vals[:0], keys[:0])
+    assert np.fromfile(out, np.uint32).size == 0
+
+
+def test_golden_fixtures_read_as_the_reference_reads_them(bj):
+    import json
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    for case in json.load(open(os.path.join(golden, "manifest.json"))):
+        path = os.path.join(golden, case["r_file"])
+        k, v = bj.read_relation(path, case["R"], read_val=False, val_base=1)
+        assert np.array_equal(k, np.fromfile(path, np.uint32)[:case["R"]])
+        assert v[0] == 1 and v[-1] == case["R"]

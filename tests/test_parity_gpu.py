@@ -328,3 +328,26 @@ def test_gather_rate_helper(bj, torch_cuda):
     assert (1 << 23) < issued <= (1 << 24)
     with pytest.raises(bj.BrigError):
         bj.gather_rate(table[:1000], 1 << 20, sink)
+
+
+def test_adaptive_bloom_switches_off_and_retests(bj, oracle, torch_cuda):
+    """use_bloom = BLOOM_ADAPTIVE: a run whose filter lets more than 30% of S through turns the filter
+    off for the handle's next single joins, every 16th of which tests it again; once a test run
+    sees few survivors the filter stays on. Every run is exact."""
+    hi = bj.gen_host(71, 200_000, 300_000, 0.6)   # 60% of S matches: the filter does not pay
+    lo = bj.gen_host(72, 200_000, 300_000, 0.05)  # 5% matches: it does
+    exp = {id(x): oracle.pairs(*x) for x in (hi, lo)}
+    with bj.Join(use_bloom=bj.BLOOM_ADAPTIVE) as j:
+        def run(data):
+            st, r, s, _ = run_device(bj, torch_cuda, *data, cap=len(data[2]), handle=j)
+            er, es = exp[id(data)]
+            assert st.count == len(er)
+            assert_same_pairs(oracle, r, s, er, es)
+            return st.bloom_num_hashes > 0, st.s_survivors
+        on, surv = run(hi)  # first run filtered: its survivors (> 30%) come back behind it
+        assert on and surv > 0.3 * len(hi[2])
+        states = [run(hi)[0] for _ in range(16)]  # runs 2..17: off, except the 16th (a re-test)
+        assert states == [False] * 15 + [True]
+        states = [run(lo)[0] for _ in range(16)]  # runs 18..33: off until the re-test at 33
+        assert states == [False] * 15 + [True]
+        assert run(lo)[0] and run(lo)[0]  # the re-test saw 5% survivors: the filter stays on
