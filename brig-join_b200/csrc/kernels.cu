@@ -1497,12 +1497,11 @@ __device__ __forceinline__ void scan_dir(uint32_t* off, uint32_t nb, uint32_t* t
 //     tuple's rank in its bucket), scans the counts into bucket starts (off[nb] = the chunk size)
 //     and places every tuple at off[bucket] + rank: a bucketised table with at least as many
 //     buckets as tuples, bucket b = [off[b], off[b+1]). Every build key also sets one bit of a
-//     131072-bit presence bitmap;
-//   * streams the other side: its first kProbeFirst tuples from shared memory, where a bulk copy
-//     issued at the start of the task has put them while the table was built, the rest straight
-//     from global memory with kProbeU coalesced tuples per thread in flight (and the range two
-//     iterations ahead prefetched into L2). A streamed tuple whose bitmap bit is clear cannot match
-//     (at most 4096 keys set at most 3% of the bits); the others are compacted with ballot/popc into
+//     262144-bit presence bitmap;
+//   * streams the other side from global memory with kProbeU coalesced tuples per thread in flight
+//     (its first two iterations are prefetched into L2 while the table is built, and later the
+//     range two iterations ahead). A streamed tuple whose bitmap bit is clear cannot match (at
+//     most 4096 keys set at most 1.6% of the bits); the others are compacted with ballot/popc into
 //     the warp's candidate queue in shared memory. Every 32 queued candidates the warp scans their
 //     buckets in lock step, one candidate per lane, and compacts matches into the warp's output
 //     staging buffer, which is written out with one global atomic per flush. So the bucket scans,
@@ -1511,11 +1510,13 @@ __device__ __forceinline__ void scan_dir(uint32_t* off, uint32_t nb, uint32_t* t
 // keys of one task share the top bits of mix32) and of the bucket bits.
 constexpr int kProbeU = 4;                        // streamed tuples per thread in flight
 constexpr int kBuildPer = kMaxTable / kThreads;   // build tuples per thread
-constexpr int kBitmapWords = 4096;                // 131072-bit presence bitmap (3% false candidates at 4096 keys, against 6% at 65536 bits: probe 2.15 against 2.22 ms at 640M)
+// 262144-bit presence bitmap: 1.6% false candidates at 4096 keys, against 3% at 131072 bits and 6%
+// at 65536 (probe at 640M x 640M: 2.02, 2.10 and 2.22 ms). Its 16 KB more shared memory come from the
+// buffer that held the first 2048 streamed tuples of a task, which the L2 prefetch replaces.
+constexpr int kBitmapWords = 8192;
 constexpr int kQueue = 64;                        // candidates queued per warp
-constexpr int kProbeFirst = 2048;                 // first probe-side tuples of a task, bulk-copied
 
-__device__ __forceinline__ uint32_t presence_bit(uint32_t key) { return (key * 0x9E3779B1u) >> 15; }
+__device__ __forceinline__ uint32_t presence_bit(uint32_t key) { return (key * 0x9E3779B1u) >> 14; }
 
 // Output staging of one warp: the pairs found so far for join `d`.
 struct WarpOut {
@@ -1622,9 +1623,9 @@ __device__ __forceinline__ void probe_candidates(const JoinDesc& d, const uint2*
     }
 }
 
-// Streams tuples [0, n) of `src` (shared memory when kShared, else global) through the filter and
+// Streams tuples [0, n) of `src` (global memory) through the filter and
 // the warp's candidate queue; full warps of candidates are probed as they form.
-template <bool kShared, int U, bool kGuard>
+template <int U, bool kGuard>
 __device__ __forceinline__ void probe_step(const JoinDesc& d, const uint2* __restrict__ src, uint32_t base, uint32_t n,
                                            const uint32_t* bitmap, uint2* q, int& qn, const uint2* table,
                                            const uint32_t* off, uint32_t mask, bool bs, int emit_key, int lane,
@@ -1633,8 +1634,7 @@ __device__ __forceinline__ void probe_step(const JoinDesc& d, const uint2* __res
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const uint32_t i = base + u * kThreads + threadIdx.x;
-        if (kShared) e[u] = (!kGuard || i < n) ? src[i] : make_uint2(0u, 0u);
-        else e[u] = (!kGuard || i < n) ? __ldcs(src + i) : make_uint2(0u, 0u);
+        e[u] = (!kGuard || i < n) ? __ldcs(src + i) : make_uint2(0u, 0u);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -1659,7 +1659,7 @@ __device__ __forceinline__ void probe_step(const JoinDesc& d, const uint2* __res
     }
 }
 
-template <bool kShared, int U>
+template <int U>
 __device__ __forceinline__ void probe_stream(const JoinDesc& d, const uint2* __restrict__ src, uint32_t n,
                                              const uint32_t* bitmap, uint2* q, int& qn, const uint2* table,
                                              const uint32_t* off, uint32_t mask, bool bs, int emit_key, int lane,
@@ -1668,11 +1668,11 @@ __device__ __forceinline__ void probe_stream(const JoinDesc& d, const uint2* __r
     uint32_t base = 0;
     for (; base + kStep <= n; base += kStep) {
         // streamed from global memory: keep the range two iterations ahead on its way into L2
-        if (!kShared && threadIdx.x == 0 && base + 2 * kStep < n)
+        if (threadIdx.x == 0 && base + 2 * kStep < n)
             prefetch_l2_range(src + base + 2 * kStep, src + min_i64((int64_t)n, (int64_t)base + 3 * kStep));
-        probe_step<kShared, U, false>(d, src, base, n, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
+        probe_step<U, false>(d, src, base, n, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
     }
-    if (base < n) probe_step<kShared, U, true>(d, src, base, n, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
+    if (base < n) probe_step<U, true>(d, src, base, n, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
 }
 
 // A task of the probe queue with its join's buffers resolved: the build and streamed ranges.
@@ -1704,17 +1704,14 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         int table_cap, int emit_key) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint2* table = reinterpret_cast<uint2*>(smem);                              // [table_cap]
-    uint2* pbuf = table + table_cap;                                            // [kProbeFirst + 2]
-    uint2* queue = pbuf + kProbeFirst + 2;                                      // [warps][kQueue]
+    uint2* queue = table + table_cap;                                           // [warps][kQueue]
     uint32_t* bitmap = reinterpret_cast<uint32_t*>(queue + (kThreads / 32) * kQueue);  // [kBitmapWords]
     uint32_t* off = bitmap + kBitmapWords;                                      // [table_cap + 1] (+pad)
     uint32_t* wbuf = off + table_cap + 4;
     __shared__ uint32_t tmp[kThreads / 32];
     __shared__ long long s_task[2];
     __shared__ ProbeTask s_info[2];  // the current task and the next one, resolved by thread 0
-    __shared__ __align__(8) uint64_t bar;
     unsigned long long* errors = &gwords[kGErrors];
-    const uint32_t polls = wait_polls(gwords);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int words_per_warp = kWarpBuf * (emit_key ? 3 : 2);
     WarpOut o;
@@ -1724,14 +1721,11 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
     o.count = 0;
     uint2* q = queue + wid * kQueue;
     int cur = -1;
-    uint32_t ph = 0;
     const long long ntasks = (long long)gwords[kGTasks];
     if (threadIdx.x == 0) {
         const long long t0 = (long long)atomicAdd(&gwords[kGQueue], 1ull);
         s_task[0] = t0;
         resolve_task(J, tasks, t0, ntasks, s_info[0]);
-        mbar_init(&bar, 1);
-        mbar_init_fence();
     }
     __syncthreads();
     for (int slot = 0;; slot ^= 1) {
@@ -1743,13 +1737,9 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         const uint2* __restrict__ bsrc = tk.bsrc;
         const uint2* __restrict__ psrc = tk.psrc;
         const uint32_t pn = tk.p_len;
-        const uint32_t first = pn < (uint32_t)kProbeFirst ? pn : (uint32_t)kProbeFirst;
-        // the first probe chunk is copied into shared memory while the table is built
         if (threadIdx.x == 0) {
-            PackedTiles{psrc}.issue(0, (int)first, reinterpret_cast<unsigned char*>(pbuf), &bar);
-            // the first two global iterations of the probe side go to L2 while the table is built
-            if (pn > first)
-                prefetch_l2_range(psrc + first, psrc + min_i64((int64_t)pn, (int64_t)first + 2 * kProbeU * kThreads));
+            // the first two iterations of the probe side go to L2 while the table is built
+            prefetch_l2_range(psrc, psrc + min_i64((int64_t)pn, (int64_t)2 * kProbeU * kThreads));
             s_task[slot ^ 1] = (long long)atomicAdd(&gwords[kGQueue], 1ull);  // resolved after the probe
         }
         if (tk.join != cur) {
@@ -1765,7 +1755,7 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
         uint32_t nb = 32;
         while (nb < (uint32_t)nr) nb <<= 1;
         const uint32_t mask = nb - 1;
-        // the previous task's probe is done with table, off, bitmap and pbuf
+        // the previous task's probe is done with table, off and bitmap
         for (uint32_t i = threadIdx.x; i <= nb; i += kThreads) off[i] = 0;
         for (int i = threadIdx.x; i < kBitmapWords; i += kThreads) bitmap[i] = 0;
         // ---- build: count per bucket (the atomic's result is the rank), set the bitmap bits
@@ -1798,15 +1788,10 @@ k_probe(const JoinDesc* __restrict__ J, const Task* __restrict__ tasks, unsigned
             const int i = k * kThreads + threadIdx.x;
             if (i < nr) table[off[br[k] >> 16] + (br[k] & 0xffffu)] = __ldg(bsrc + i);
         }
-        mbar_wait(&bar, ph, errors, polls);
-        ph ^= 1u;
         __syncthreads();
-        // ---- probe: the first chunk from shared memory, the rest straight from global memory
+        // ---- probe: the other side streamed from global memory
         int qn = 0;  // candidates in this warp's queue (warp-uniform)
-        probe_stream<true, 2>(d, pbuf + PackedTiles{psrc}.mis(0), first, bitmap, q, qn, table, off, mask, bs,
-                           emit_key, lane, o);
-        if (pn > first)
-            probe_stream<false, kProbeU>(d, psrc + first, pn - first, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
+        probe_stream<kProbeU>(d, psrc, pn, bitmap, q, qn, table, off, mask, bs, emit_key, lane, o);
         if (qn > 0) probe_candidates(d, q, qn, table, off, mask, bs, emit_key, lane, o);
         // the next task's record and buffers, read while the other warps finish this task, and its
         // build chunk on its way into L2
@@ -1935,7 +1920,7 @@ cudaError_t enqueue_scan(const uint32_t* in, int64_t* out, int64_t n, int64_t* t
 }
 
 size_t probe_smem_bytes(int table_cap, int emit_key) {
-    return (size_t)table_cap * 8 + (size_t)(kProbeFirst + 2) * 8 + (size_t)(kThreads / 32) * kQueue * 8 +
+    return (size_t)table_cap * 8 + (size_t)(kThreads / 32) * kQueue * 8 +
            (size_t)kBitmapWords * 4 +
            ((size_t)table_cap + 4) * 4 +
            (size_t)(kThreads / 32) * kWarpBuf * (emit_key ? 3 : 2) * 4;

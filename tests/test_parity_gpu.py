@@ -293,7 +293,7 @@ def test_config0_16M_x_16M(bj, oracle, torch_cuda, preset):
 
 def test_bounded_waits_report_internal_error_and_stay_exact(bj, oracle, torch_cuda):
     """wait_poll_limit = -1 gives every bounded wait of the kernels (the bulk-copy mbarriers of the
-    scatters and the probe) no polls: each one counts a device-side error at once and then waits
+    scatters) no polls: each one counts a device-side error at once and then waits
     for its copy with the default bound. The run must end (no hang), report BRIG_E_INTERNAL, publish
     -1 as the device count, keep its pairs exact, and leave the context usable for the next run."""
     rk, rv, sk, sv = bj.gen_host(77, 300_000, 400_000, 0.2)
