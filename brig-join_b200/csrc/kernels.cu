@@ -1011,7 +1011,10 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 // load and a two-word test; full groups of U keys per thread run without bounds tests. Survivors
 // are re-ranked per warp with one ballot per key and one shared atomic per warp group, and their
 // level-2 ids recomputed (about one key in nine survives at 10% matches).
-constexpr int kL2BloomU = 6;  // keys per thread with their filter words in flight
+// Keys per thread with their filter words in flight. Each group also loads the next group's tuples
+// before it reads its own filter words, so the stream's DRAM latency overlaps the filter reads (at
+// 640M keys: 3.07 ms against 3.22 ms with six keys and no look-ahead).
+constexpr int kL2BloomU = 4;
 
 // One group of U keys per thread starting at slice offset r0; kTail: the group may end past len.
 template <int M, int K, bool kTail>
@@ -1019,13 +1022,17 @@ __device__ __forceinline__ void l2_bloom_group(const uint2* __restrict__ src, in
                                                const uint32_t* __restrict__ bloom, uint32_t seg_blocks,
                                                uint32_t fine0, const PartFn& pf, const uint2* pat,
                                                uint2* __restrict__ cmp, uint32_t* cnt,
-                                               uint32_t* s_surv, unsigned long long* errors, int lane) {
+                                               uint32_t* s_surv, unsigned long long* errors, int lane,
+                                               uint2 (&e)[kL2BloomU]) {
     constexpr int U = kL2BloomU;
-    uint2 e[U];
+    // the next group's tuples, loaded while this group's filter words are read
+    uint2 ne[U];
+    if constexpr (!kTail) {
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-        const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
-        e[u] = (!kTail || r < len) ? __ldcs(src + r) : make_uint2(0u, 0u);
+        for (int u = 0; u < U; ++u) {
+            const int32_t r = r0 + (U + u) * kThreads + (int32_t)threadIdx.x;
+            ne[u] = r < len ? __ldcs(src + r) : make_uint2(0u, 0u);
+        }
     }
     uint2 wv[U], mk[U];
 #pragma unroll
@@ -1069,6 +1076,10 @@ __device__ __forceinline__ void l2_bloom_group(const uint2* __restrict__ src, in
             base += __popc(bal[u]);
         }
     }
+    if constexpr (!kTail) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) e[u] = ne[u];
+    }
 }
 
 template <int M, int K>
@@ -1105,12 +1116,18 @@ k_l2_bloom(const JoinDesc* __restrict__ J, int nj, const int64_t* __restrict__ s
         const int32_t full = len - len % (U * kThreads);
         const uint32_t fine0 = x.p * P2;
         int32_t r0 = 0;
+        uint2 e[U];  // the tuples of the group in hand; each group loads the next one's
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int32_t r = u * kThreads + (int32_t)threadIdx.x;
+            e[u] = r < len ? __ldcs(src + r) : make_uint2(0u, 0u);
+        }
         for (; r0 < full; r0 += U * kThreads)
             l2_bloom_group<M, K, false>(src, r0, len, bloom, seg_blocks, fine0, pf, s_pat, cmp, cnt,
-                                     &s_surv, &gwords[kGErrors], lane);
+                                     &s_surv, &gwords[kGErrors], lane, e);
         if (r0 < len)
             l2_bloom_group<M, K, true>(src, r0, len, bloom, seg_blocks, fine0, pf, s_pat, cmp, cnt,
-                                    &s_surv, &gwords[kGErrors], lane);
+                                    &s_surv, &gwords[kGErrors], lane, e);
         __syncthreads();
         uint32_t* H = hist2 + R.h2_base + x.local_off * P2;
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) H[(int64_t)q * x.ns + x.sl] = cnt[q];
