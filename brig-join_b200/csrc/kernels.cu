@@ -765,13 +765,20 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
             uint2* __restrict__ cmp = R.cmp;
             const int32_t len = (int32_t)(e - b);  // a slice is far below 2^31 tuples
             const uint32_t* __restrict__ skey = key + b;
+            // each group loads the next group's keys before it reads its own filter words
+            uint32_t kk[kProbeILP];
+#pragma unroll
+            for (int u = 0; u < kProbeILP; ++u) {
+                const int32_t r = u * kThreads + (int32_t)threadIdx.x;
+                kk[u] = r < len ? __ldcs(skey + r) : 0u;
+            }
             for (int32_t r0 = 0; r0 < len; r0 += kProbeILP * kThreads) {
-                uint32_t kk[kProbeILP];
+                uint32_t nk[kProbeILP];
                 uint2 wv[kProbeILP], mk[kProbeILP];
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
-                    const int32_t r = r0 + u * kThreads + (int32_t)threadIdx.x;
-                    kk[u] = r < len ? __ldcs(skey + r) : 0u;
+                    const int32_t r = r0 + (kProbeILP + u) * kThreads + (int32_t)threadIdx.x;
+                    nk[u] = r < len ? __ldcs(skey + r) : 0u;
                 }
 #pragma unroll
                 for (int u = 0; u < kProbeILP; ++u) {
@@ -812,6 +819,8 @@ k_l1_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
                         base += __popc(bal[u]);
                     }
                 }
+#pragma unroll
+                for (int u = 0; u < kProbeILP; ++u) kk[u] = nk[u];
             }
         }
         __syncthreads();
