@@ -992,16 +992,25 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
         for (uint32_t q = threadIdx.x; q < P2; q += kThreads) cnt[q] = 0;
         __syncthreads();
         const uint2* __restrict__ l1 = R.l1;
+        // each group of eight keys per thread loads the next group before it counts its own
+        uint32_t kk[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int64_t i = begin + threadIdx.x + u * kThreads;
+            kk[u] = i < end ? __ldcs(&l1[i].x) : 0u;
+        }
         for (int64_t i0 = begin + threadIdx.x; i0 < end; i0 += 8 * kThreads) {
-            uint32_t kk[8];
+            uint32_t nk[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                const int64_t i = i0 + u * kThreads;
-                kk[u] = i < end ? __ldcs(&l1[i].x) : 0u;
+                const int64_t i = i0 + (8 + u) * kThreads;
+                nk[u] = i < end ? __ldcs(&l1[i].x) : 0u;
             }
 #pragma unroll
             for (int u = 0; u < 8; ++u)
                 if (i0 + u * kThreads < end) atomicAdd(&cnt[bin(kk[u])], 1u);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) kk[u] = nk[u];
         }
         __syncthreads();
         uint32_t* H = hist2 + R.h2_base + x.local_off * P2;
