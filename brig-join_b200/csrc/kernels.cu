@@ -8,8 +8,7 @@
 //   gpu_make_sorted_table_for_both (src/kernel_functions.cu:95-133)    -> k_l1_scatter
 //   gpu_run_hist_second_pass + gpu_build_table_second_pass_kv (src/kernel_functions.cu:163-281)
 //                                     -> k_l2_plan + k_l2_hist + k_l2_scatter + k_l2_bounds
-//   queryAndCompactKernelPartitioned, alternatively fused into S's level-2 histogram pass
-//                                                                            -> k_l2_hist (Bloom)
+//   queryAndCompactKernelPartitioned, alternatively as S's level-2 pass      -> k_l2_bloom
 //   insertKernelPartitioned (src/bloom.cu:698-722)                     -> k_bloom_build
 //   gpu_probe_with_second_pass / gpu_fused_probe_transfer local part
 //   (src/kernel_functions.cu:294-454, 612-789), including the split path (:356-395)
@@ -1023,12 +1022,13 @@ k_l2_hist(const JoinDesc* __restrict__ J, int nj, int rel, const int64_t* __rest
 // against the filter segment of its finest partition, and the survivors are compacted into
 // cmp[slice begin, + survivors) and counted by level-2 id. The filter segments of one level-1
 // partition are contiguous (1.5 MB at 640M keys, 10 bits/key) and the slices of neighbouring
-// partitions run together, so the filter words come from L2. The pass is bound by the integer ALU
-// pipe, so the per-key work is kept to the minimum: one mix of the key from which its level-2 id,
-// block, word pair (bloom_slot) and pattern index derive, one 8-byte filter load, one 8-byte pattern
-// load and a two-word test; full groups of U keys per thread run without bounds tests. Survivors
-// are re-ranked per warp with one ballot per key and one shared atomic per warp group, and their
-// level-2 ids recomputed (about one key in nine survives at 10% matches).
+// partitions run together, so the filter words come from L2. One random filter read per key bounds
+// the pass (the L1/texture pipeline looks up about one line per SM cycle), so the per-key work is
+// kept to the minimum: one mix of the key from which its level-2 id, block, word pair (bloom_slot)
+// and masks derive (compile-time shifts for k = 7, one 8-byte pattern look-up otherwise), one 8-byte
+// filter load and a two-word test; full groups of U keys per thread run without bounds tests.
+// Survivors are re-ranked per warp with one ballot per key and one shared atomic per warp group, and
+// their level-2 ids recomputed (about one key in nine survives at 10% matches).
 // Keys per thread with their filter words in flight. Each group also loads the next group's tuples
 // before it reads its own filter words, so the stream's DRAM latency overlaps the filter reads (at
 // 640M keys: 3.07 ms against 3.22 ms with six keys and no look-ahead).
