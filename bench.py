@@ -220,9 +220,9 @@ def stage_bytes(nr, ns, surv, matches, bloom_bits, bloom_level):
 # measured traffic to the benchmarked launch; the per-tuple traffic of these streaming kernels does
 # not depend on the relation size once the inputs exceed the L2.
 NCU_TRAFFIC_PER_TUPLE = {
-    "r_hist": (4.05, "nr"), "r_scatter": (15.93, "nr"), "r_l2_hist": (8.01, "nr"), "r_l2_scatter": (16.30, "nr"),
+    "r_hist": (4.05, "nr"), "r_scatter": (15.93, "nr"), "r_l2_hist": (8.05, "nr"), "r_l2_scatter": (16.30, "nr"),
     "bloom_build": (9.01, "nr"), "s_hist_probe": (4.01, "ns"), "s_scatter": (15.94, "ns"),
-    "s_l2_hist": (10.15, "ns"), "probe": (9.93, "nr"),
+    "s_l2_hist": (9.99, "ns"), "probe": (9.87, "nr"),
 }
 
 
