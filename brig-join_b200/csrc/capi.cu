@@ -193,6 +193,42 @@ static int finish_host_run(brig_join_t* h, uint32_t* out_r_val, uint32_t* out_s_
     return (int)BRIG_OK;
 }
 
+// The end of a host-array join with S in chunks: each chunk's pairs are copied back as soon as its
+// probe has ended, on a stream of their own, while later chunks are still copied in and joined.
+static int finish_chunked_run(brig_join_t* h, uint32_t* out_r_val, uint32_t* out_s_val, uint32_t* out_key,
+                              int64_t capacity, int64_t* count, cudaStream_t st) {
+    Engine& e = *h->eng;
+    auto& b = e.hio;
+    h->last_kind = 1;
+    h->last_items = 1;
+    int64_t done = 0;  // pairs whose copy is issued
+    for (int c = 0; c < e.chunks_run; ++c) {
+        brig::cuda_check(cudaEventSynchronize(e.chunk_done[c]), "cudaEventSynchronize");
+        const int64_t upto = std::min(e.chunk_count[c], capacity);
+        if (upto > done) {
+            const size_t n = (size_t)(upto - done) * 4;
+            brig::cuda_check(cudaMemcpyAsync(out_r_val + done, b.outr + done, n, cudaMemcpyDeviceToHost, e.d2h_stream),
+                             "D2H r_val");
+            brig::cuda_check(cudaMemcpyAsync(out_s_val + done, b.outs + done, n, cudaMemcpyDeviceToHost, e.d2h_stream),
+                             "D2H s_val");
+            if (out_key)
+                brig::cuda_check(cudaMemcpyAsync(out_key + done, b.outk + done, n, cudaMemcpyDeviceToHost, e.d2h_stream),
+                                 "D2H key");
+            done = upto;
+        }
+    }
+    std::vector<int64_t> c;
+    int64_t errors = 0;
+    e.sync_counters(c, errors);
+    brig::cuda_check(cudaStreamSynchronize(e.d2h_stream), "cudaStreamSynchronize");
+    brig::cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    if (errors) fail(BRIG_E_INTERNAL, "device-side consistency check failed");
+    const int64_t cnt = c[brig::kCntMatches];
+    if (count) *count = cnt;
+    if (cnt > capacity) return (int)set_error(BRIG_E_OVERFLOW, "match count exceeds output capacity");
+    return (int)BRIG_OK;
+}
+
 int brig_join_run_host(brig_join_t* h, const uint32_t* r_key, const uint32_t* r_val, int64_t n_r,
                        const uint32_t* s_key, const uint32_t* s_val, int64_t n_s, uint32_t* out_r_val,
                        uint32_t* out_s_val, uint32_t* out_key, int64_t capacity, int64_t* count,
@@ -209,7 +245,7 @@ int brig_join_run_host(brig_join_t* h, const uint32_t* r_key, const uint32_t* r_
         const int chunks = e.config().s_chunks;
         if (chunks > 1 && n_r > 0 && n_s > 0) {
             e.run_host_chunked(r_key, r_val, n_r, s_key, s_val, n_s, chunks, capacity, out_key != nullptr, st);
-            return finish_host_run(h, out_r_val, out_s_val, out_key, capacity, count, st);
+            return finish_chunked_run(h, out_r_val, out_s_val, out_key, capacity, count, st);
         }
         e.ensure_host_io(n_r, n_s, capacity, out_key != nullptr);
         // Large inputs: S is copied on the engine's copy stream after R, while R's passes and the

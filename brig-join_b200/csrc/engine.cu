@@ -348,6 +348,9 @@ Engine::~Engine() {
     if (stage_free_) cudaEventDestroy(stage_free_);
     if (done_) cudaEventDestroy(done_);
     if (copy_stream) cudaStreamDestroy(copy_stream);
+    if (d2h_stream) cudaStreamDestroy(d2h_stream);
+    for (cudaEvent_t ev : chunk_done) cudaEventDestroy(ev);
+    if (chunk_count) cudaFreeHost(chunk_count);
     if (r_copied) cudaEventDestroy(r_copied);
     if (s_copied) cudaEventDestroy(s_copied);
     for (int b = 0; b < 2; ++b) {
@@ -438,6 +441,19 @@ void Engine::run_host_chunked(const uint32_t* rk, const uint32_t* rv, int64_t nr
     const int64_t chunk = (ns + chunks - 1) / chunks;
     const int64_t nc = (ns + chunk - 1) / chunk;
     ensure_host_io(nr, 2 * chunk, cap, emit_key);  // waits for the handle's previous run
+    if (chunk_count_cap < nc) {
+        if (chunk_count) cudaFreeHost(chunk_count);
+        chunk_count = nullptr;
+        chunk_count_cap = 0;
+        cuda_check(cudaMallocHost(&chunk_count, (size_t)nc * sizeof(int64_t)), "cudaMallocHost");
+        chunk_count_cap = (int)nc;
+    }
+    while ((int64_t)chunk_done.size() < nc) {
+        cudaEvent_t ev;
+        cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        chunk_done.push_back(ev);
+    }
+    if (!d2h_stream) cuda_check(cudaStreamCreateWithFlags(&d2h_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     // One plan and one workspace layout for every chunk, sized by the largest chunk: R's buffers and
     // the filter stay where they are, and a smaller last chunk only leaves trailing slices empty.
     std::vector<JoinPlan> plans{plan_join(cfg_, nr, chunk)};
@@ -480,7 +496,12 @@ void Engine::run_host_chunked(const uint32_t* rk, const uint32_t* rv, int64_t nr
         cuda_check(cudaStreamWaitEvent(st, chunk_copied[b], 0), "cudaStreamWaitEvent");
         launch(JoinIO{hio.rk, hio.rv, dk, dv, nr, n, out}, kRunPartS | kRunProbe, true);
         cuda_check(cudaEventRecord(chunk_free[b], st), "cudaEventRecord");
+        // the pairs so far end at the match count (each chunk's probe appends after the previous one's)
+        cuda_check(cudaMemcpyAsync(chunk_count + c, counters + kCntMatches, sizeof(int64_t), cudaMemcpyDeviceToHost, st),
+                   "chunk count read-back");
+        cuda_check(cudaEventRecord(chunk_done[c], st), "cudaEventRecord");
     }
+    chunks_run = (int)nc;
     cuda_check(cudaEventRecord(done_, st), "cudaEventRecord");
     have_run_ = true;
     plans_ = plans;

@@ -151,6 +151,14 @@ public:
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t r_copied = nullptr, s_copied = nullptr;
     cudaEvent_t chunk_copied[2] = {}, chunk_free[2] = {};
+    // With S in chunks: the match count after chunk c's probe (pinned, chunk_count[c]) and an event
+    // after its read-back (chunk_done[c]), so each chunk's pairs can be copied back on d2h_stream
+    // while later chunks are copied in and joined (the link carries both directions at once).
+    std::vector<cudaEvent_t> chunk_done;
+    int64_t* chunk_count = nullptr;
+    int chunk_count_cap = 0;
+    int chunks_run = 0;
+    cudaStream_t d2h_stream = nullptr;
 
     // Host-array join with S in `chunks` pieces (brig_join_config.s_chunks): R is copied, partitioned
     // and filtered once; each S chunk is copied into one of two device buffers on copy_stream while
