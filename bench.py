@@ -6,7 +6,7 @@ Default workload: the full-size single join, |R| = |S| = 640,000,000 uint32 (key
 with 7 hashes. A step is one complete join (partition R and S, build and probe the Bloom filter,
 shared-memory hash build and probe, pair materialisation) over inputs resident in HBM.
 
-  python bench.py [--gpus N --steps K --warmup W] [--workload c1|c0|batch|serve|sweep] [--impl reference]
+  python bench.py [--gpus N --steps K --warmup W] [--workload c1|c0|batch|serve|sweep|shard] [--impl reference]
 
 One JSON line on rank 0. `value` is the device-timed join throughput (|R|+|S|)/t over all ranks;
 `e2e` the same metric through the host-array C entry point (H2D inputs, join, D2H pairs; S in
@@ -527,6 +527,109 @@ def serve_measure(pool_n, requests, rates, streams):
     }
 
 
+# ---- sharded join across GPUs ---------------------------------------------------------------------
+def run_shard_workload(args):
+    """The sharded join (brig_join.shard) on every rank of the job: one global pair of relations of
+    |R| = |S| = rows x ranks tuples (the device generator, 10% of S matching), each rank holding a
+    contiguous slice of both. A step is one ShardedJoin.run on every rank: R grouped by owner and
+    exchanged over NCCL, the owners' filters (10 bits/key, k = 7) built and gathered, S prefiltered,
+    grouped and exchanged, the local joins. Weak scaling: the rows per rank stay fixed. The first
+    run's global pair count is checked against the constructed match count. Also reported: the
+    R grouping kernels' bandwidth (key read for the counts; key and value read and written for the
+    scatter: 20 bytes per tuple) and the plain single-GPU join of one rank's slices."""
+    import datetime
+    import socket
+    import torch
+    import torch.distributed as dist
+    import brig_join as bj
+    import brig_join.shard as sh
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if "MASTER_ADDR" not in os.environ:
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(so.getsockname()[1])
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300),
+                            device_id=torch.device("cuda", local))
+    try:
+        n = args.rows if args.rows > 0 else 1 << 26
+        total = n * world
+        i32 = torch.int32
+        stream = torch.cuda.current_stream()
+        g = [torch.empty(total, dtype=i32, device="cuda") for _ in range(4)]
+        bj.gen_device(42, total, total, 0.1, 0.0, *g, stream=stream.cuda_stream)
+        rk, rv, sk, sv = (t[rank * n:(rank + 1) * n].clone() for t in g)
+        m = int(math.floor(0.1 * total))
+        job = sh.ShardedJoin(sh.TorchComm(), bits_per_key=10.0, num_hashes=7)
+        ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+        for w in range(max(args.warmup, 1)):
+            x = job.run(rk, rv, sk, sv)
+            if w == 0:  # values are global row numbers: every pair key-equal, every S row at most once
+                assert x.total == m, f"global count {x.total} != {m}"
+                r, s_ = x.r_val.long(), x.s_val.long()
+                assert bool((g[0][r] == g[2][s_]).all().item()), "pair check failed"
+                assert int(torch.unique(s_).numel()) == x.count, "an S row matched twice"
+                del r, s_, g
+            del x
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for _ in range(args.steps):
+            x = job.run(rk, rv, sk, sv)
+            del x
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / args.steps
+        # the R grouping kernels alone
+        ops = job.ops
+        for _ in range(3):
+            ops.split(world, rk, rv)
+        torch.cuda.synchronize()
+        a0, a1 = ev(), ev()
+        reps = 10
+        a0.record(stream)
+        for _ in range(reps):
+            ops.split(world, rk, rv)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        split_ms = a0.elapsed_time(a1) / reps
+        # the plain join of this rank's slices
+        cap = n + 4096
+        out_r = torch.empty(cap, dtype=i32, device="cuda")
+        out_s = torch.empty(cap, dtype=i32, device="cuda")
+        with bj.Join(use_bloom=1, bloom_bits_per_key=10.0, bloom_num_hashes=7) as jn:
+            for _ in range(3):
+                jn.run(rk, rv, n, sk, sv, n, out_r, out_s, cap, stream=stream.cuda_stream)
+            b0, b1 = ev(), ev()
+            b0.record(stream)
+            for _ in range(5):
+                jn.run(rk, rv, n, sk, sv, n, out_r, out_s, cap, stream=stream.cuda_stream)
+            b1.record(stream)
+            torch.cuda.synchronize()
+            plain_ms = b0.elapsed_time(b1) / 5
+        if rank == 0:
+            peak = peaks()[0]
+            split_gbs = 20.0 * n / (split_ms * 1e-3) / 1e9
+            line = {"metric": "sharded join tuples/s ((|R|+|S|)/t)", "value": 2 * total * 1e3 / ms, "unit": UNIT,
+                    "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+                    "higher_is_better": True, "scaling": "weak", "dtype": "u32", "data": "synthetic",
+                    "config": {"workload": f"sharded join {total} x {total} over {world} rank(s), 10% match, "
+                                           "owner filters 10 bits/key k=7", "rows_per_rank": n},
+                    "r_split_ms": round(split_ms, 3),
+                    "r_split_roofline": {"bound": "hbm", "achieved": round(split_gbs, 1), "peak": peak,
+                                         "unit": "GB/s", "frac": round(split_gbs / peak, 3),
+                                         "bytes_per_tuple": 20},
+                    "plain_join_ms_one_rank_slices": round(plain_ms, 3)}
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.destroy_process_group()
+    return 0
+
+
 def run_serve_workload(args):
     rates = [float(x) for x in args.rates.split(",")]
     print(json.dumps(serve_measure(args.pool, args.requests, rates, args.streams)), flush=True)
@@ -539,7 +642,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["batch", "serve", "sweep"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS) + ["batch", "serve", "sweep", "shard"])
     ap.add_argument("--joins", type=int, default=256, help="batch workload: number of joins")
     ap.add_argument("--batch-config", default="",
                     help="batch workload: a JSON object of configuration fields to use instead of autotuning")
@@ -574,6 +677,8 @@ def main():
         return run_sweep_workload(args)
     if args.workload == "serve":
         return run_serve_workload(args)
+    if args.workload == "shard":
+        return run_shard_workload(args)
     wl = dict(WORKLOADS[args.workload])
     if args.bloom is not None:
         wl["bloom"] = args.bloom

@@ -145,6 +145,12 @@ class ServeResult(C.Structure):
     ]
 
 
+class ShardSpec(C.Structure):
+    _fields_ = [("nranks", C.c_int32), ("bloom_num_hashes", C.c_int32), ("filter", C.c_void_p),
+                ("filter_loc", C.c_void_p), ("heavy", C.c_void_p), ("n_heavy", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
 class BrigError(RuntimeError):
     def __init__(self, status: int, msg: str, where: str = ""):
         self.status = status
@@ -194,6 +200,13 @@ def lib() -> C.CDLL:
     L.brig_join_gather_rate.argtypes = [vp, C.c_int64, C.c_int64, vp, _i64p, vp]
     L.brig_join_read_relation.argtypes = [C.c_char_p, C.c_int64, C.c_int32, C.c_uint32, vp, vp]
     L.brig_join_write_pairs.argtypes = [C.c_char_p, vp, vp, vp, C.c_int64]
+    L.brig_shard_owner.argtypes = [C.c_uint32, C.c_int32]
+    L.brig_shard_owner.restype = C.c_int32
+    L.brig_shard_filter_words.argtypes = [C.c_int64, C.c_double]
+    L.brig_shard_filter_words.restype = C.c_int64
+    L.brig_shard_count.argtypes = [C.POINTER(ShardSpec), vp, C.c_int64, vp, vp]
+    L.brig_shard_scatter.argtypes = [C.POINTER(ShardSpec), vp, vp, C.c_int64, vp, vp, vp, vp, vp]
+    L.brig_shard_bloom_build.argtypes = [vp, C.c_int64, vp, C.c_int64, C.c_int32, vp]
     if hasattr(L, "brig_serve_create"):
         L.brig_serve_create.argtypes = [C.POINTER(Config), C.POINTER(ServeConfig), C.POINTER(vp)]
         L.brig_serve_submit.argtypes = [vp, C.POINTER(ServeRequest), _i64p]

@@ -652,30 +652,9 @@ __device__ __forceinline__ void init_bars(uint64_t* bars) {
     __syncthreads();
 }
 
-// The Bloom kernels keep the launch's pattern table (one pair of masks per pattern index, filled for
-// the launch's k, which every filtered join of a launch shares) in shared memory. Fill is
-// block-wide; the caller synchronises. k == 0: no filter.
-__device__ __forceinline__ void fill_patterns(uint2* pat, int k) {
-    if (k == 0) return;
-    for (int i = threadIdx.x; i < kPatterns; i += blockDim.x)
-        pat[i] = make_uint2(bloom_pattern(0, (uint32_t)i, k), bloom_pattern(1, (uint32_t)i, k));
-}
-// Masks of a key at slot s: compile-time shifts (K == kBloomFastK) or the pattern table.
-template <int K>
-__device__ __forceinline__ uint2 slot_masks(const uint2* pat, const BloomSlot& s) {
-    if constexpr (K == kBloomFastK) return bloom_masks7(s.g);
-    else return pat[s.pidx];
-}
-// Shared-memory entries of the pattern table of a kernel of class K (none for k = 7).
-template <int K>
-constexpr int pat_entries() { return K == kBloomFastK ? 1 : kPatterns; }
 // The mask class of a join (the K of the instantiation that handles it).
 __device__ __forceinline__ int bloom_kclass(const JoinDesc& d) {
     return (d.bloom != nullptr && d.bloom_k == kBloomFastK) ? kBloomFastK : 0;
-}
-// A word pair passes when it holds every bit of both masks.
-__device__ __forceinline__ bool bloom_pass(uint2 w, uint2 mk) {
-    return (((w.x & mk.x) ^ mk.x) | ((w.y & mk.y) ^ mk.y)) == 0u;
 }
 // Finest partition of a key with mix m (hash mode: the top b1 + b2 bits) or key (modulo mode).
 template <int M>

@@ -336,6 +336,60 @@ int brig_join_read_relation(const char* path, int64_t n, int32_t read_val, uint3
 int brig_join_write_pairs(const char* path, const uint32_t* key, const uint32_t* r_val, const uint32_t* s_val,
                           int64_t n);
 
+/* ---- Sharded joins across GPUs: key ownership ------------------------------------------------
+ * The local steps of a join whose relations are spread over nranks GPUs, one process per GPU; the
+ * exchanges between the steps are the caller's (NCCL all-to-all and all-gather; brig_join.shard in
+ * the Python package is one such caller). Replaces the reference's multi-PE path: the ownership
+ * shuffle of R and of the prefiltered S (src/r_shuffle.cu:33-191), the Bloom filter merge
+ * (src/bf_allreduce.cu:236-284) and, for skewed inputs, S' rebalancing and R replication
+ * (src/s_redistribute.cu:26-152, src/r_replicate.cu:13-100). Per rank:
+ *   1. brig_shard_count + brig_shard_scatter on its R: R grouped into owner bins; bin r goes to rank
+ *      r (all-to-all), the heavy bin (below) to every rank (all-gather);
+ *   2. brig_shard_bloom_build over the R tuples it received: its owner's filter of
+ *      brig_shard_filter_words words; the filters are gathered on every rank (they cover disjoint
+ *      keys, so no OR reduction is needed) and located by filter_loc;
+ *   3. brig_shard_count + brig_shard_scatter on its S with the gathered filters: only S tuples that
+ *      pass their owner's filter are kept; bin r goes to rank r, the heavy bin stays;
+ *   4. brig_join_run of its owned R with the S it received, and of the gathered heavy R with the
+ *      heavy S it kept.
+ * Each output pair comes out on exactly one rank. A key's owner is brig_shard_owner(key, nranks), a
+ * hash independent of the engine's partition bits. Heavy keys are a sorted list of distinct keys
+ * that every rank passes alike; their tuples go to bin nranks and skip the filter. */
+#define BRIG_SHARD_MAX_RANKS 64
+#define BRIG_SHARD_MAX_HEAVY 1024
+typedef struct brig_shard_spec {
+    int32_t nranks;              /* owners, 1..BRIG_SHARD_MAX_RANKS */
+    int32_t bloom_num_hashes;    /* k of the owners' filters (1..16) when filter is not NULL */
+    const uint32_t* filter;      /* device: every owner's filter words (8-byte aligned), or NULL */
+    const int64_t* filter_loc;   /* device int64[2 * nranks]: word offset (even) and word count of
+                                    owner r's filter in `filter`; a count below 8, or an odd or
+                                    negative offset, drops the owner's tuples */
+    const uint32_t* heavy;       /* device: sorted distinct heavy keys, or NULL */
+    int32_t n_heavy;             /* 0..BRIG_SHARD_MAX_HEAVY */
+    int32_t reserved;
+} brig_shard_spec;
+
+/* Owner of `key` among nranks ranks (host), or -1 when nranks is out of range. */
+int32_t brig_shard_owner(uint32_t key, int32_t nranks);
+/* Words of an owner's filter for n_keys R tuples at bits_per_key (a multiple of 8, at least 8), or
+ * -1 for a bad argument or a filter of 2^32 words or more. */
+int64_t brig_shard_filter_words(int64_t n_keys, double bits_per_key);
+/* Counts the tuples of each bin: counts (device int64[nbins], nbins = nranks + (n_heavy > 0)) is
+ * zeroed and filled, stream-ordered. */
+int brig_shard_count(const brig_shard_spec* sp, const uint32_t* key, int64_t n, int64_t* counts, void* stream);
+/* Writes the tuples grouped by bin, bin b at [start_b, start_b + counts[b]) of out_key/out_val
+ * (start = exclusive scan of counts, which must come from brig_shard_count on the same inputs and
+ * spec; the outputs hold their sum). scratch: device int64[2 * nbins + 2]; scratch[0..nbins] receives
+ * the bin starts and the total, and scratch[2 * nbins + 1] the number of tuples that found their bin
+ * full (0 unless the inputs changed since the count). Tuples keep no order inside a bin. */
+int brig_shard_scatter(const brig_shard_spec* sp, const uint32_t* key, const uint32_t* val, int64_t n,
+                       const int64_t* counts, int64_t* scratch, uint32_t* out_key, uint32_t* out_val, void* stream);
+/* Builds an owner's filter over n keys into words[n_words] (device, 8-byte aligned, n_words a
+ * multiple of 8; zeroed first): the engine's blocked filter of word pairs with one segment, k =
+ * num_hashes (the per-partition build of the reference, src/bloom.cu:698-722, over the owned keys). */
+int brig_shard_bloom_build(const uint32_t* key, int64_t n, uint32_t* words, int64_t n_words, int32_t num_hashes,
+                           void* stream);
+
 /* Message for the last failed call on this thread (empty string if none). */
 const char* brig_join_last_error(void);
 

@@ -1,0 +1,215 @@
+"""The sharded join's device steps on one GPU: the owner grouping, heavy bin and filter prefilter of
+brig_shard_count / brig_shard_scatter against a host restatement, the owners' filters (no false
+negatives, bounded false positives), and whole sharded joins against the oracle with the ranks
+as threads of this process (exchanges through host memory, no kernel waiting on another) and
+as a one-rank NCCL group."""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from shard_helpers import Hub, ThreadComm, owners_np, run_ranks, spread
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+@pytest.fixture(scope="module")
+def shard(bj, torch_cuda):
+    import brig_join.shard as sh
+    return sh
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.uint32).view(np.int32)).to("cuda")
+
+
+def host(t):
+    return t.cpu().numpy().view(np.uint32)
+
+
+def bins_of(keys, vals, counts):
+    offs = np.concatenate([[0], np.cumsum(counts)])
+    return [(keys[offs[b]:offs[b + 1]], vals[offs[b]:offs[b + 1]]) for b in range(len(counts))]
+
+
+def same_multiset(k1, v1, k2, v2):
+    a = np.sort(k1.astype(np.uint64) << np.uint64(32) | v1.astype(np.uint64))
+    b = np.sort(k2.astype(np.uint64) << np.uint64(32) | v2.astype(np.uint64))
+    return np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("n", [0, 1, 4095, 4097, 300_001])
+@pytest.mark.parametrize("nranks", [1, 3, 8, 64])
+def test_split_groups_by_owner(shard, torch_cuda, n, nranks):
+    rng = np.random.default_rng(n + nranks)
+    k = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    v = np.arange(n, dtype=np.uint32)
+    ops = shard.CudaShardOps()
+    ok, ov, counts = ops.split(nranks, dev(torch_cuda, k), dev(torch_cuda, v))
+    torch_cuda.cuda.synchronize()
+    assert len(counts) == nranks and sum(counts) == n
+    own = owners_np(k, nranks)
+    assert counts == np.bincount(own, minlength=nranks).tolist()
+    for b, (bk, bv) in enumerate(bins_of(host(ok), host(ov), counts)):
+        sel = own == b
+        assert same_multiset(bk, bv, k[sel], v[sel]), b
+
+
+def test_split_heavy_bin(shard, torch_cuda):
+    rng = np.random.default_rng(4)
+    n, nranks = 200_000, 4
+    k = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    heavy = np.sort(np.unique(np.concatenate([k[rng.integers(0, n, 5)], [0xFFFFFFFF, 0]]))).astype(np.uint32)
+    k[rng.integers(0, n, 30_000)] = heavy[2]
+    v = np.arange(n, dtype=np.uint32)
+    ops = shard.CudaShardOps()
+    ok, ov, counts = ops.split(nranks, dev(torch_cuda, k), dev(torch_cuda, v), heavy=dev(torch_cuda, heavy))
+    assert len(counts) == nranks + 1
+    bins = owners_np(k, nranks)
+    bins[np.isin(k, heavy)] = nranks
+    assert counts == np.bincount(bins, minlength=nranks + 1).tolist()
+    for b, (bk, bv) in enumerate(bins_of(host(ok), host(ov), counts)):
+        assert same_multiset(bk, bv, k[bins == b], v[bins == b]), b
+
+
+@pytest.mark.parametrize("bits,k", [(10.0, 7), (8.0, 6), (14.0, 10), (4.0, 1)])
+def test_owner_filters_prefilter_s(shard, torch_cuda, oracle, bits, k):
+    """Every owner's filter over its R keys, gathered: an S tuple whose key is in R always survives,
+    a key in no filter survives at about the filter's false-positive rate."""
+    nranks = 5
+    rk, _, _, _ = oracle.gen(8, 400_000, 1, 0.0, want_vals=False)
+    own = owners_np(rk, nranks)
+    ops = shard.CudaShardOps()
+    words = [ops.bloom_build(dev(torch_cuda, rk[own == o]), bits, k) for o in range(nranks)]
+    sizes = [w.numel() for w in words]
+    assert sizes == [shard.filter_words(int((own == o).sum()), bits) for o in range(nranks)]
+    filt = torch_cuda.cat(words)
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+    loc = torch_cuda.from_numpy(np.stack([offs, sizes], 1).reshape(-1).astype(np.int64)).cuda()
+    miss = np.arange(0x90000000, 0x90000000 + 400_000, dtype=np.uint32)  # R keys are below 2^31
+    sk = np.concatenate([rk, miss])
+    sv = np.arange(len(sk), dtype=np.uint32)
+    ok, ov, counts = ops.split(nranks, dev(torch_cuda, sk), dev(torch_cuda, sv), filt=filt, filter_loc=loc,
+                               num_hashes=k)
+    got_v = host(ov)
+    assert np.isin(np.arange(len(rk), dtype=np.uint32), got_v).all()  # no false negatives
+    fpr = (got_v >= len(rk)).sum() / len(miss)
+    # k = 7 takes its masks from shifts (about 2% at 10 bits/key), the other k from the pattern
+    # table, whose 1024 pattern pairs raise the floor: 1.4% measured at 14 bits/key with k = 10
+    assert fpr < {7: 0.03, 6: 0.06, 10: 0.025, 1: 0.6}[k], fpr
+    for b, (bk, _) in enumerate(bins_of(host(ok), got_v, counts)):
+        assert (owners_np(bk, nranks) == b).all()
+
+
+def test_owner_without_filter_blocks_drops_its_tuples(shard, torch_cuda):
+    """A filter location of fewer than 8 words (an owner that received no R tuple) keeps none of
+    that owner's S tuples."""
+    nranks = 3
+    k = np.arange(1, 30_001, dtype=np.uint32)
+    v = np.arange(30_000, dtype=np.uint32)
+    filt = torch_cuda.full((16,), -1, dtype=torch_cuda.int32, device="cuda")  # all bits set
+    loc = torch_cuda.tensor([0, 8, 8, 0, 8, 8], dtype=torch_cuda.int64, device="cuda")  # owner 1: no words
+    ok, ov, counts = shard.CudaShardOps().split(nranks, dev(torch_cuda, k), dev(torch_cuda, v), filt=filt,
+                                                filter_loc=loc, num_hashes=7)
+    own = owners_np(k, nranks)
+    assert counts == [int((own == 0).sum()), 0, int((own == 2).sum())]
+    loc = torch_cuda.tensor([1, 8, 0, 8, 8, 8], dtype=torch_cuda.int64, device="cuda")  # owner 0: odd offset
+    _, _, counts = shard.CudaShardOps().split(nranks, dev(torch_cuda, k), dev(torch_cuda, v), filt=filt,
+                                              filter_loc=loc, num_hashes=7)
+    assert counts == [0, int((own == 1).sum()), int((own == 2).sum())]
+
+
+def test_scatter_counts_tuples_that_find_their_bin_full(shard, bj, torch_cuda):
+    """Counts taken on half of the keys, scatter over all of them: the writes stay inside the
+    buffers sized by the counts and the tuples that did not fit are reported."""
+    lib = bj.lib()
+    n, nranks = 100_000, 4
+    k = dev(torch_cuda, np.random.default_rng(2).integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32))
+    v = dev(torch_cuda, np.arange(n, dtype=np.uint32))
+    sp = bj.ShardSpec(nranks, 0, None, None, None, 0, 0)
+    counts = torch_cuda.empty(nranks, dtype=torch_cuda.int64, device="cuda")
+    assert lib.brig_shard_count(C.byref(sp), k.data_ptr(), n // 2, counts.data_ptr(), None) == 0
+    total = int(counts.sum().item())
+    ok = torch_cuda.full((total + 64,), -7, dtype=torch_cuda.int32, device="cuda")
+    ov = torch_cuda.full((total + 64,), -7, dtype=torch_cuda.int32, device="cuda")
+    scratch = torch_cuda.empty(2 * nranks + 2, dtype=torch_cuda.int64, device="cuda")
+    assert lib.brig_shard_scatter(C.byref(sp), k.data_ptr(), v.data_ptr(), n, counts.data_ptr(), scratch.data_ptr(),
+                                  ok.data_ptr(), ov.data_ptr(), None) == 0
+    torch_cuda.cuda.synchronize()
+    assert int(scratch[2 * nranks + 1].item()) == n - total
+    assert scratch[:nranks + 1].tolist()[-1] == total
+    assert (ok[total:] == -7).all() and (ov[total:] == -7).all()  # nothing past the bins
+    assert lib.brig_shard_count(None, k.data_ptr(), n, counts.data_ptr(), None) == bj.BRIG_E_INVALID
+    sp_bad = bj.ShardSpec(65, 0, None, None, None, 0, 0)
+    assert lib.brig_shard_count(C.byref(sp_bad), k.data_ptr(), n, counts.data_ptr(), None) == bj.BRIG_E_INVALID
+
+
+@pytest.mark.parametrize("bits", [0.0, 10.0])
+@pytest.mark.parametrize("hot", [0.0, 0.25])
+def test_thread_ranks_on_one_gpu_give_the_oracle_pairs(shard, oracle, torch_cuda, bits, hot):
+    size = 4
+    (rk, rv, sk, sv), parts = spread(oracle, 31, 400_000, 1_000_000, size, match=0.2, hot=hot)
+    hub = Hub(size)
+
+    def rank(r):
+        job = shard.ShardedJoin(ThreadComm(hub, r), bits_per_key=bits)
+        x = job.run(*(dev(torch_cuda, a) for a in parts[r]))
+        torch_cuda.cuda.synchronize()
+        return x
+
+    res = run_ranks(hub, rank)
+    got_r = np.concatenate([host(x.r_val) for x in res])
+    got_s = np.concatenate([host(x.s_val) for x in res])
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    assert len(got_r) == len(exp_r) and all(x.total == len(exp_r) for x in res)
+    a, b = oracle.sort_pairs(got_r, got_s), oracle.sort_pairs(exp_r, exp_s)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    if hot:
+        assert int(rk[7]) in res[0].heavy_keys.tolist()
+    if bits:
+        assert sum(x.stats["s_survivors"] for x in res) < 0.5 * len(sk)
+
+
+NCCL_ONE_RANK = r"""
+import datetime, os, sys
+import numpy as np, torch, torch.distributed as dist
+sys.path[:0] = [sys.argv[1], sys.argv[2], os.path.join(sys.argv[2], "brig-join_b200")]
+import brig_join.shard as sh
+from oracle import oracle as o
+os.environ["MASTER_ADDR"] = "127.0.0.1"
+os.environ["MASTER_PORT"] = sys.argv[3]
+os.environ["NCCL_NVLS_ENABLE"] = "0"
+dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60),
+                        device_id=torch.device("cuda:0"))
+try:
+    rk, rv, sk, sv = o.gen(17, 300_000, 600_000, 0.3)
+    d = lambda a: torch.from_numpy(a.view(np.int32)).cuda()
+    x = sh.ShardedJoin(sh.TorchComm(), bits_per_key=10.0).run(d(rk), d(rv), d(sk), d(sv))
+    torch.cuda.synchronize()
+    np.savez(sys.argv[4], r=x.r_val.cpu().numpy(), s=x.s_val.cpu().numpy(), total=x.total)
+finally:
+    dist.destroy_process_group()
+"""
+
+
+def test_nccl_one_rank_group(oracle, tmp_path):
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = str(tmp_path / "nccl1.npz")
+    r = subprocess.run([sys.executable, "-c", NCCL_ONE_RANK, HERE, ROOT, str(port), out], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-4000:]
+    d = np.load(out)
+    rk, rv, sk, sv = oracle.gen(17, 300_000, 600_000, 0.3)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    assert int(d["total"]) == len(exp_r)
+    a = oracle.sort_pairs(d["r"].view(np.uint32), d["s"].view(np.uint32))
+    b = oracle.sort_pairs(exp_r, exp_s)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
