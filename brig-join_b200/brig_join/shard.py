@@ -29,7 +29,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import BRIG_E_OVERFLOW, BRIG_OK, Join, ShardSpec, _ptr, check, lib
+from . import BRIG_OK, Join, ShardSpec, _ptr, check, lib
 
 MAX_RANKS = 64
 MAX_HEAVY = 1024
@@ -88,7 +88,7 @@ class TorchComm:
         n = torch.tensor([x.numel()], dtype=torch.int64, device=x.device)
         ns = [torch.empty_like(n) for _ in range(self.size)]
         d.all_gather(ns, n, group=self.group)
-        sizes = [int(t.item()) for t in ns]
+        sizes = torch.cat(ns).tolist()
         m = max(1, max(sizes))
         pad = torch.zeros(m, dtype=x.dtype, device=x.device)
         pad[: x.numel()] = x
@@ -107,6 +107,7 @@ class CudaShardOps:
 
     def __init__(self, **join_kw):
         self.join_handle = Join(**join_kw)
+        self._lost = []  # each scatter's count of tuples that found their bin full, read by verify()
 
     @staticmethod
     def _stream():
@@ -131,10 +132,16 @@ class CudaShardOps:
         scratch = torch.empty(2 * nb + 2, dtype=torch.int64, device=dev)
         check(lib().brig_shard_scatter(C.byref(sp), _ptr(key), _ptr(val), key.numel(), _ptr(counts), _ptr(scratch),
                                        _ptr(ok), _ptr(ov), st), "brig_shard_scatter")
-        lost = int(scratch[2 * nb + 1].item())
-        if lost:
-            raise RuntimeError(f"brig_shard_scatter: {lost} tuples found their bin full")
+        self._lost.append(scratch[2 * nb + 1:])
         return ok[:total], ov[:total], cl
+
+    def verify(self):
+        """Raises if a scatter since the last call found a bin full (one read for all of them)."""
+        if self._lost:
+            lost = int(torch.cat(self._lost).sum().item())
+            self._lost = []
+            if lost:
+                raise RuntimeError(f"brig_shard_scatter: {lost} tuples found their bin full")
 
     def bloom_build(self, key, bits_per_key: float, num_hashes: int) -> torch.Tensor:
         key = _i32(key)
@@ -196,6 +203,8 @@ class ShardedJoin:
     def heavy_keys(self, s_key: torch.Tensor) -> np.ndarray:
         """The heavy keys, from a sample of every rank's S (collective: every rank calls it)."""
         comm = self.comm
+        if comm.size == 1:  # one rank: every tuple stays, there is nothing to balance
+            return np.zeros(0, dtype=np.uint32)
         s_key = _i32(s_key)
         n = s_key.numel()
         m = min(n, self.sample) if self.heavy_share > 0 else 0
@@ -264,6 +273,8 @@ class ShardedJoin:
             parts_r.append(b_r)
             parts_s.append(b_s)
         out_r, out_s = torch.cat(parts_r), torch.cat(parts_s)
+        if hasattr(ops, "verify"):
+            ops.verify()
         count = out_r.numel()
         total = comm.all_reduce_sum(count, r_key.device)
         stats = {"r_owned": r_own_k.numel(), "s_received": s_own_k.numel(), "s_survivors": sum(sc),

@@ -39,6 +39,10 @@ constexpr int kShardTile = kShardThreads * kShardItems;
 constexpr int kMaxBins = BRIG_SHARD_MAX_RANKS + 1;
 constexpr uint32_t kOwnerSeed = 0x6a09e667u;  // the first 32 fractional bits of sqrt(2)
 
+// CTAs of k_shard_split per SM: 32 registers a thread for the count without filters, 42 for the
+// scatter without filters, 64 with filters (8 filter word pairs and masks in flight).
+constexpr int shard_ctas(bool write, bool filter) { return filter ? 2 : (write ? 3 : 4); }
+
 BRIG_HD uint32_t owner_of(uint32_t key, uint32_t nranks) { return fastrange32(mix32(key ^ kOwnerSeed), nranks); }
 
 struct ShardArgs {
@@ -62,9 +66,11 @@ __device__ __forceinline__ bool in_sorted(const uint32_t* a, int n, uint32_t k) 
 }
 
 // counts: [nbins] (kWrite false). start: [nbins + 1] bin starts in out_key/out_val, cursor: [nbins]
-// tuples placed so far per bin, errors: tuples that found their bin full (kWrite true).
-template <bool kWrite, int K>
-__global__ void __launch_bounds__(kShardThreads, 2)
+// tuples placed so far per bin, errors: tuples that found their bin full (kWrite true). kFilter:
+// the spec has filters (K: their mask class); without them a thread needs fewer registers and
+// more CTAs fit on an SM (shard_ctas), so more key loads are in flight.
+template <bool kWrite, bool kFilter, int K>
+__global__ void __launch_bounds__(kShardThreads, shard_ctas(kWrite, kFilter))
 k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __restrict__ val, int64_t n,
               unsigned long long* counts, const int64_t* __restrict__ start, unsigned long long* cursor,
               uint32_t* __restrict__ out_key, uint32_t* __restrict__ out_val, unsigned long long* errors) {
@@ -74,12 +80,12 @@ k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __r
     __shared__ int64_t s_floc[2 * BRIG_SHARD_MAX_RANKS];
     __shared__ uint32_t s_heavy[BRIG_SHARD_MAX_HEAVY];
     __shared__ uint2 s_pat[pat_entries<K>()];
-    if (K != kBloomFastK && a.filter) fill_patterns(s_pat, a.k);
+    if (kFilter && K != kBloomFastK) fill_patterns(s_pat, a.k);
     for (int i = threadIdx.x; i < a.nbins; i += kShardThreads) {
         s_cnt[i] = 0;
         if (kWrite) s_end[i] = start[i + 1];
     }
-    if (a.filter)
+    if (kFilter)
         for (int i = threadIdx.x; i < 2 * a.nranks; i += kShardThreads) s_floc[i] = a.floc[i];
     for (int i = threadIdx.x; i < a.n_heavy; i += kShardThreads) s_heavy[i] = a.heavy[i];
     __syncthreads();
@@ -110,7 +116,7 @@ k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __r
             }
             const uint32_t o = owner_of(kk[u], nr);
             bin[u] = (int)o;
-            if (a.filter) {
+            if (kFilter) {
                 const int64_t off = s_floc[2 * o], words = s_floc[2 * o + 1];
                 if (words < 8 || off < 0 || (off & 1)) {  // no filter block (the owner holds no R
                     bin[u] = -1;                           // tuple), or no aligned word pair to read
@@ -124,7 +130,7 @@ k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __r
         uint32_t rank[kShardItems];
 #pragma unroll
         for (int u = 0; u < kShardItems; ++u) {
-            if (a.filter && bin[u] >= 0 && bin[u] < (int)nr && !bloom_pass(w[u], mk[u])) bin[u] = -1;
+            if (kFilter && bin[u] >= 0 && bin[u] < (int)nr && !bloom_pass(w[u], mk[u])) bin[u] = -1;
             const int b = bin[u];
             const uint32_t peers = __match_any_sync(0xffffffffu, b);
             const int leader = __ffs(peers) - 1;
@@ -226,12 +232,16 @@ void launch_split(const ShardArgs& a, const uint32_t* key, const uint32_t* val, 
                   unsigned long long* errors, cudaStream_t st) {
     if (n == 0) return;
     const int64_t ntiles = (n + kShardTile - 1) / kShardTile;
-    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * 2);
-    if (a.filter && a.k != kBloomFastK)
-        k_shard_split<kWrite, 0><<<grid, kShardThreads, 0, st>>>(a, key, val, n, counts, start, cursor, ok, ov, errors);
+    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * shard_ctas(kWrite, a.filter != nullptr));
+    if (!a.filter)
+        k_shard_split<kWrite, false, kBloomFastK><<<grid, kShardThreads, 0, st>>>(a, key, val, n, counts, start, cursor,
+                                                                                  ok, ov, errors);
+    else if (a.k != kBloomFastK)
+        k_shard_split<kWrite, true, 0><<<grid, kShardThreads, 0, st>>>(a, key, val, n, counts, start, cursor, ok, ov,
+                                                                       errors);
     else
-        k_shard_split<kWrite, kBloomFastK><<<grid, kShardThreads, 0, st>>>(a, key, val, n, counts, start, cursor, ok, ov,
-                                                                           errors);
+        k_shard_split<kWrite, true, kBloomFastK><<<grid, kShardThreads, 0, st>>>(a, key, val, n, counts, start, cursor,
+                                                                                 ok, ov, errors);
     note_launches(1);
     cuda_check(cudaGetLastError(), "k_shard_split");
 }
