@@ -148,7 +148,7 @@ class ServeResult(C.Structure):
 class ShardSpec(C.Structure):
     _fields_ = [("nranks", C.c_int32), ("bloom_num_hashes", C.c_int32), ("filter", C.c_void_p),
                 ("filter_loc", C.c_void_p), ("heavy", C.c_void_p), ("n_heavy", C.c_int32),
-                ("reserved", C.c_int32)]
+                ("reserved", C.c_int32), ("bin_cache", C.c_void_p)]
 
 
 class BrigError(RuntimeError):

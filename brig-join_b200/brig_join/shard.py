@@ -113,14 +113,18 @@ class CudaShardOps:
     def _stream():
         return torch.cuda.current_stream().cuda_stream
 
-    def split(self, nranks: int, key, val, heavy=None, filt=None, filter_loc=None, num_hashes=0):
+    def split(self, nranks: int, key, val, heavy=None, filt=None, filter_loc=None, num_hashes=0, cache=None):
         """Groups (key, val) into owner bins (and a heavy bin when `heavy` holds keys); with a filter
-        only tuples that pass their owner's filter are kept. Returns (keys, values, bin counts)."""
+        only tuples that pass their owner's filter are kept. Returns (keys, values, bin counts).
+        cache: keep each tuple's bin between the count and the scatter (default: with a filter, where
+        it saves the second filter read)."""
         key, val = _i32(key), _i32(val)
         dev = key.device
         nh = 0 if heavy is None else heavy.numel()
+        use_cache = (filt is not None) if cache is None else cache
+        bins = torch.empty(max(key.numel(), 1), dtype=torch.uint8, device=dev) if use_cache else None
         sp = ShardSpec(nranks, num_hashes if filt is not None else 0, _ptr(filt), _ptr(filter_loc),
-                       _ptr(heavy) if nh else None, nh, 0)
+                       _ptr(heavy) if nh else None, nh, 0, _ptr(bins))
         nb = nranks + (1 if nh else 0)
         counts = torch.empty(nb, dtype=torch.int64, device=dev)
         st = self._stream()

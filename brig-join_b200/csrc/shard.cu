@@ -22,7 +22,7 @@
 // bins. Each warp ranks its lanes of one bin together (one shared-memory atomic per bin and warp),
 // so the stores of a warp's tuples of one bin are consecutive. k_shard_offsets turns the counts
 // into bin starts. k_shard_bloom_build builds one owner's filter: the engine's blocked word-pair
-// filter (brig_common.cuh) with a single segment.
+// filter (brig_common.cuh) with a single segment, one 64-bit atomicOr per key.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -40,8 +40,11 @@ constexpr int kMaxBins = BRIG_SHARD_MAX_RANKS + 1;
 constexpr uint32_t kOwnerSeed = 0x6a09e667u;  // the first 32 fractional bits of sqrt(2)
 
 // CTAs of k_shard_split per SM: 32 registers a thread for the count without filters, 42 for the
-// scatter without filters, 64 with filters (8 filter word pairs and masks in flight).
-constexpr int shard_ctas(bool write, bool filter) { return filter ? 2 : (write ? 3 : 4); }
+// scatter without filters, 64 with filters (8 filter word pairs and masks in flight) and for the
+// scatter that reads a bin cache.
+constexpr int shard_ctas(bool write, bool filter, bool cache = false) {
+    return (filter || cache) ? 2 : (write ? 3 : 4);
+}
 
 BRIG_HD uint32_t owner_of(uint32_t key, uint32_t nranks) { return fastrange32(mix32(key ^ kOwnerSeed), nranks); }
 
@@ -52,6 +55,7 @@ struct ShardArgs {
     const uint32_t* heavy;   // sorted heavy keys
     int32_t n_heavy;
     int32_t k;               // hashes of the filters
+    uint8_t* cache;          // [n] bin of every tuple (0xff: dropped), or nullptr
 };
 
 // Whether k is in the sorted array a[0, n).
@@ -68,9 +72,11 @@ __device__ __forceinline__ bool in_sorted(const uint32_t* a, int n, uint32_t k) 
 // counts: [nbins] (kWrite false). start: [nbins + 1] bin starts in out_key/out_val, cursor: [nbins]
 // tuples placed so far per bin, errors: tuples that found their bin full (kWrite true). kFilter:
 // the spec has filters (K: their mask class); without them a thread needs fewer registers and
-// more CTAs fit on an SM (shard_ctas), so more key loads are in flight.
-template <bool kWrite, bool kFilter, int K>
-__global__ void __launch_bounds__(kShardThreads, shard_ctas(kWrite, kFilter))
+// more CTAs fit on an SM (shard_ctas), so more key loads are in flight. With a bin cache the count
+// pass stores every tuple's bin and the scatter (kCache) reads it instead of testing the filters
+// again.
+template <bool kWrite, bool kFilter, int K, bool kCache = false>
+__global__ void __launch_bounds__(kShardThreads, shard_ctas(kWrite, kFilter, kCache))
 k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __restrict__ val, int64_t n,
               unsigned long long* counts, const int64_t* __restrict__ start, unsigned long long* cursor,
               uint32_t* __restrict__ out_key, uint32_t* __restrict__ out_val, unsigned long long* errors) {
@@ -103,34 +109,56 @@ k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __r
             kk[u] = i < n ? key[i] : 0u;
             bin[u] = i < n ? 0 : -1;
         }
-        // owners, and the filter words of every key in flight together
-        uint2 w[kShardItems], mk[kShardItems];
+        if constexpr (kCache) {
 #pragma unroll
-        for (int u = 0; u < kShardItems; ++u) {
-            w[u] = make_uint2(0u, 0u);
-            mk[u] = make_uint2(0u, 0u);
-            if (bin[u] < 0) continue;
-            if (a.n_heavy > 0 && in_sorted(s_heavy, a.n_heavy, kk[u])) {
-                bin[u] = (int)nr;
-                continue;
+            for (int u = 0; u < kShardItems; ++u) {
+                const int64_t i = t0 + u * kShardThreads + threadIdx.x;
+                if (i < n) {
+                    const uint32_t c = a.cache[i];
+                    bin[u] = c == 0xffu ? -1 : (int)c;
+                }
             }
-            const uint32_t o = owner_of(kk[u], nr);
-            bin[u] = (int)o;
-            if (kFilter) {
-                const int64_t off = s_floc[2 * o], words = s_floc[2 * o + 1];
-                if (words < 8 || off < 0 || (off & 1)) {  // no filter block (the owner holds no R
-                    bin[u] = -1;                           // tuple), or no aligned word pair to read
+        } else {
+            // owners, and the filter words of every key in flight together
+            uint2 w[kShardItems], mk[kShardItems];
+#pragma unroll
+            for (int u = 0; u < kShardItems; ++u) {
+                w[u] = make_uint2(0u, 0u);
+                mk[u] = make_uint2(0u, 0u);
+                if (bin[u] < 0) continue;
+                if (a.n_heavy > 0 && in_sorted(s_heavy, a.n_heavy, kk[u])) {
+                    bin[u] = (int)nr;
                     continue;
                 }
-                const BloomSlot sl = bloom_slot(mix32(kk[u]), 0u, (uint32_t)(words >> 3));
-                mk[u] = slot_masks<K>(s_pat, sl);
-                w[u] = __ldg(reinterpret_cast<const uint2*>(a.filter + off + sl.widx));
+                const uint32_t o = owner_of(kk[u], nr);
+                bin[u] = (int)o;
+                if (kFilter) {
+                    const int64_t off = s_floc[2 * o], words = s_floc[2 * o + 1];
+                    if (words < 8 || off < 0 || (off & 1)) {  // no filter block (the owner holds no R
+                        bin[u] = -1;                           // tuple), or no aligned word pair to read
+                        continue;
+                    }
+                    const BloomSlot sl = bloom_slot(mix32(kk[u]), 0u, (uint32_t)(words >> 3));
+                    mk[u] = slot_masks<K>(s_pat, sl);
+                    w[u] = __ldg(reinterpret_cast<const uint2*>(a.filter + off + sl.widx));
+                }
+            }
+            if constexpr (kFilter) {
+#pragma unroll
+                for (int u = 0; u < kShardItems; ++u)
+                    if (bin[u] >= 0 && bin[u] < (int)nr && !bloom_pass(w[u], mk[u])) bin[u] = -1;
+            }
+            if (!kWrite && a.cache != nullptr) {
+#pragma unroll
+                for (int u = 0; u < kShardItems; ++u) {
+                    const int64_t i = t0 + u * kShardThreads + threadIdx.x;
+                    if (i < n) a.cache[i] = (uint8_t)(bin[u] < 0 ? 0xff : bin[u]);
+                }
             }
         }
         uint32_t rank[kShardItems];
 #pragma unroll
         for (int u = 0; u < kShardItems; ++u) {
-            if (kFilter && bin[u] >= 0 && bin[u] < (int)nr && !bloom_pass(w[u], mk[u])) bin[u] = -1;
             const int b = bin[u];
             const uint32_t peers = __match_any_sync(0xffffffffu, b);
             const int leader = __ffs(peers) - 1;
@@ -193,8 +221,10 @@ k_shard_bloom_build(const uint32_t* __restrict__ key, int64_t n, uint32_t* words
     for (int64_t i = (int64_t)blockIdx.x * kShardThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kShardThreads) {
         const BloomSlot sl = bloom_slot(mix32(key[i]), 0u, nblocks);
         const uint2 mk = slot_masks<K>(s_pat, sl);
-        atomicOr(words + sl.widx, mk.x);
-        if (mk.y) atomicOr(words + sl.widx + 1, mk.y);
+        // one 64-bit atomic on the word pair (even word low): the build is bound by the number of
+        // atomics the L2 serves, not by their width
+        atomicOr(reinterpret_cast<unsigned long long*>(words + sl.widx),
+                 ((unsigned long long)mk.y << 32) | (unsigned long long)mk.x);
     }
 }
 
@@ -223,6 +253,7 @@ ShardArgs check_spec(const brig_shard_spec* sp, int64_t n, const uint32_t* key) 
     a.heavy = sp->heavy;
     a.n_heavy = sp->n_heavy;
     a.k = sp->bloom_num_hashes;
+    a.cache = sp->bin_cache;
     return a;
 }
 
@@ -232,7 +263,19 @@ void launch_split(const ShardArgs& a, const uint32_t* key, const uint32_t* val, 
                   unsigned long long* errors, cudaStream_t st) {
     if (n == 0) return;
     const int64_t ntiles = (n + kShardTile - 1) / kShardTile;
-    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sm_count() * shard_ctas(kWrite, a.filter != nullptr));
+    const int sms = sm_count();
+    const int grid = (int)std::min<int64_t>(ntiles, (int64_t)sms * shard_ctas(kWrite, a.filter != nullptr));
+    if constexpr (kWrite) {
+        if (a.cache) {
+            const int grid_c = (int)std::min<int64_t>(ntiles, (int64_t)sms * shard_ctas(true, false, true));
+            k_shard_split<true, false, kBloomFastK, true><<<grid_c, kShardThreads, 0, st>>>(a, key, val, n, counts,
+                                                                                           start, cursor, ok, ov,
+                                                                                           errors);
+            note_launches(1);
+            cuda_check(cudaGetLastError(), "k_shard_split");
+            return;
+        }
+    }
     if (!a.filter)
         k_shard_split<kWrite, false, kBloomFastK><<<grid, kShardThreads, 0, st>>>(a, key, val, n, counts, start, cursor,
                                                                                   ok, ov, errors);

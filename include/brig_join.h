@@ -367,6 +367,9 @@ typedef struct brig_shard_spec {
     const uint32_t* heavy;       /* device: sorted distinct heavy keys, or NULL */
     int32_t n_heavy;             /* 0..BRIG_SHARD_MAX_HEAVY */
     int32_t reserved;
+    uint8_t* bin_cache;          /* device uint8[n] or NULL: brig_shard_count stores each tuple's bin
+                                    (0xff: dropped) and brig_shard_scatter, given the same spec and
+                                    inputs, reads it instead of testing the filters again */
 } brig_shard_spec;
 
 /* Owner of `key` among nranks ranks (host), or -1 when nranks is out of range. */

@@ -60,15 +60,19 @@ def test_split_groups_by_owner(shard, torch_cuda, n, nranks):
         assert same_multiset(bk, bv, k[sel], v[sel]), b
 
 
-def test_split_heavy_bin(shard, torch_cuda):
+@pytest.mark.parametrize("cache", [False, True])
+def test_split_heavy_bin(shard, torch_cuda, cache):
+    """The heavy bin, with the scatter recomputing the bins or reading the count pass's bin cache."""
     rng = np.random.default_rng(4)
-    n, nranks = 200_000, 4
+    n, nranks = 200_003, 4
     k = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
     heavy = np.sort(np.unique(np.concatenate([k[rng.integers(0, n, 5)], [0xFFFFFFFF, 0]]))).astype(np.uint32)
     k[rng.integers(0, n, 30_000)] = heavy[2]
     v = np.arange(n, dtype=np.uint32)
     ops = shard.CudaShardOps()
-    ok, ov, counts = ops.split(nranks, dev(torch_cuda, k), dev(torch_cuda, v), heavy=dev(torch_cuda, heavy))
+    ok, ov, counts = ops.split(nranks, dev(torch_cuda, k), dev(torch_cuda, v), heavy=dev(torch_cuda, heavy),
+                               cache=cache)
+    ops.verify()
     assert len(counts) == nranks + 1
     bins = owners_np(k, nranks)
     bins[np.isin(k, heavy)] = nranks
@@ -96,6 +100,12 @@ def test_owner_filters_prefilter_s(shard, torch_cuda, oracle, bits, k):
     sv = np.arange(len(sk), dtype=np.uint32)
     ok, ov, counts = ops.split(nranks, dev(torch_cuda, sk), dev(torch_cuda, sv), filt=filt, filter_loc=loc,
                                num_hashes=k)
+    ok2, ov2, counts2 = ops.split(nranks, dev(torch_cuda, sk), dev(torch_cuda, sv), filt=filt, filter_loc=loc,
+                                  num_hashes=k, cache=False)  # the scatter tests the filters again
+    ops.verify()
+    assert counts2 == counts
+    for (a, b), (c, d) in zip(bins_of(host(ok), host(ov), counts), bins_of(host(ok2), host(ov2), counts2)):
+        assert same_multiset(a, b, c, d)
     got_v = host(ov)
     assert np.isin(np.arange(len(rk), dtype=np.uint32), got_v).all()  # no false negatives
     fpr = (got_v >= len(rk)).sum() / len(miss)
