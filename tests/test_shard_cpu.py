@@ -94,6 +94,29 @@ def test_thread_ranks_give_the_oracle_pairs(shard, oracle, bits, hot):
         assert sum(x.stats["s_survivors"] for x in res) < len(sk)
 
 
+def test_a_rank_without_tuples(shard, oracle):
+    """One rank holds no R and no S tuple, another no R: they still take part in every exchange and
+    the union of the results is the oracle's."""
+    size = 3
+    (rk, rv, sk, sv), parts = spread(oracle, 13, 9000, 20000, size, match=0.4, hot=0.2)
+    e = np.zeros(0, dtype=np.uint32)
+    parts = [parts[0], (e, e, e, e), (e, e, np.concatenate([parts[1][2], parts[2][2]]),
+                                      np.concatenate([parts[1][3], parts[2][3]]))]
+    rk, rv = parts[0][0], parts[0][1]
+    hub = Hub(size)
+
+    def rank(r):
+        job = shard.ShardedJoin(ThreadComm(hub, r), HostShardOps(oracle), sample=4096)
+        return job.run(*(torch.from_numpy(a.view(np.int32).copy()) for a in parts[r]))
+
+    res = run_ranks(hub, rank)
+    got_r, got_s = union(res)
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    assert all(x.total == len(exp_r) for x in res)
+    a, b = oracle.sort_pairs(got_r, got_s), oracle.sort_pairs(exp_r, exp_s)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
 def test_heavy_keys_keep_a_hot_key_off_its_owner(shard, oracle):
     """A key held by 40% of S: with the heavy-key handling every rank receives about its fair
     share; without it the hot key's owner receives its whole share of S."""

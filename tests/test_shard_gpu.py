@@ -185,6 +185,30 @@ def test_thread_ranks_on_one_gpu_give_the_oracle_pairs(shard, oracle, torch_cuda
         assert sum(x.stats["s_survivors"] for x in res) < 0.5 * len(sk)
 
 
+def test_thread_ranks_with_empty_ranks_on_one_gpu(shard, oracle, torch_cuda):
+    """Rank 1 holds nothing and rank 2 holds S only; with the filters and a hot key."""
+    size = 3
+    (_, _, sk, sv), parts = spread(oracle, 41, 200_000, 500_000, size, match=0.3, hot=0.2)
+    e = np.zeros(0, dtype=np.uint32)
+    parts = [parts[0], (e, e, e, e), (e, e, np.concatenate([parts[1][2], parts[2][2]]),
+                                      np.concatenate([parts[1][3], parts[2][3]]))]
+    rk, rv = parts[0][0], parts[0][1]
+    hub = Hub(size)
+
+    def rank(r):
+        x = shard.ShardedJoin(ThreadComm(hub, r), bits_per_key=10.0).run(*(dev(torch_cuda, a) for a in parts[r]))
+        torch_cuda.cuda.synchronize()
+        return x
+
+    res = run_ranks(hub, rank)
+    got_r = np.concatenate([host(x.r_val) for x in res])
+    got_s = np.concatenate([host(x.s_val) for x in res])
+    exp_r, exp_s = oracle.pairs(rk, rv, sk, sv)
+    assert all(x.total == len(exp_r) for x in res)
+    a, b = oracle.sort_pairs(got_r, got_s), oracle.sort_pairs(exp_r, exp_s)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
 NCCL_ONE_RANK = r"""
 import datetime, os, sys
 import numpy as np, torch, torch.distributed as dist
