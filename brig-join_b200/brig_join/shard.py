@@ -107,7 +107,7 @@ class CudaShardOps:
 
     def __init__(self, **join_kw):
         self.join_handle = Join(**join_kw)
-        self._lost = []  # each scatter's count of tuples that found their bin full, read by verify()
+        self._lost = []  # each scatter's count of tuples that found their bin full, read by lost()
 
     @staticmethod
     def _stream():
@@ -139,13 +139,13 @@ class CudaShardOps:
         self._lost.append(scratch[2 * nb + 1:])
         return ok[:total], ov[:total], cl
 
-    def verify(self):
-        """Raises if a scatter since the last call found a bin full (one read for all of them)."""
-        if self._lost:
-            lost = int(torch.cat(self._lost).sum().item())
-            self._lost = []
-            if lost:
-                raise RuntimeError(f"brig_shard_scatter: {lost} tuples found their bin full")
+    def lost(self) -> int:
+        """Tuples that found their bin full in the scatters since the last call (one read for all)."""
+        if not self._lost:
+            return 0
+        n = int(torch.cat(self._lost).sum().item())
+        self._lost = []
+        return n
 
     def bloom_build(self, key, bits_per_key: float, num_hashes: int) -> torch.Tensor:
         key = _i32(key)
@@ -187,7 +187,11 @@ class ShardResult:
 class ShardedJoin:
     """A join of relations spread over the ranks of `comm`, each rank holding some tuples of R and S.
 
-    bits_per_key = 0 turns the prefilter off; heavy_share = 0 turns the heavy-key handling off."""
+    bits_per_key = 0 turns the prefilter off; heavy_share = 0 turns the heavy-key handling off.
+    Every rank runs the same collectives in the same order. A scatter that found a bin full on any
+    rank makes every rank raise after the last collective. A rank that fails in between leaves the
+    others waiting in their next collective until the process group's timeout, so give the group a
+    short timeout."""
 
     def __init__(self, comm, ops=None, bits_per_key: float = 10.0, num_hashes: int = 7, heavy_share: float = 0.1,
                  sample: int = 65536, max_heavy: int = 256, seed: int = 0, **join_kw):
@@ -277,10 +281,12 @@ class ShardedJoin:
             parts_r.append(b_r)
             parts_s.append(b_s)
         out_r, out_s = torch.cat(parts_r), torch.cat(parts_s)
-        if hasattr(ops, "verify"):
-            ops.verify()
         count = out_r.numel()
         total = comm.all_reduce_sum(count, r_key.device)
+        # every rank learns of a failed scatter on any rank and raises, after the same collectives
+        lost = comm.all_reduce_sum(ops.lost() if hasattr(ops, "lost") else 0, r_key.device)
+        if lost:
+            raise RuntimeError(f"brig_shard_scatter: {lost} tuples found their bin full")
         stats = {"r_owned": r_own_k.numel(), "s_received": s_own_k.numel(), "s_survivors": sum(sc),
                  "s_heavy_kept": sum(sc[ws:]), "r_heavy": (r_hvy_k.numel() if heavy_t is not None else 0)}
         return ShardResult(out_r, out_s, count, total, heavy, stats)

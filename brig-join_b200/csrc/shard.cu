@@ -192,7 +192,8 @@ k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __r
     }
     if constexpr (!kWrite) {
         __syncthreads();
-        if (threadIdx.x < a.nbins && s_cnt[threadIdx.x]) atomicAdd(&counts[threadIdx.x], (unsigned long long)s_cnt[threadIdx.x]);
+        if (threadIdx.x < a.nbins && s_cnt[threadIdx.x])
+            atomicAdd(&counts[threadIdx.x], (unsigned long long)s_cnt[threadIdx.x]);
     }
 }
 
