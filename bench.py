@@ -528,15 +528,17 @@ def serve_measure(pool_n, requests, rates, streams):
 
 
 # ---- sharded join across GPUs ---------------------------------------------------------------------
-def run_shard_workload(args):
+def shard_measure(rows, steps, warmup):
     """The sharded join (brig_join.shard) on every rank of the job: one global pair of relations of
     |R| = |S| = rows x ranks tuples (the device generator, 10% of S matching), each rank holding a
     contiguous slice of both. A step is one ShardedJoin.run on every rank: R grouped by owner and
     exchanged over NCCL, the owners' filters (10 bits/key, k = 7) built and gathered, S prefiltered,
     grouped and exchanged, the local joins. Weak scaling: the rows per rank stay fixed. The first
-    run's global pair count is checked against the constructed match count. Also reported: the
-    R grouping kernels' bandwidth (key read for the counts; key and value read and written for the
-    scatter: 20 bytes per tuple) and the plain single-GPU join of one rank's slices."""
+    run's global pair count is checked against the constructed match count, and its pairs against
+    the keys. Also reported: the R grouping kernels' bandwidth (key read for the counts; key and
+    value read and written for the scatter: 20 bytes per tuple) and the plain single-GPU join of one
+    rank's slices. Joins the job's process group, or makes a one-rank NCCL group for itself.
+    Returns rank 0's line (None on the other ranks)."""
     import datetime
     import socket
     import torch
@@ -546,15 +548,17 @@ def run_shard_workload(args):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if "MASTER_ADDR" not in os.environ:
-        with socket.socket() as so:
-            so.bind(("127.0.0.1", 0))
-            os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(so.getsockname()[1])
     torch.cuda.set_device(local)
-    dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300),
-                            device_id=torch.device("cuda", local))
+    own_group = not dist.is_initialized()
+    if own_group:
+        if "MASTER_ADDR" not in os.environ or world == 1:
+            with socket.socket() as so:
+                so.bind(("127.0.0.1", 0))
+                os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(so.getsockname()[1])
+        dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
     try:
-        n = args.rows if args.rows > 0 else 1 << 26
+        n = rows
         total = n * world
         i32 = torch.int32
         stream = torch.cuda.current_stream()
@@ -564,7 +568,7 @@ def run_shard_workload(args):
         m = int(math.floor(0.1 * total))
         job = sh.ShardedJoin(sh.TorchComm(), bits_per_key=10.0, num_hashes=7)
         ev = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-        for w in range(max(args.warmup, 1)):
+        for w in range(max(warmup, 1)):
             x = job.run(rk, rv, sk, sv)
             if w == 0:  # values are global row numbers: every pair key-equal, every S row at most once
                 assert x.total == m, f"global count {x.total} != {m}"
@@ -577,13 +581,13 @@ def run_shard_workload(args):
         torch.cuda.synchronize()
         e0, e1 = ev(), ev()
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(steps):
             x = job.run(rk, rv, sk, sv)
             del x
         e1.record(stream)
         torch.cuda.synchronize()
         dist.barrier()
-        ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / args.steps
+        ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda") / steps
         # the R grouping kernels alone
         ops = job.ops
         for _ in range(3):
@@ -611,22 +615,29 @@ def run_shard_workload(args):
             b1.record(stream)
             torch.cuda.synchronize()
             plain_ms = b0.elapsed_time(b1) / 5
-        if rank == 0:
-            peak = peaks()[0]
-            split_gbs = 20.0 * n / (split_ms * 1e-3) / 1e9
-            line = {"metric": "sharded join tuples/s ((|R|+|S|)/t)", "value": 2 * total * 1e3 / ms, "unit": UNIT,
-                    "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
-                    "higher_is_better": True, "scaling": "weak", "dtype": "u32", "data": "synthetic",
-                    "config": {"workload": f"sharded join {total} x {total} over {world} rank(s), 10% match, "
-                                           "owner filters 10 bits/key k=7", "rows_per_rank": n},
-                    "r_split_ms": round(split_ms, 3),
-                    "r_split_roofline": {"bound": "hbm", "achieved": round(split_gbs, 1), "peak": peak,
-                                         "unit": "GB/s", "frac": round(split_gbs / peak, 3),
-                                         "bytes_per_tuple": 20},
-                    "plain_join_ms_one_rank_slices": round(plain_ms, 3)}
-            print(json.dumps(line), flush=True)
+        if rank != 0:
+            return None
+        peak, peak_kind = peaks()
+        split_gbs = 20.0 * n / (split_ms * 1e-3) / 1e9
+        return {"metric": "sharded join tuples/s ((|R|+|S|)/t)", "value": 2 * total * 1e3 / ms, "unit": UNIT,
+                "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": round(ms, 3),
+                "higher_is_better": True, "scaling": "weak", "dtype": "u32", "data": "synthetic",
+                "config": {"workload": f"sharded join {total} x {total} over {world} rank(s), 10% match, "
+                                       "owner filters 10 bits/key k=7", "rows_per_rank": n},
+                "r_split_ms": round(split_ms, 3),
+                "r_split_roofline": {"bound": "hbm", "achieved": round(split_gbs, 1), "peak": peak,
+                                     "unit": "GB/s", "frac": round(split_gbs / peak, 3), "bytes_per_tuple": 20,
+                                     "peak_kind": peak_kind},
+                "plain_join_ms_one_rank_slices": round(plain_ms, 3)}
     finally:
-        dist.destroy_process_group()
+        if own_group:
+            dist.destroy_process_group()
+
+
+def run_shard_workload(args):
+    line = shard_measure(args.rows if args.rows > 0 else 1 << 26, args.steps, args.warmup)
+    if line is not None:
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -864,6 +875,14 @@ def main():
                            "one_at_a_time": [{k: x[k] for k in ("offered_req_per_s", "p50_ms", "p99_ms",
                                                                 "tuples_per_s")}
                                              for x in sv_["one_at_a_time"]]}
+        torch.cuda.empty_cache()
+        try:  # the sharded join's path on this one GPU (a one-rank NCCL group)
+            sh_ = shard_measure(1 << 25, 5, 3)
+            extras["shard"] = {k: sh_[k] for k in ("value", "unit", "ms_per_step", "r_split_ms", "r_split_roofline",
+                                                   "plain_join_ms_one_rank_slices")}
+            extras["shard"]["workload"] = sh_["config"]["workload"]
+        except Exception as e:  # noqa: BLE001 - reported in the line; the join's figures stand
+            extras["shard"] = {"error": f"{type(e).__name__}: {e}"[:300]}
 
     if rank == 0:
         line = {
