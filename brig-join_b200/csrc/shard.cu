@@ -39,11 +39,11 @@ constexpr int kShardTile = kShardThreads * kShardItems;
 constexpr int kMaxBins = BRIG_SHARD_MAX_RANKS + 1;
 constexpr uint32_t kOwnerSeed = 0x6a09e667u;  // the first 32 fractional bits of sqrt(2)
 
-// CTAs of k_shard_split per SM: 32 registers a thread for the count without filters, 42 for the
-// scatter without filters, 64 with filters (8 filter word pairs and masks in flight) and for the
-// scatter that reads a bin cache.
+// CTAs of k_shard_split per SM: 32 registers a thread for the count without filters, 64 for the
+// scatters (keys, values, bins and ranks of 8 tuples) and with filters (8 filter word pairs and
+// masks in flight).
 constexpr int shard_ctas(bool write, bool filter, bool cache = false) {
-    return (filter || cache) ? 2 : (write ? 3 : 4);
+    return (filter || cache || write) ? 2 : 4;
 }
 
 BRIG_HD uint32_t owner_of(uint32_t key, uint32_t nranks) { return fastrange32(mix32(key ^ kOwnerSeed), nranks); }
@@ -101,12 +101,15 @@ k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __r
     const int64_t ntiles = (n + kShardTile - 1) / kShardTile;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const int64_t t0 = t * kShardTile;
-        uint32_t kk[kShardItems];
+        uint32_t kk[kShardItems], vv[kShardItems];
         int bin[kShardItems];
+        // a scatter without filters keeps every tuple: its values load with its keys
+        constexpr bool kAllKept = kWrite && !kFilter && !kCache;
 #pragma unroll
         for (int u = 0; u < kShardItems; ++u) {
             const int64_t i = t0 + u * kShardThreads + threadIdx.x;
             kk[u] = i < n ? key[i] : 0u;
+            vv[u] = (kAllKept && i < n) ? val[i] : 0u;
             bin[u] = i < n ? 0 : -1;
         }
         if constexpr (kCache) {
@@ -156,6 +159,12 @@ k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __r
                 }
             }
         }
+        if constexpr (kWrite && !kAllKept) {
+            // the kept tuples' values, in flight while the tile is ranked and the bins reserved
+#pragma unroll
+            for (int u = 0; u < kShardItems; ++u)
+                if (bin[u] >= 0) vv[u] = val[t0 + u * kShardThreads + threadIdx.x];
+        }
         uint32_t rank[kShardItems];
 #pragma unroll
         for (int u = 0; u < kShardItems; ++u) {
@@ -182,7 +191,7 @@ k_shard_split(ShardArgs a, const uint32_t* __restrict__ key, const uint32_t* __r
                 const int64_t p = s_base[b] + rank[u];
                 if (p < s_end[b]) {
                     out_key[p] = kk[u];
-                    out_val[p] = val[t0 + u * kShardThreads + threadIdx.x];
+                    out_val[p] = vv[u];
                 } else {
                     atomicAdd(errors, 1ull);
                 }
