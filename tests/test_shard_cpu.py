@@ -117,6 +117,61 @@ def test_a_rank_without_tuples(shard, oracle):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
+def test_heavy_keys_take_the_heaviest_up_to_the_cap(shard, oracle):
+    """Five hot keys of different weights and a cap of two: every rank picks the same two, the
+    heaviest ones."""
+    size = 3
+    rng = np.random.default_rng(3)
+    (rk, rv, sk, sv), parts = spread(oracle, 17, 5000, 60_000, size, match=0.1)
+    sk = sk.copy()
+    hot = rk[10:15]
+    rows = rng.permutation(len(sk))
+    start = 0
+    for key, share in zip(hot, (0.20, 0.16, 0.12, 0.08, 0.04)):
+        n = int(share * len(sk))
+        sk[rows[start:start + n]] = key
+        start += n
+    cut = [(len(sk) * r // size, len(sk) * (r + 1) // size) for r in range(size)]
+    parts = [(parts[r][0], parts[r][1], sk[a:b], sv[a:b]) for r, (a, b) in enumerate(cut)]
+    hub = Hub(size)
+
+    def rank(r):
+        job = shard.ShardedJoin(ThreadComm(hub, r), HostShardOps(oracle), bits_per_key=0.0, max_heavy=2,
+                                sample=8192)
+        return job.heavy_keys(torch.from_numpy(parts[r][2].view(np.int32).copy()))
+
+    got = run_ranks(hub, rank)
+    assert all(np.array_equal(g, got[0]) for g in got)
+    assert got[0].tolist() == sorted(int(k) for k in hot[:2])
+
+
+def test_exchanges_of_nothing(shard):
+    """Every rank sends and gathers empty blocks: the exchanges return empty tensors and sizes."""
+    size = 2
+    hub = Hub(size)
+
+    def rank(r):
+        c = ThreadComm(hub, r)
+        y, rc = c.all_to_all_v(torch.zeros(0, dtype=torch.int32), [0, 0])
+        g, sizes = c.all_gather_v(torch.zeros(0, dtype=torch.int32))
+        return y.numel(), rc, g.numel(), sizes, c.all_reduce_sum(0, "cpu")
+
+    assert run_ranks(hub, rank) == [(0, [0, 0], 0, [0, 0], 0)] * size
+
+
+def test_sharded_join_arguments(shard, oracle):
+    class Many:
+        rank, size = 0, 65
+
+    with pytest.raises(ValueError):
+        shard.ShardedJoin(Many(), HostShardOps(oracle))
+    with pytest.raises(ValueError):
+        shard.ShardedJoin(ThreadComm(Hub(1), 0), HostShardOps(oracle), max_heavy=shard.MAX_HEAVY + 1)
+    with pytest.raises(TypeError):
+        shard.ShardedJoin(ThreadComm(Hub(1), 0), HostShardOps(oracle)).run(
+            *(torch.zeros(3, dtype=torch.int64) for _ in range(4)))
+
+
 def test_heavy_keys_keep_a_hot_key_off_its_owner(shard, oracle):
     """A key held by 40% of S: with the heavy-key handling every rank receives about its fair
     share; without it the hot key's owner receives its whole share of S."""
